@@ -1,0 +1,128 @@
+"""The oracle pinned against the reference's own golden vectors and known answers.
+
+CPU only.  These tests establish that oracle/cs_oracle.c (the checker every GPU parity
+test uses) reproduces the reference: the field known answers and MSM golden files from
+the reference's C test suite (test/c/test_utils_host.cpp, test/c/aux_data), plus
+outputs of the reference library itself captured in tests/golden/ref_transforms.npz.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import random_field, hstep_roots_table, limbs_to_int, R, Q
+
+
+def test_field_known_answers(oracle, golden):
+    kat = golden("field_kat.npz")
+    # test_mul (test_utils_host.cpp:7160): montmult_h(A, B, MOD_FIELD) == C
+    got = oracle.montmult(kat["A"], kat["B"], 1)
+    assert np.array_equal(got, kat["C"])
+    # test_mul_ext (test_utils_host.cpp:8589): Fp2 products, pidx 1
+    X = kat["ext_X"]
+    n = X.shape[0] // 2
+    for i in range(n):
+        z = np.zeros(16, np.uint32)
+        a = np.ascontiguousarray(X[2 * i]); b = np.ascontiguousarray(X[2 * i + 1])
+        oracle.lib.or_montmult_ext(z.ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_uint32)),
+                                   a.ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_uint32)),
+                                   b.ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_uint32)), 1)
+        assert np.array_equal(z, kat["ext_X0X1"][i]), i
+
+
+def test_roots_known_answers(oracle, golden):
+    kat = golden("field_kat.npz")
+    # test_findroots (test_utils_host.cpp:7343): the 128 powers of p_root128
+    roots = oracle.root_powers(kat["p_root128"], 128)
+    assert np.array_equal(roots, kat["roots_128"])
+    # p_root128 is a primitive 128th root; ours (proots_field[7]) generates the same group
+    w = limbs_to_int(oracle.from_mont(kat["p_root128"], 1)[0])
+    assert pow(w, 128, R) == 1 and pow(w, 64, R) != 1
+    ours = limbs_to_int(oracle.from_mont(oracle.find_roots(7)[1], 1)[0])
+    assert pow(ours, 128, R) == 1 and pow(ours, 64, R) != 1
+
+
+@pytest.mark.parametrize("ec2,name", [(0, "g1_msm_1024.npz"), (1, "g2_msm_1024.npz")])
+@pytest.mark.parametrize("order", [1, 6, 8])
+def test_msm_golden(oracle, golden, ec2, name, order):
+    g = golden(name)
+    out = oracle.msm(g["scalars"], g["points"], ec2=ec2, order=order)
+    assert np.array_equal(out, g["reduction"])
+
+
+@pytest.mark.parametrize("ec2,name", [(0, "g1_msm_1024.npz"), (1, "g2_msm_1024.npz")])
+def test_scmul_golden(oracle, golden, ec2, name):
+    g = golden(name)
+    per = oracle.jac2aff(g["per_point_jac"], ec2)
+    got = oracle.scmul(g["scalars"][:64], g["points"][:64], ec2)
+    assert np.array_equal(got, per)
+
+
+def test_golden_points_on_curve(oracle, golden):
+    for ec2, name in ((0, "g1_msm_1024.npz"), (1, "g2_msm_1024.npz")):
+        g = golden(name)
+        for i in (0, 1, 500, 1022, 1023):
+            assert oracle.isoncurve(g["points"][i], ec2)
+
+
+@pytest.mark.parametrize("L", [4, 7, 10])
+def test_ntt_matches_reference_fixture(oracle, golden, L):
+    f = golden("ref_transforms.npz")
+    A = f[f"ntt_in_{L}"]
+    roots = oracle.find_roots(L + 1)
+    assert np.array_equal(oracle.ntt(A, roots, L, 1, 2, 1, 1), f[f"ntt_fwd_{L}"])
+    assert np.array_equal(oracle.intt(A, roots, L, 2, 1, 1), f[f"ntt_inv_mont_{L}"])
+    assert np.array_equal(oracle.intt(A, roots, L, 2, 0, 1), f[f"ntt_inv_ext_{L}"])
+
+
+@pytest.mark.parametrize("L", [4, 7, 10])
+def test_hstep_matches_reference_fixture(oracle, golden, L):
+    f = golden("ref_transforms.npz")
+    roots = oracle.find_roots(L + 1)
+    M = oracle.interpolandmul(f[f"hstep_A_{L}"], f[f"hstep_B_{L}"], roots, L, 2)
+    assert np.array_equal(M, f[f"hstep_M_{L}"])
+
+
+@pytest.mark.parametrize("nv", [16, 300])
+def test_mpoly_matches_reference_fixture(oracle, golden, nv):
+    f = golden("ref_transforms.npz")
+    nc = int(f[f"mpoly_ncons_{nv}"][0])
+    out = oracle.mpoly_eval(f[f"mpoly_w_{nv}"], f[f"mpoly_pin_{nv}"], nc, 0, nv, 1)
+    assert np.array_equal(out, f[f"mpoly_out_{nv}"])
+
+
+def test_hstep_coset_equals_reference_variant_on_satisfying_input(oracle):
+    """For A*B - C divisible by Z = x^m - 1 both H-step variants give the quotient."""
+    L = 6
+    m = 1 << L
+    rng = np.random.Generator(np.random.PCG64(7))
+    roots = oracle.find_roots(L + 1)
+    A = oracle.to_mont(random_field(rng, m), 1)
+    B = oracle.to_mont(random_field(rng, m), 1)
+    C = oracle.montmult(A, B, 1)  # C = A*B on the domain -> satisfying
+    Mref = oracle.interpolandmul(A, B, roots, L, 2)
+    H = oracle.hstep_coset(A, B, C, L)
+    assert np.array_equal(H[:m - 1], Mref[m:2 * m - 1])
+    assert not H[m - 1].any()
+    assert not Mref[2 * m - 1].any()
+
+
+def test_random_against_reference_library(oracle, reflib):
+    rng = np.random.Generator(np.random.PCG64(11))
+    # field
+    a = random_field(rng, 64, 0); b = random_field(rng, 64, 0)
+    assert np.array_equal(oracle.montmult(a, b, 0), reflib.montmult(a, b, 0))
+    # msm with uniform scalars over random points, G1 and G2
+    from oracle.oracle import G1_GEN, G2_GEN, ints_to_limbs, to_mont_int
+    g1 = np.concatenate([ints_to_limbs([to_mont_int(c, 0)]) for c in G1_GEN]).reshape(16)
+    g2 = np.concatenate([ints_to_limbs([to_mont_int(c, 0) for c in xy]) for xy in G2_GEN]).reshape(32)
+    for ec2, g in ((0, g1), (1, g2)):
+        k = random_field(rng, 200, 1)
+        pts = oracle.scmul(k, g.reshape(1, -1), ec2)
+        s = random_field(rng, 200, 1)
+        assert np.array_equal(oracle.msm(s, pts, ec2), reflib.msm(s, pts, ec2))
+    # H step with the reference prover's own roots-table layout and 4-step split
+    L = 9
+    A = oracle.to_mont(random_field(rng, 1 << L), 1)
+    B = oracle.to_mont(random_field(rng, 1 << L), 1)
+    table = hstep_roots_table(oracle, L)
+    assert np.array_equal(oracle.interpolandmul(A, B, oracle.find_roots(L + 1), L, 2),
+                          reflib.interpolandmul(A, B, table, L, 2))
