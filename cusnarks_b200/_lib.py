@@ -1,0 +1,91 @@
+"""ctypes binding of libcusnarks_b200.so (declarations: include/cusnarks_b200.h).
+
+The library is the product: every call here runs CUDA kernels.  There is no CPU
+fallback -- if the shared library is missing or cannot be loaded, ``lib()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libcusnarks_b200.so")
+
+CS_OK = 0
+CS_ERR_CUDA = 1
+CS_ERR_ARG = 2
+CS_ERR_NOMEM = 3
+CS_ERR_UNSUPPORTED = 4
+CS_ERR_NODEVICE = 5
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_vp = ctypes.c_void_p
+
+
+class CsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"cusnarks_b200 error {code}: {msg}")
+        self.code = code
+
+
+class JacaddReduced(ctypes.Structure):
+    """jacadd_reduced_t (reference src/cuda/types.h:548-567)."""
+    _fields_ = [("out_ep", _vp), ("scl", _vp), ("x", _vp), ("n", ctypes.c_uint32),
+                ("ec2", ctypes.c_uint32), ("compute_table", ctypes.c_uint32), ("ec_table", _vp),
+                ("pidx", ctypes.c_uint32), ("max_threads", ctypes.c_uint32),
+                ("start_idx", ctypes.c_uint32), ("last_idx", ctypes.c_uint32),
+                ("thread_id", ctypes.c_uint32), ("pippen", ctypes.c_uint32),
+                ("offset", ctypes.c_uint64), ("total_words", ctypes.c_uint64),
+                ("order", ctypes.c_uint32), ("filename", ctypes.c_char_p)]
+
+
+# (name, restype, argtypes)
+_SIGNATURES = [
+    ("cs_ctx_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("cs_ctx_destroy", None, [_vp]),
+    ("cs_ctx_set_stream", ctypes.c_int, [_vp, _vp]),
+    ("cs_ctx_stream", _vp, [_vp]),
+    ("cs_ctx_sync", ctypes.c_int, [_vp]),
+    ("cs_ctx_error", ctypes.c_char_p, [_vp]),
+    ("cs_ctx_last_ms", ctypes.c_float, [_vp]),
+    ("cs_last_status", ctypes.c_int, []),
+    ("cs_last_error", ctypes.c_char_p, []),
+    ("cs_msm", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp, ctypes.c_int]),
+    ("cs_msm_device", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp, ctypes.c_int]),
+    ("cs_msm_workspace_bytes", ctypes.c_size_t, [ctypes.c_uint32, ctypes.c_int, ctypes.c_int]),
+    ("ec_jacreduce_server_h", None, [ctypes.POINTER(JacaddReduced)]),
+    ("ec2_jacreduce_server_h", None, [ctypes.POINTER(JacaddReduced)]),
+]
+
+_lock = threading.Lock()
+_lib = None
+
+
+def exported_symbols():
+    return [name for name, _, _ in _SIGNATURES]
+
+
+def lib() -> ctypes.CDLL:
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with `python -m cusnarks_b200.build` "
+                    "(nvcc, sm_100a).  There is no CPU fallback.")
+            L = ctypes.CDLL(LIB_PATH)
+            for name, res, args in _SIGNATURES:
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = L
+    return _lib
+
+
+def check(code: int, ctx=None):
+    if code != CS_OK:
+        L = lib()
+        msg = (L.cs_ctx_error(ctx) if ctx else L.cs_last_error()) or b""
+        raise CsError(code, msg.decode(errors="replace"))

@@ -1,0 +1,237 @@
+// capi.cu -- extern "C" entry points (include/cusnarks_b200.h).
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/cusnarks_b200.h"
+#include "msm.cuh"
+#include "runtime.cuh"
+
+namespace csb {
+
+int fail(cs_ctx* ctx, cudaError_t e, const char* where) {
+  if (ctx) ctx->err = std::string(where) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();  // clear the sticky-free error state
+  return e == cudaErrorMemoryAllocation ? CS_ERR_NOMEM : CS_ERR_CUDA;
+}
+int fail_msg(cs_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+}  // namespace csb
+
+using csb::fail;
+using csb::fail_msg;
+
+namespace {
+
+thread_local int t_status = CS_OK;
+thread_local std::string t_error;
+
+std::mutex g_default_mu;
+cs_ctx* g_default[64] = {nullptr};
+
+int set_thread_status(int st, cs_ctx* ctx) {
+  t_status = st;
+  t_error = (st == CS_OK || ctx == nullptr) ? std::string() : ctx->err;
+  return st;
+}
+
+// Process-wide context of the calling thread's current device, for the drop-in calls.
+cs_ctx* default_ctx(int* status) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+    *status = CS_ERR_NODEVICE;
+    t_error = std::string("no CUDA device: ") + cudaGetErrorString(e);
+    cudaGetLastError();
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  if (!g_default[dev]) {
+    cs_ctx* c = nullptr;
+    int st = cs_ctx_create(dev, &c);
+    if (st != CS_OK) {
+      *status = st;
+      t_error = "context creation failed";
+      return nullptr;
+    }
+    g_default[dev] = c;
+  }
+  *status = CS_OK;
+  return g_default[dev];
+}
+
+struct EventScope {
+  cs_ctx* ctx;
+  explicit EventScope(cs_ctx* c) : ctx(c) { cudaEventRecord(ctx->ev_start, ctx->stream); }
+  void stop() { cudaEventRecord(ctx->ev_stop, ctx->stream); }
+};
+
+int msm_device_locked(cs_ctx* ctx, int ec2, const uint32_t* s, const uint32_t* p, uint32_t n,
+                      uint32_t* out, int window) {
+  const size_t need = csb::msm_workspace_bytes(n, window, ec2 != 0);
+  cudaError_t e = ctx->work.reserve(need, ctx->stream);
+  if (e != cudaSuccess) return fail(ctx, e, "msm workspace");
+  csb::MsmConfig cfg;
+  cfg.c = window;
+  EventScope ev(ctx);
+  e = ec2 ? csb::msm_g2(s, p, n, out, ctx->work.ptr, ctx->work.bytes, cfg, ctx->stream)
+          : csb::msm_g1(s, p, n, out, ctx->work.ptr, ctx->work.bytes, cfg, ctx->stream);
+  ev.stop();
+  if (e != cudaSuccess) return fail(ctx, e, "msm launch");
+  return CS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cs_ctx_create(int device, cs_ctx** out) {
+  if (!out) return CS_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return CS_ERR_NODEVICE;
+  }
+  if (device < 0 || device >= ndev) return CS_ERR_ARG;
+  std::unique_ptr<cs_ctx> c(new cs_ctx());
+  c->device = device;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev_start);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev_stop);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return CS_ERR_CUDA;
+  }
+  c->own_stream = true;
+  *out = c.release();
+  return CS_OK;
+}
+
+void cs_ctx_destroy(cs_ctx* ctx) {
+  if (!ctx) return;
+  cudaStreamSynchronize(ctx->stream);
+  ctx->work.release();
+  ctx->in.release();
+  ctx->out.release();
+  if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
+  if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+int cs_ctx_set_stream(cs_ctx* ctx, void* stream) {
+  if (!ctx) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (ctx->own_stream && ctx->stream) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+  }
+  ctx->stream = static_cast<cudaStream_t>(stream);
+  ctx->own_stream = false;
+  return CS_OK;
+}
+
+void* cs_ctx_stream(cs_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+int cs_ctx_sync(cs_ctx* ctx) {
+  if (!ctx) return CS_ERR_ARG;
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return fail(ctx, e, "stream sync");
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
+  cudaGetLastError();
+  return CS_OK;
+}
+
+const char* cs_ctx_error(cs_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+float cs_ctx_last_ms(cs_ctx* ctx) { return ctx ? ctx->last_ms : 0.f; }
+
+size_t cs_msm_workspace_bytes(uint32_t n, int ec2, int window) {
+  return csb::msm_workspace_bytes(n, window, ec2 != 0);
+}
+
+int cs_msm_device(cs_ctx* ctx, int ec2, const uint32_t* d_scalars, const uint32_t* d_points,
+                  uint32_t n, uint32_t* d_out, int window) {
+  if (!ctx || (!d_out) || (n && (!d_scalars || !d_points))) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  return msm_device_locked(ctx, ec2, d_scalars, d_points, n, d_out, window);
+}
+
+int cs_msm(cs_ctx* ctx, int ec2, const uint32_t* scalars, const uint32_t* points, uint32_t n,
+           uint32_t* out_affine, int window) {
+  if (!ctx || !out_affine || (n && (!scalars || !points))) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  const size_t pw = ec2 ? 32 : 16;
+  const size_t sbytes = (size_t)n * 8 * 4, pbytes = (size_t)n * pw * 4;
+  const size_t sb_al = (sbytes + 255) & ~size_t(255);
+  cudaError_t e = ctx->in.reserve(sb_al + pbytes + 256, ctx->stream);
+  if (e != cudaSuccess) return fail(ctx, e, "msm input buffer");
+  e = ctx->out.reserve(256, ctx->stream);
+  if (e != cudaSuccess) return fail(ctx, e, "msm output buffer");
+  uint32_t* ds = static_cast<uint32_t*>(ctx->in.ptr);
+  uint32_t* dp = reinterpret_cast<uint32_t*>(static_cast<char*>(ctx->in.ptr) + sb_al);
+  uint32_t* dout = static_cast<uint32_t*>(ctx->out.ptr);
+  if (n) {
+    if ((e = cudaMemcpyAsync(ds, scalars, sbytes, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+      return fail(ctx, e, "msm H2D scalars");
+    if ((e = cudaMemcpyAsync(dp, points, pbytes, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+      return fail(ctx, e, "msm H2D points");
+  }
+  int st = msm_device_locked(ctx, ec2, ds, dp, n, dout, window);
+  if (st != CS_OK) return st;
+  if ((e = cudaMemcpyAsync(out_affine, dout, pw * 4, cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess)
+    return fail(ctx, e, "msm D2H");
+  if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(ctx, e, "msm sync");
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
+  return CS_OK;
+}
+
+// ------------------------------------------------------------ drop-in entry points ---
+int cs_last_status(void) { return t_status; }
+const char* cs_last_error(void) { return t_error.c_str(); }
+
+void ec_jacreduce_server_h(jacadd_reduced_t* args) {
+  if (!args || !args->out_ep) {
+    t_status = CS_ERR_ARG;
+    t_error = "ec_jacreduce_server_h: null arguments";
+    return;
+  }
+  if (args->filename != nullptr) {
+    t_status = CS_ERR_UNSUPPORTED;
+    t_error = "ec_jacreduce_server_h: precomputed table files are not supported";
+    return;
+  }
+  if (args->pidx != 0) {
+    t_status = CS_ERR_ARG;
+    t_error = "ec_jacreduce_server_h: curve coordinates live in MOD_GROUP (pidx 0)";
+    return;
+  }
+  if (args->n && (!args->scl || !args->x)) {
+    t_status = CS_ERR_ARG;
+    t_error = "ec_jacreduce_server_h: null scalar or point array";
+    return;
+  }
+  int st = CS_OK;
+  cs_ctx* ctx = default_ctx(&st);
+  if (!ctx) {
+    t_status = st;
+    return;
+  }
+  st = cs_msm(ctx, args->ec2 ? 1 : 0, args->scl, args->x, args->n, args->out_ep, 0);
+  set_thread_status(st, ctx);
+}
+
+void ec2_jacreduce_server_h(jacadd_reduced_t* args) { ec_jacreduce_server_h(args); }
+
+}  // extern "C"

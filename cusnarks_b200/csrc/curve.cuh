@@ -1,0 +1,190 @@
+// curve.cuh -- BN254 G1 (over Fq) and G2 (over Fq2) point arithmetic on sm_100a.
+//
+// Accumulators use extended Jacobian "XYZZ" coordinates (x = X/ZZ, y = Y/ZZZ,
+// ZZ^3 = ZZZ^2): a mixed addition costs 8M + 2S and needs no inversion, a full addition
+// 12M + 2S, a doubling 6M + 3S (formulas from the Explicit-Formulas Database,
+// add-2008-s / madd-2008-s / dbl-2008-s-1 for a = 0).  Infinity is ZZ = 0.
+//
+// Affine points in memory follow the reference layout (src/cuda/types.h ECP_JAC_INDIMS):
+// G1 = X | Y (16 words), G2 = X.c0 | X.c1 | Y.c0 | Y.c1 (32 words), Montgomery form, with
+// the reference's infinity encoding (0, 1_mont) (src/cuda/constants.cpp:264-292).
+#pragma once
+#include "field.cuh"
+
+namespace csb {
+
+template <class F>
+struct Affine {
+  F x, y;
+};
+
+template <class F>
+struct XYZZ {
+  F X, Y, ZZ, ZZZ;
+
+  static CSB_DEV XYZZ inf() { return {F::zero(), F::one(), F::zero(), F::zero()}; }
+  CSB_DEV bool is_inf() const { return ZZ.is_zero(); }
+  static CSB_DEV XYZZ from_affine(const Affine<F>& a) { return {a.x, a.y, F::one(), F::one()}; }
+};
+
+// the reference's affine infinity: X == 0 and Y == 1 (Montgomery)
+template <class F>
+CSB_DEV bool affine_is_inf(const Affine<F>& a) {
+  return a.x.is_zero() && a.y == F::one();
+}
+
+// dbl-2008-s-1 (a = 0)
+template <class F>
+CSB_DEV XYZZ<F> xyzz_dbl(const XYZZ<F>& p) {
+  if (p.is_inf()) return p;
+  const F U = p.Y.dbl();
+  const F V = U.sqr();
+  const F W = U * V;
+  const F S = p.X * V;
+  const F X2 = p.X.sqr();
+  const F M = X2.dbl() + X2;
+  XYZZ<F> r;
+  r.X = M.sqr() - S.dbl();
+  r.Y = M * (S - r.X) - W * p.Y;
+  r.ZZ = V * p.ZZ;
+  r.ZZZ = W * p.ZZZ;
+  return r;
+}
+
+// mdbl-2008-s-1: double an affine point
+template <class F>
+CSB_DEV XYZZ<F> xyzz_mdbl(const Affine<F>& p) {
+  const F U = p.y.dbl();
+  const F V = U.sqr();
+  const F W = U * V;
+  const F S = p.x * V;
+  const F X2 = p.x.sqr();
+  const F M = X2.dbl() + X2;
+  XYZZ<F> r;
+  r.X = M.sqr() - S.dbl();
+  r.Y = M * (S - r.X) - W * p.y;
+  r.ZZ = V;
+  r.ZZZ = W;
+  return r;
+}
+
+// madd-2008-s: p (XYZZ) + q (affine, not infinity)
+template <class F>
+CSB_DEV XYZZ<F> xyzz_madd(const XYZZ<F>& p, const Affine<F>& q) {
+  if (p.is_inf()) return XYZZ<F>::from_affine(q);
+  const F U2 = q.x * p.ZZ;
+  const F S2 = q.y * p.ZZZ;
+  const F P = U2 - p.X;
+  const F R = S2 - p.Y;
+  if (P.is_zero()) {
+    if (R.is_zero()) return xyzz_mdbl(q);
+    return XYZZ<F>::inf();
+  }
+  const F PP = P.sqr();
+  const F PPP = P * PP;
+  const F Q = p.X * PP;
+  XYZZ<F> r;
+  r.X = R.sqr() - PPP - Q.dbl();
+  r.Y = R * (Q - r.X) - p.Y * PPP;
+  r.ZZ = p.ZZ * PP;
+  r.ZZZ = p.ZZZ * PPP;
+  return r;
+}
+
+// add-2008-s: p + q, both XYZZ
+template <class F>
+CSB_DEV XYZZ<F> xyzz_add(const XYZZ<F>& p, const XYZZ<F>& q) {
+  if (p.is_inf()) return q;
+  if (q.is_inf()) return p;
+  const F U1 = p.X * q.ZZ;
+  const F U2 = q.X * p.ZZ;
+  const F S1 = p.Y * q.ZZZ;
+  const F S2 = q.Y * p.ZZZ;
+  const F P = U2 - U1;
+  const F R = S2 - S1;
+  if (P.is_zero()) {
+    if (R.is_zero()) return xyzz_dbl(p);
+    return XYZZ<F>::inf();
+  }
+  const F PP = P.sqr();
+  const F PPP = P * PP;
+  const F Q = U1 * PP;
+  XYZZ<F> r;
+  r.X = R.sqr() - PPP - Q.dbl();
+  r.Y = R * (Q - r.X) - S1 * PPP;
+  r.ZZ = p.ZZ * q.ZZ * PP;
+  r.ZZZ = p.ZZZ * q.ZZZ * PPP;
+  return r;
+}
+
+template <class F>
+CSB_DEV XYZZ<F> xyzz_neg(const XYZZ<F>& p) {
+  XYZZ<F> r = p;
+  r.Y = p.Y.neg();
+  return r;
+}
+
+// XYZZ -> affine with the reference infinity encoding
+template <class F>
+CSB_DEV Affine<F> xyzz_to_affine(const XYZZ<F>& p) {
+  if (p.is_inf()) return {F::zero(), F::one()};
+  const F t = (p.ZZ * p.ZZZ).inv();   // 1 / (ZZ ZZZ)
+  const F izz = t * p.ZZZ;            // 1 / ZZ
+  const F izzz = t * p.ZZ;            // 1 / ZZZ
+  return {p.X * izz, p.Y * izzz};
+}
+
+// ------------------------------------------------------------------ memory I/O -------
+// 128-bit loads/stores of limbs; pointers must be 16-byte aligned.
+CSB_DEV void ld_limbs8(uint32_t (&v)[8], const uint32_t* p) {
+  const uint4 a = __ldg(reinterpret_cast<const uint4*>(p));
+  const uint4 b = __ldg(reinterpret_cast<const uint4*>(p) + 1);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+CSB_DEV void st_limbs8(uint32_t* p, const uint32_t (&v)[8]) {
+  reinterpret_cast<uint4*>(p)[0] = make_uint4(v[0], v[1], v[2], v[3]);
+  reinterpret_cast<uint4*>(p)[1] = make_uint4(v[4], v[5], v[6], v[7]);
+}
+template <class M>
+CSB_DEV Fp<M> ld_fp(const uint32_t* p) { Fp<M> r; ld_limbs8(r.v, p); return r; }
+template <class M>
+CSB_DEV void st_fp(uint32_t* p, const Fp<M>& a) { st_limbs8(p, a.v); }
+
+// number of 32-bit words of one coordinate
+template <class F> struct FieldWords;
+template <> struct FieldWords<Fq> { static constexpr int value = 8; };
+template <> struct FieldWords<Fq2> { static constexpr int value = 16; };
+
+CSB_DEV void ld_field(Fq& a, const uint32_t* p) { ld_limbs8(a.v, p); }
+CSB_DEV void ld_field(Fq2& a, const uint32_t* p) { ld_limbs8(a.c0.v, p); ld_limbs8(a.c1.v, p + 8); }
+CSB_DEV void st_field(uint32_t* p, const Fq& a) { st_limbs8(p, a.v); }
+CSB_DEV void st_field(uint32_t* p, const Fq2& a) { st_limbs8(p, a.c0.v); st_limbs8(p + 8, a.c1.v); }
+
+template <class F>
+CSB_DEV Affine<F> ld_affine(const uint32_t* p) {
+  constexpr int W = FieldWords<F>::value;
+  Affine<F> a;
+  ld_field(a.x, p);
+  ld_field(a.y, p + W);
+  return a;
+}
+template <class F>
+CSB_DEV void st_affine(uint32_t* p, const Affine<F>& a) {
+  constexpr int W = FieldWords<F>::value;
+  st_field(p, a.x);
+  st_field(p + W, a.y);
+}
+template <class F>
+CSB_DEV XYZZ<F> ld_xyzz(const uint32_t* p) {
+  constexpr int W = FieldWords<F>::value;
+  XYZZ<F> a;
+  ld_field(a.X, p); ld_field(a.Y, p + W); ld_field(a.ZZ, p + 2 * W); ld_field(a.ZZZ, p + 3 * W);
+  return a;
+}
+template <class F>
+CSB_DEV void st_xyzz(uint32_t* p, const XYZZ<F>& a) {
+  constexpr int W = FieldWords<F>::value;
+  st_field(p, a.X); st_field(p + W, a.Y); st_field(p + 2 * W, a.ZZ); st_field(p + 3 * W, a.ZZZ);
+}
+
+}  // namespace csb

@@ -1,0 +1,206 @@
+// field.cuh -- 256-bit Montgomery arithmetic for BN254 on sm_100a.
+//
+// Elements are 8 little-endian 32-bit limbs held in registers, Montgomery form
+// x * 2^256 mod p, always fully reduced to [0, p) at the boundary of every operation, so
+// results are word-for-word the values the reference's host code produces
+// (src/cuda/ff.cpp montmult_h / addm_h / subm_h, same layout as src/cuda/types.h
+// NWORDS_256BIT).  Products are CIOS Montgomery multiplications built from
+// mad.lo.cc / madc.hi.cc carry chains (IMAD with carry-in/out).  BN254 moduli are below
+// 2^254, so the CIOS accumulator never needs a tenth limb and a single conditional
+// subtraction finishes every product.
+#pragma once
+#include <cstdint>
+
+namespace csb {
+
+#define CSB_DEV __device__ __forceinline__
+
+// ---------------------------------------------------------------- moduli ------------
+struct ModQ {  // base field q (the reference's MOD_GROUP, pidx 0)
+  static constexpr uint32_t P0 = 0xd87cfd47u, P1 = 0x3c208c16u, P2 = 0x6871ca8du, P3 = 0x97816a91u,
+                            P4 = 0x8181585du, P5 = 0xb85045b6u, P6 = 0xe131a029u, P7 = 0x30644e72u;
+  static constexpr uint32_t NP0 = 0xe4866389u;  // -q^-1 mod 2^32
+  static constexpr uint32_t ONE0 = 0xc58f0d9du, ONE1 = 0xd35d438du, ONE2 = 0xf5c70b3du, ONE3 = 0x0a78eb28u,
+                            ONE4 = 0x7879462cu, ONE5 = 0x666ea36fu, ONE6 = 0x9a07df2fu, ONE7 = 0x0e0a77c1u;
+  static constexpr uint32_t R20 = 0x538afa89u, R21 = 0xf32cfc5bu, R22 = 0xd44501fbu, R23 = 0xb5e71911u,
+                            R24 = 0x0a417ff6u, R25 = 0x47ab1effu, R26 = 0xcab8351fu, R27 = 0x06d89f71u;
+};
+struct ModR {  // scalar field r (the reference's MOD_FIELD, pidx 1)
+  static constexpr uint32_t P0 = 0xf0000001u, P1 = 0x43e1f593u, P2 = 0x79b97091u, P3 = 0x2833e848u,
+                            P4 = 0x8181585du, P5 = 0xb85045b6u, P6 = 0xe131a029u, P7 = 0x30644e72u;
+  static constexpr uint32_t NP0 = 0xefffffffu;  // -r^-1 mod 2^32
+  static constexpr uint32_t ONE0 = 0x4ffffffbu, ONE1 = 0xac96341cu, ONE2 = 0x9f60cd29u, ONE3 = 0x36fc7695u,
+                            ONE4 = 0x7879462eu, ONE5 = 0x666ea36fu, ONE6 = 0x9a07df2fu, ONE7 = 0x0e0a77c1u;
+  static constexpr uint32_t R20 = 0xae216da7u, R21 = 0x1bb8e645u, R22 = 0xe35c59e3u, R23 = 0x53fe3ab1u,
+                            R24 = 0x53bb8085u, R25 = 0x8c49833du, R26 = 0x7f4e44a5u, R27 = 0x0216d0b1u;
+};
+
+// ------------------------------------------------------------ carry-chain helpers ----
+// Each helper is one PTX instruction; `volatile` keeps the carry flag sequence in
+// program order.
+#define MAD_LO_CC(d, a, b)  asm volatile("mad.lo.cc.u32 %0, %1, %2, %0;" : "+r"(d) : "r"(a), "r"(b))
+#define MADC_LO_CC(d, a, b) asm volatile("madc.lo.cc.u32 %0, %1, %2, %0;" : "+r"(d) : "r"(a), "r"(b))
+#define MAD_HI_CC(d, a, b)  asm volatile("mad.hi.cc.u32 %0, %1, %2, %0;" : "+r"(d) : "r"(a), "r"(b))
+#define MADC_HI_CC(d, a, b) asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(d) : "r"(a), "r"(b))
+#define MADC_HI(d, a, b)    asm volatile("madc.hi.u32 %0, %1, %2, %0;" : "+r"(d) : "r"(a), "r"(b))
+#define ADDC_Z(d)           asm volatile("addc.u32 %0, 0, 0;" : "=r"(d))
+#define ADD_CC(d, a, b)     asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
+#define ADDC_CC(d, a, b)    asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
+#define ADDC(d, a, b)       asm volatile("addc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
+#define SUB_CC(d, a, b)     asm volatile("sub.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
+#define SUBC_CC(d, a, b)    asm volatile("subc.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
+#define SUBC(d, a, b)       asm volatile("subc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
+
+// t[0..8] += a[0..7] * b.  Requires the true sum to fit in 9 limbs.
+CSB_DEV void row_mad(uint32_t (&t)[9], const uint32_t (&a)[8], uint32_t b) {
+  MAD_LO_CC(t[0], a[0], b);  MADC_LO_CC(t[1], a[1], b); MADC_LO_CC(t[2], a[2], b);
+  MADC_LO_CC(t[3], a[3], b); MADC_LO_CC(t[4], a[4], b); MADC_LO_CC(t[5], a[5], b);
+  MADC_LO_CC(t[6], a[6], b); MADC_LO_CC(t[7], a[7], b);
+  uint32_t c; ADDC_Z(c); t[8] += c;
+  MAD_HI_CC(t[1], a[0], b);  MADC_HI_CC(t[2], a[1], b); MADC_HI_CC(t[3], a[2], b);
+  MADC_HI_CC(t[4], a[3], b); MADC_HI_CC(t[5], a[4], b); MADC_HI_CC(t[6], a[5], b);
+  MADC_HI_CC(t[7], a[6], b); MADC_HI(t[8], a[7], b);
+}
+
+template <class M>
+struct Fp {
+  uint32_t v[8];
+
+  static CSB_DEV Fp zero() { Fp r; for (int i = 0; i < 8; i++) r.v[i] = 0; return r; }
+  static CSB_DEV Fp one() {
+    return Fp{{M::ONE0, M::ONE1, M::ONE2, M::ONE3, M::ONE4, M::ONE5, M::ONE6, M::ONE7}};
+  }
+  static CSB_DEV Fp r2() { return Fp{{M::R20, M::R21, M::R22, M::R23, M::R24, M::R25, M::R26, M::R27}}; }
+
+  CSB_DEV bool is_zero() const {
+    return (v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7]) == 0;
+  }
+  CSB_DEV bool operator==(const Fp& o) const {
+    return ((v[0] ^ o.v[0]) | (v[1] ^ o.v[1]) | (v[2] ^ o.v[2]) | (v[3] ^ o.v[3]) |
+            (v[4] ^ o.v[4]) | (v[5] ^ o.v[5]) | (v[6] ^ o.v[6]) | (v[7] ^ o.v[7])) == 0;
+  }
+  CSB_DEV bool is_one() const { return *this == one(); }
+
+  // r = t - p if t >= p else t, for t < 2p (t given in 8 limbs).
+  static CSB_DEV void reduce_once(uint32_t (&t)[8]) {
+    uint32_t u[8], br;
+    SUB_CC(u[0], t[0], M::P0); SUBC_CC(u[1], t[1], M::P1); SUBC_CC(u[2], t[2], M::P2);
+    SUBC_CC(u[3], t[3], M::P3); SUBC_CC(u[4], t[4], M::P4); SUBC_CC(u[5], t[5], M::P5);
+    SUBC_CC(u[6], t[6], M::P6); SUBC_CC(u[7], t[7], M::P7); SUBC(br, 0u, 0u);
+    // br = 0xffffffff if t < p (borrow), 0 otherwise
+#pragma unroll
+    for (int i = 0; i < 8; i++) t[i] = (t[i] & br) | (u[i] & ~br);
+  }
+
+  friend CSB_DEV Fp operator+(const Fp& a, const Fp& b) {
+    uint32_t t[8];
+    ADD_CC(t[0], a.v[0], b.v[0]);  ADDC_CC(t[1], a.v[1], b.v[1]); ADDC_CC(t[2], a.v[2], b.v[2]);
+    ADDC_CC(t[3], a.v[3], b.v[3]); ADDC_CC(t[4], a.v[4], b.v[4]); ADDC_CC(t[5], a.v[5], b.v[5]);
+    ADDC_CC(t[6], a.v[6], b.v[6]); ADDC(t[7], a.v[7], b.v[7]);
+    reduce_once(t);
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = t[i];
+    return r;
+  }
+  friend CSB_DEV Fp operator-(const Fp& a, const Fp& b) {
+    uint32_t t[8], br;
+    SUB_CC(t[0], a.v[0], b.v[0]);  SUBC_CC(t[1], a.v[1], b.v[1]); SUBC_CC(t[2], a.v[2], b.v[2]);
+    SUBC_CC(t[3], a.v[3], b.v[3]); SUBC_CC(t[4], a.v[4], b.v[4]); SUBC_CC(t[5], a.v[5], b.v[5]);
+    SUBC_CC(t[6], a.v[6], b.v[6]); SUBC_CC(t[7], a.v[7], b.v[7]); SUBC(br, 0u, 0u);
+    // add p back if the subtraction borrowed
+    const uint32_t p0 = M::P0 & br, p1 = M::P1 & br, p2 = M::P2 & br, p3 = M::P3 & br;
+    const uint32_t p4 = M::P4 & br, p5 = M::P5 & br, p6 = M::P6 & br, p7 = M::P7 & br;
+    Fp r;
+    ADD_CC(r.v[0], t[0], p0);  ADDC_CC(r.v[1], t[1], p1); ADDC_CC(r.v[2], t[2], p2);
+    ADDC_CC(r.v[3], t[3], p3); ADDC_CC(r.v[4], t[4], p4); ADDC_CC(r.v[5], t[5], p5);
+    ADDC_CC(r.v[6], t[6], p6); ADDC(r.v[7], t[7], p7);
+    return r;
+  }
+  CSB_DEV Fp neg() const { return zero() - *this; }
+  CSB_DEV Fp dbl() const { return *this + *this; }
+
+  // CIOS Montgomery product.
+  friend CSB_DEV Fp operator*(const Fp& a, const Fp& b) {
+    const uint32_t (&A)[8] = a.v;
+    const uint32_t P[8] = {M::P0, M::P1, M::P2, M::P3, M::P4, M::P5, M::P6, M::P7};
+    uint32_t t[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) t[i] = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      row_mad(t, A, b.v[i]);
+      const uint32_t m = t[0] * M::NP0;
+      row_mad(t, P, m);
+      // t[0] is now zero: shift one limb down
+#pragma unroll
+      for (int j = 0; j < 8; j++) t[j] = t[j + 1];
+      t[8] = 0;
+    }
+    uint32_t r8[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) r8[i] = t[i];
+    reduce_once(r8);
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = r8[i];
+    return r;
+  }
+  CSB_DEV Fp sqr() const { return (*this) * (*this); }
+
+  // x -> x * R mod p (normal form to Montgomery); any 256-bit x < 2^256 is accepted
+  // because the CIOS bound only needs a*b < p * 2^256.
+  CSB_DEV Fp to_mont() const { return (*this) * r2(); }
+  CSB_DEV Fp from_mont() const {
+    Fp o = zero();
+    o.v[0] = 1;
+    return (*this) * o;
+  }
+
+  // a^(p-2): Fermat inverse (0 -> 0), plain square-and-multiply (rarely used: final
+  // affine conversions only).
+  CSB_DEV Fp inv() const {
+    const uint32_t E[8] = {M::P0 - 2u, M::P1, M::P2, M::P3, M::P4, M::P5, M::P6, M::P7};
+    Fp acc = one();
+#pragma unroll 1
+    for (int bit = 255; bit >= 0; bit--) {
+      acc = acc.sqr();
+      if ((E[bit >> 5] >> (bit & 31)) & 1u) acc = acc * (*this);
+    }
+    return acc;
+  }
+};
+
+using Fq = Fp<ModQ>;
+using Fr = Fp<ModR>;
+
+// ------------------------------------------------------------ Fq2 = Fq[u]/(u^2+1) ----
+struct Fq2 {
+  Fq c0, c1;
+  static CSB_DEV Fq2 zero() { return {Fq::zero(), Fq::zero()}; }
+  static CSB_DEV Fq2 one() { return {Fq::one(), Fq::zero()}; }
+  CSB_DEV bool is_zero() const { return c0.is_zero() && c1.is_zero(); }
+  CSB_DEV bool operator==(const Fq2& o) const { return c0 == o.c0 && c1 == o.c1; }
+  friend CSB_DEV Fq2 operator+(const Fq2& a, const Fq2& b) { return {a.c0 + b.c0, a.c1 + b.c1}; }
+  friend CSB_DEV Fq2 operator-(const Fq2& a, const Fq2& b) { return {a.c0 - b.c0, a.c1 - b.c1}; }
+  // Karatsuba, 3 products (src/cuda/ff.cpp montmult_ext_h: same non-residue -1)
+  friend CSB_DEV Fq2 operator*(const Fq2& a, const Fq2& b) {
+    const Fq v0 = a.c0 * b.c0;
+    const Fq v1 = a.c1 * b.c1;
+    const Fq s = (a.c0 + a.c1) * (b.c0 + b.c1);
+    return {v0 - v1, s - v0 - v1};
+  }
+  // (a0 + a1 u)^2 = (a0 + a1)(a0 - a1) + 2 a0 a1 u
+  CSB_DEV Fq2 sqr() const {
+    const Fq p = c0 * c1;
+    return {(c0 + c1) * (c0 - c1), p + p};
+  }
+  CSB_DEV Fq2 neg() const { return {c0.neg(), c1.neg()}; }
+  CSB_DEV Fq2 dbl() const { return {c0.dbl(), c1.dbl()}; }
+  CSB_DEV Fq2 inv() const {
+    const Fq d = (c0.sqr() + c1.sqr()).inv();
+    return {c0 * d, (c1 * d).neg()};
+  }
+};
+
+}  // namespace csb

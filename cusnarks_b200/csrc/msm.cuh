@@ -1,0 +1,52 @@
+// msm.cuh -- Pippenger multi-scalar multiplication for BN254 G1/G2 on sm_100a.
+//
+// Replaces the reference's GPU multi-exp (src/cuda/ecbn128_device.cu:508
+// madecjac_shfl_kernel + :567 redecjac_kernel, per-thread Shamir tables and a shuffle
+// tree) and produces the value of its CPU multi-exp ec_jacreduce_server_h
+// (src/cuda/ec.cpp:1536): sum_i k_i * P_i as an affine Montgomery point.
+//
+// Pipeline for one instance of N terms, window width c, W = floor(254/c) + 1 windows,
+// B = 2^(c-1) buckets per window:
+//   1. digits:   each scalar (any 256-bit value) is reduced mod r and recoded into W
+//                signed c-bit digits d in (-2^(c-1), 2^(c-1)]; every nonzero digit adds
+//                one to the count of bucket (window, |d|-1).  Zero scalars and points at
+//                infinity produce no entries.
+//   2. scan:     exclusive prefix sum of the W*B counts -> bucket offsets.
+//   3. scatter:  digits are recomputed and (point index | sign) is written into the slot
+//                of its bucket: a counting sort of the N*W (bucket, point) pairs.
+//   4. accumulate: buckets are summed with mixed XYZZ + affine additions.  Buckets are
+//                split into tasks of at most TASK points; tasks run longest first so
+//                warps see similar trip counts.  Partial sums of split buckets are added
+//                back together by a second pass.
+//   5. reduce:   per window, sum_b (b+1) * bucket_b by hierarchical running sums over
+//                segments of 8 buckets (level k leaves sum_i i*y_i with weight 8^k and
+//                the segment total for the next level).
+//   6. finish:   level results are combined with 3-bit Horner steps, windows with c-bit
+//                Horner steps, and the result is converted to affine.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+
+namespace csb {
+
+struct MsmConfig {
+  int c = 0;          // window bits; 0 = pick from N
+  int task = 64;      // max points per accumulation task
+};
+
+// Bytes of device scratch one MSM of n terms needs (G2 when ec2).
+size_t msm_workspace_bytes(uint32_t n, int c, bool ec2);
+int msm_default_window(uint32_t n, bool ec2);
+
+// d_scalars: n x 8 words (normal form), d_points: n affine points (16 or 32 words),
+// d_out: one affine point (16 or 32 words), d_work: msm_workspace_bytes() bytes,
+// 256-byte aligned.  Everything runs on `stream`; nothing is allocated.
+cudaError_t msm_g1(const uint32_t* d_scalars, const uint32_t* d_points, uint32_t n,
+                   uint32_t* d_out, void* d_work, size_t work_bytes, const MsmConfig& cfg,
+                   cudaStream_t stream);
+cudaError_t msm_g2(const uint32_t* d_scalars, const uint32_t* d_points, uint32_t n,
+                   uint32_t* d_out, void* d_work, size_t work_bytes, const MsmConfig& cfg,
+                   cudaStream_t stream);
+
+}  // namespace csb

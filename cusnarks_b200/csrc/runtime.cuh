@@ -1,0 +1,80 @@
+// runtime.cuh -- per-context device state for the C ABI: stream, scratch arena, staging
+// buffers, timing events and the last error message.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+namespace csb {
+
+// Grow-only device buffer (256-byte aligned).  Growing synchronises the owning stream
+// first so no in-flight kernel still uses the old block.
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  cudaError_t reserve(size_t need, cudaStream_t st) {
+    if (need <= bytes) return cudaSuccess;
+    if (ptr) {
+      cudaError_t e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) return e;
+      cudaFree(ptr);
+      ptr = nullptr;
+      bytes = 0;
+    }
+    size_t sz = need + need / 8;  // headroom for slightly larger calls
+    cudaError_t e = cudaMalloc(&ptr, sz);
+    if (e != cudaSuccess) { ptr = nullptr; return e; }
+    bytes = sz;
+    return cudaSuccess;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+};
+
+struct PinnedBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  cudaError_t reserve(size_t need) {
+    if (need <= bytes) return cudaSuccess;
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMallocHost(&ptr, need);
+    if (e != cudaSuccess) { ptr = nullptr; return e; }
+    bytes = need;
+    return cudaSuccess;
+  }
+  void release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+};
+
+}  // namespace csb
+
+// The opaque context behind cs_ctx_t in the C header.
+struct cs_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  csb::DeviceBuffer work;      // kernel scratch
+  csb::DeviceBuffer in;        // device copies of host inputs
+  csb::DeviceBuffer out;       // device results
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  float last_ms = 0.f;
+  std::string err;
+  std::mutex mu;               // one call at a time per context
+};
+
+namespace csb {
+// Records a CUDA error on the context and maps it to the C ABI status code.
+int fail(cs_ctx* ctx, cudaError_t e, const char* where);
+int fail_msg(cs_ctx* ctx, int code, const std::string& msg);
+}  // namespace csb
