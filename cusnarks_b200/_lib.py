@@ -29,6 +29,15 @@ class CsError(RuntimeError):
         self.code = code
 
 
+class InterpolAndMul(ctypes.Structure):
+    """ntt_interpolandmul_t (reference src/cuda/types.h:530-546)."""
+    _fields_ = [("A", _vp), ("B", _vp), ("roots", _vp), ("Nrows", ctypes.c_uint32),
+                ("Ncols", ctypes.c_uint32), ("mNrows", ctypes.c_uint32), ("mNcols", ctypes.c_uint32),
+                ("nroots", ctypes.c_uint32), ("rstride", ctypes.c_uint32), ("pidx", ctypes.c_uint32),
+                ("max_threads", ctypes.c_uint32), ("start_idx", ctypes.c_uint32),
+                ("last_idx", ctypes.c_uint32), ("thread_id", ctypes.c_uint32)]
+
+
 class JacaddReduced(ctypes.Structure):
     """jacadd_reduced_t (reference src/cuda/types.h:548-567)."""
     _fields_ = [("out_ep", _vp), ("scl", _vp), ("x", _vp), ("n", ctypes.c_uint32),
@@ -49,11 +58,36 @@ _SIGNATURES = [
     ("cs_ctx_sync", ctypes.c_int, [_vp]),
     ("cs_ctx_error", ctypes.c_char_p, [_vp]),
     ("cs_ctx_last_ms", ctypes.c_float, [_vp]),
+    ("cs_ctx_last_phase_ms", ctypes.c_float, [_vp]),
     ("cs_last_status", ctypes.c_int, []),
     ("cs_last_error", ctypes.c_char_p, []),
     ("cs_msm", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp, ctypes.c_int]),
     ("cs_msm_device", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp, ctypes.c_int]),
     ("cs_msm_workspace_bytes", ctypes.c_size_t, [ctypes.c_uint32, ctypes.c_int, ctypes.c_int]),
+    ("cs_msm_default_window", ctypes.c_int, [ctypes.c_uint32, ctypes.c_int]),
+    ("cs_msm_num_windows", ctypes.c_int, [ctypes.c_int]),
+    ("cs_scmul_device", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, ctypes.c_uint32, _vp]),
+    ("cs_bench_imad_peak", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    ("cs_bench_pipe", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    ("cs_bench_mulmod", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    ("cs_kernel_launches", ctypes.c_ulonglong, []),
+    ("cs_field_op_device", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_uint32]),
+    ("cs_field_last_status", ctypes.c_int, []),
+    ("montmult_h", None, [_vp, _vp, _vp, ctypes.c_uint32]),
+    ("montsquare_h", None, [_vp, _vp, ctypes.c_uint32]),
+    ("addm_h", None, [_vp, _vp, _vp, ctypes.c_uint32]),
+    ("subm_h", None, [_vp, _vp, _vp, ctypes.c_uint32]),
+    ("montinv_h", None, [_vp, _vp, ctypes.c_uint32]),
+    ("to_montgomeryN_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32]),
+    ("from_montgomeryN_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ntt_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int32, ctypes.c_uint32]),
+    ("intt_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_ulonglong, ctypes.c_uint32]),
+    ("find_roots_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ntt_interpolandmul_server_h", ctypes.POINTER(ctypes.c_uint32), [_vp]),
+    ("get_Mtranspose_h", ctypes.POINTER(ctypes.c_uint32), []),
+    ("cs_ntt_last_status", ctypes.c_int, []),
+    ("cs_ntt_device", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint32, ctypes.c_int, ctypes.c_int]),
+    ("cs_hstep_device", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, ctypes.c_uint32, _vp]),
     ("ec_jacreduce_server_h", None, [ctypes.POINTER(JacaddReduced)]),
     ("ec2_jacreduce_server_h", None, [ctypes.POINTER(JacaddReduced)]),
 ]

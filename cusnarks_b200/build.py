@@ -11,6 +11,7 @@ from __future__ import annotations
 import argparse
 import concurrent.futures as cf
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -37,15 +38,27 @@ def sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
 
 
-def headers():
-    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    hs.append(os.path.join(ROOT, "include", "cusnarks_b200.h"))
-    return hs
+_INC = re.compile(r'^\s*#\s*include\s*"([^"]+)"', re.M)
+
+
+def deps(path: str, seen=None) -> set:
+    """Transitive closure of the quoted #includes of a source file."""
+    seen = set() if seen is None else seen
+    try:
+        text = open(path).read()
+    except OSError:
+        return seen
+    for inc in _INC.findall(text):
+        p = os.path.normpath(os.path.join(os.path.dirname(path), inc))
+        if p not in seen and os.path.exists(p):
+            seen.add(p)
+            deps(p, seen)
+    return seen
 
 
 def _compile(src: str, verbose: bool) -> str:
     obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
-    newest_dep = max([os.path.getmtime(src)] + [os.path.getmtime(h) for h in headers()])
+    newest_dep = max([os.path.getmtime(src)] + [os.path.getmtime(h) for h in deps(src)])
     if os.path.exists(obj) and os.path.getmtime(obj) >= newest_dep:
         return obj
     cmd = [nvcc(), *GENCODE, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]

@@ -58,6 +58,11 @@ class Context:
     def last_ms(self) -> float:
         return float(self._lib.cs_ctx_last_ms(self.handle))
 
+    @property
+    def last_phase_ms(self) -> float:
+        """Device ms of the bucket-accumulation kernels of the last MSM."""
+        return float(self._lib.cs_ctx_last_phase_ms(self.handle))
+
     # ------------------------------------------------------------------------ MSM ----
     def msm(self, scalars, points, ec2: bool = False, window: int = 0) -> np.ndarray:
         """sum_i scalars[i] * points[i]; affine Montgomery result (16 or 32 words)."""
@@ -80,3 +85,42 @@ class Context:
     @staticmethod
     def msm_workspace_bytes(n: int, ec2: bool = False, window: int = 0) -> int:
         return int(lib().cs_msm_workspace_bytes(n, int(bool(ec2)), window))
+
+    # -------------------------------------------------------------- field ops -----
+    FOP = {"mul": 0, "add": 1, "sub": 2, "sqr": 3, "inv": 4, "to_mont": 5, "from_mont": 6,
+           "mul_lohi": 7, "fq2_mul": 8}
+
+    def field_op_device(self, op: str, pidx: int, d_a: int, d_b: int, d_out: int, n: int):
+        check(self._lib.cs_field_op_device(self.handle, self.FOP[op], pidx, ctypes.c_void_p(d_a),
+                                           ctypes.c_void_p(d_b or 0), ctypes.c_void_p(d_out), n),
+              self.handle)
+
+    # ------------------------------------------------------------ transforms ------
+    def ntt_device(self, d_in: int, d_out: int, log_n: int, direction: int = 1, fmat: int = 1):
+        check(self._lib.cs_ntt_device(self.handle, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out),
+                                      log_n, direction, fmat), self.handle)
+
+    def hstep_device(self, variant: int, d_a: int, d_b: int, d_c: int, log_m: int, d_out: int):
+        """variant 0: reference (2m coefficients of A*B); 1: coset quotient (m coefficients)."""
+        check(self._lib.cs_hstep_device(self.handle, variant, ctypes.c_void_p(d_a), ctypes.c_void_p(d_b),
+                                        ctypes.c_void_p(d_c or 0), log_m, ctypes.c_void_p(d_out)),
+              self.handle)
+
+    # ------------------------------------------------------------- scalar mult ----
+    def scmul_device(self, d_scalars: int, d_points: int, n: int, d_out: int, ec2: bool = False,
+                     point_stride_words: int | None = None):
+        """out[i] = scalars[i] * points[i]; point_stride_words=0 for one shared base."""
+        if point_stride_words is None:
+            point_stride_words = 32 if ec2 else 16
+        check(self._lib.cs_scmul_device(self.handle, int(bool(ec2)), ctypes.c_void_p(d_scalars),
+                                        ctypes.c_void_p(d_points), point_stride_words, n,
+                                        ctypes.c_void_p(d_out)), self.handle)
+
+    def imad_peak(self) -> float:
+        v = ctypes.c_double()
+        check(self._lib.cs_bench_imad_peak(self.handle, ctypes.byref(v)), self.handle)
+        return float(v.value)
+
+
+def kernel_launches() -> int:
+    return int(lib().cs_kernel_launches())

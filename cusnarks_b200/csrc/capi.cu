@@ -1,13 +1,19 @@
 // capi.cu -- extern "C" entry points (include/cusnarks_b200.h).
+#include <atomic>
 #include <cstring>
 #include <memory>
 #include <string>
 
 #include "../../include/cusnarks_b200.h"
+#include "ecops.cuh"
 #include "msm.cuh"
 #include "runtime.cuh"
 
 namespace csb {
+
+void domain_release(cs_ctx* ctx);  // hstep.cu
+static std::atomic<unsigned long long> g_launches{0};
+void note_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int fail(cs_ctx* ctx, cudaError_t e, const char* where) {
   if (ctx) ctx->err = std::string(where) + ": " + cudaGetErrorString(e);
@@ -76,6 +82,9 @@ int msm_device_locked(cs_ctx* ctx, int ec2, const uint32_t* s, const uint32_t* p
   if (e != cudaSuccess) return fail(ctx, e, "msm workspace");
   csb::MsmConfig cfg;
   cfg.c = window;
+  cfg.acc_start = ctx->ev_phase0;
+  cfg.acc_stop = ctx->ev_phase1;
+  ctx->phase_valid = true;
   EventScope ev(ctx);
   e = ec2 ? csb::msm_g2(s, p, n, out, ctx->work.ptr, ctx->work.bytes, cfg, ctx->stream)
           : csb::msm_g1(s, p, n, out, ctx->work.ptr, ctx->work.bytes, cfg, ctx->stream);
@@ -105,6 +114,8 @@ int cs_ctx_create(int device, cs_ctx** out) {
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev_start);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev_stop);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev_phase0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev_phase1);
   cudaSetDevice(prev);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -118,11 +129,14 @@ int cs_ctx_create(int device, cs_ctx** out) {
 void cs_ctx_destroy(cs_ctx* ctx) {
   if (!ctx) return;
   cudaStreamSynchronize(ctx->stream);
+  csb::domain_release(ctx);
   ctx->work.release();
   ctx->in.release();
   ctx->out.release();
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
   if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+  if (ctx->ev_phase0) cudaEventDestroy(ctx->ev_phase0);
+  if (ctx->ev_phase1) cudaEventDestroy(ctx->ev_phase1);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -147,16 +161,23 @@ int cs_ctx_sync(cs_ctx* ctx) {
   if (e != cudaSuccess) return fail(ctx, e, "stream sync");
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
+  if (ctx->phase_valid && cudaEventElapsedTime(&ms, ctx->ev_phase0, ctx->ev_phase1) == cudaSuccess)
+    ctx->last_phase_ms = ms;
+  ctx->phase_valid = false;
   cudaGetLastError();
   return CS_OK;
 }
 
 const char* cs_ctx_error(cs_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 float cs_ctx_last_ms(cs_ctx* ctx) { return ctx ? ctx->last_ms : 0.f; }
+float cs_ctx_last_phase_ms(cs_ctx* ctx) { return ctx ? ctx->last_phase_ms : 0.f; }
 
 size_t cs_msm_workspace_bytes(uint32_t n, int ec2, int window) {
   return csb::msm_workspace_bytes(n, window, ec2 != 0);
 }
+
+int cs_msm_default_window(uint32_t n, int ec2) { return csb::msm_default_window(n, ec2 != 0); }
+int cs_msm_num_windows(int window) { return window > 0 ? 254 / window + 1 : 0; }
 
 int cs_msm_device(cs_ctx* ctx, int ec2, const uint32_t* d_scalars, const uint32_t* d_points,
                   uint32_t n, uint32_t* d_out, int window) {
@@ -194,11 +215,27 @@ int cs_msm(cs_ctx* ctx, int ec2, const uint32_t* scalars, const uint32_t* points
   if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(ctx, e, "msm sync");
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
+  if (cudaEventElapsedTime(&ms, ctx->ev_phase0, ctx->ev_phase1) == cudaSuccess) ctx->last_phase_ms = ms;
+  ctx->phase_valid = false;
+  return CS_OK;
+}
+
+int cs_scmul_device(cs_ctx* ctx, int ec2, const uint32_t* d_scalars, const uint32_t* d_points,
+                    uint32_t stride, uint32_t n, uint32_t* d_out) {
+  if (!ctx || (n && (!d_scalars || !d_points || !d_out))) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  EventScope ev(ctx);
+  cudaError_t e = ec2 ? csb::scmul_g2(d_scalars, d_points, stride, n, d_out, ctx->stream)
+                      : csb::scmul_g1(d_scalars, d_points, stride, n, d_out, ctx->stream);
+  ev.stop();
+  if (e != cudaSuccess) return fail(ctx, e, "scmul launch");
   return CS_OK;
 }
 
 // ------------------------------------------------------------ drop-in entry points ---
 int cs_last_status(void) { return t_status; }
+unsigned long long cs_kernel_launches(void) { return csb::g_launches.load(); }
 const char* cs_last_error(void) { return t_error.c_str(); }
 
 void ec_jacreduce_server_h(jacadd_reduced_t* args) {

@@ -117,6 +117,14 @@ CSB_DEV XYZZ<F> xyzz_add(const XYZZ<F>& p, const XYZZ<F>& q) {
   return r;
 }
 
+// Out-of-line copies for kernels whose cost is latency, not throughput (bucket-sum
+// scans, window combination): one body per kernel instead of one per call site keeps
+// code size and compile time in check, notably over Fq2.
+template <class F>
+__device__ __noinline__ XYZZ<F> xyzz_add_cold(const XYZZ<F> p, const XYZZ<F> q) { return xyzz_add(p, q); }
+template <class F>
+__device__ __noinline__ XYZZ<F> xyzz_dbl_cold(const XYZZ<F> p) { return xyzz_dbl(p); }
+
 template <class F>
 CSB_DEV XYZZ<F> xyzz_neg(const XYZZ<F>& p) {
   XYZZ<F> r = p;

@@ -24,6 +24,8 @@ struct ModQ {  // base field q (the reference's MOD_GROUP, pidx 0)
                             ONE4 = 0x7879462cu, ONE5 = 0x666ea36fu, ONE6 = 0x9a07df2fu, ONE7 = 0x0e0a77c1u;
   static constexpr uint32_t R20 = 0x538afa89u, R21 = 0xf32cfc5bu, R22 = 0xd44501fbu, R23 = 0xb5e71911u,
                             R24 = 0x0a417ff6u, R25 = 0x47ab1effu, R26 = 0xcab8351fu, R27 = 0x06d89f71u;
+  static constexpr uint32_t R30 = 0xda1530dfu, R31 = 0xb1cd6dafu, R32 = 0xa7283db6u, R33 = 0x62f210e6u,
+                            R34 = 0x0ada0afbu, R35 = 0xef7f0b0cu, R36 = 0x2d592544u, R37 = 0x20fd6e90u;
 };
 struct ModR {  // scalar field r (the reference's MOD_FIELD, pidx 1)
   static constexpr uint32_t P0 = 0xf0000001u, P1 = 0x43e1f593u, P2 = 0x79b97091u, P3 = 0x2833e848u,
@@ -33,6 +35,8 @@ struct ModR {  // scalar field r (the reference's MOD_FIELD, pidx 1)
                             ONE4 = 0x7879462eu, ONE5 = 0x666ea36fu, ONE6 = 0x9a07df2fu, ONE7 = 0x0e0a77c1u;
   static constexpr uint32_t R20 = 0xae216da7u, R21 = 0x1bb8e645u, R22 = 0xe35c59e3u, R23 = 0x53fe3ab1u,
                             R24 = 0x53bb8085u, R25 = 0x8c49833du, R26 = 0x7f4e44a5u, R27 = 0x0216d0b1u;
+  static constexpr uint32_t R30 = 0xb4bf0040u, R31 = 0x5e94d8e1u, R32 = 0x1cfbb6b8u, R33 = 0x2a489cbeu,
+                            R34 = 0xa19fcfedu, R35 = 0x893cc664u, R36 = 0x7fcc657cu, R37 = 0x0cf8594bu;
 };
 
 // ------------------------------------------------------------ carry-chain helpers ----
@@ -62,6 +66,38 @@ CSB_DEV void row_mad(uint32_t (&t)[9], const uint32_t (&a)[8], uint32_t b) {
   MADC_HI_CC(t[7], a[6], b); MADC_HI(t[8], a[7], b);
 }
 
+// t[0..8] += a[0..7] * b using 32x32->64 wide products (IMAD.WIDE): the even-index
+// products a0b, a2b, a4b, a6b tile limbs 0..7 without overlap and the odd ones tile
+// limbs 1..8, so each half is a ready 8-limb addend; two add.cc chains fold them in.
+// Requires the true sum to fit in 9 limbs.
+CSB_DEV void row_mad_wide(uint32_t (&t)[9], const uint32_t (&a)[8], uint32_t b) {
+  asm volatile(
+      "{\n\t.reg .b64 p;\n\t.reg .u32 lo, hi;\n\t"
+      // even products: limbs 0..7, carry into t8
+      "mul.wide.u32 p, %9, %17;\n\tmov.b64 {lo, hi}, p;\n\t"
+      "add.cc.u32 %0, %0, lo;\n\taddc.cc.u32 %1, %1, hi;\n\t"
+      "mul.wide.u32 p, %11, %17;\n\tmov.b64 {lo, hi}, p;\n\t"
+      "addc.cc.u32 %2, %2, lo;\n\taddc.cc.u32 %3, %3, hi;\n\t"
+      "mul.wide.u32 p, %13, %17;\n\tmov.b64 {lo, hi}, p;\n\t"
+      "addc.cc.u32 %4, %4, lo;\n\taddc.cc.u32 %5, %5, hi;\n\t"
+      "mul.wide.u32 p, %15, %17;\n\tmov.b64 {lo, hi}, p;\n\t"
+      "addc.cc.u32 %6, %6, lo;\n\taddc.cc.u32 %7, %7, hi;\n\t"
+      "addc.u32 %8, %8, 0;\n\t"
+      // odd products: limbs 1..8
+      "mul.wide.u32 p, %10, %17;\n\tmov.b64 {lo, hi}, p;\n\t"
+      "add.cc.u32 %1, %1, lo;\n\taddc.cc.u32 %2, %2, hi;\n\t"
+      "mul.wide.u32 p, %12, %17;\n\tmov.b64 {lo, hi}, p;\n\t"
+      "addc.cc.u32 %3, %3, lo;\n\taddc.cc.u32 %4, %4, hi;\n\t"
+      "mul.wide.u32 p, %14, %17;\n\tmov.b64 {lo, hi}, p;\n\t"
+      "addc.cc.u32 %5, %5, lo;\n\taddc.cc.u32 %6, %6, hi;\n\t"
+      "mul.wide.u32 p, %16, %17;\n\tmov.b64 {lo, hi}, p;\n\t"
+      "addc.cc.u32 %7, %7, lo;\n\taddc.u32 %8, %8, hi;\n\t}"
+      : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]),
+        "+r"(t[7]), "+r"(t[8])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
+        "r"(b));
+}
+
 template <class M>
 struct Fp {
   uint32_t v[8];
@@ -71,6 +107,7 @@ struct Fp {
     return Fp{{M::ONE0, M::ONE1, M::ONE2, M::ONE3, M::ONE4, M::ONE5, M::ONE6, M::ONE7}};
   }
   static CSB_DEV Fp r2() { return Fp{{M::R20, M::R21, M::R22, M::R23, M::R24, M::R25, M::R26, M::R27}}; }
+  static CSB_DEV Fp r3() { return Fp{{M::R30, M::R31, M::R32, M::R33, M::R34, M::R35, M::R36, M::R37}}; }
 
   CSB_DEV bool is_zero() const {
     return (v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7]) == 0;
@@ -120,8 +157,42 @@ struct Fp {
   CSB_DEV Fp neg() const { return zero() - *this; }
   CSB_DEV Fp dbl() const { return *this + *this; }
 
-  // CIOS Montgomery product.
+  // CIOS Montgomery product with wide (IMAD.WIDE) row products.
+  static CSB_DEV Fp mul_wide(const Fp& a, const Fp& b) {
+    const uint32_t (&A)[8] = a.v;
+    const uint32_t P[8] = {M::P0, M::P1, M::P2, M::P3, M::P4, M::P5, M::P6, M::P7};
+    uint32_t t[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) t[i] = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      row_mad_wide(t, A, b.v[i]);
+      const uint32_t m = t[0] * M::NP0;
+      row_mad_wide(t, P, m);
+#pragma unroll
+      for (int j = 0; j < 8; j++) t[j] = t[j + 1];
+      t[8] = 0;
+    }
+    uint32_t r8[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) r8[i] = t[i];
+    reduce_once(r8);
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = r8[i];
+    return r;
+  }
+
   friend CSB_DEV Fp operator*(const Fp& a, const Fp& b) {
+#ifdef CSB_MUL_LOHI
+    return mul_lohi(a, b);
+#else
+    return mul_wide(a, b);
+#endif
+  }
+
+  // CIOS Montgomery product with mad.lo / mad.hi carry chains.
+  static CSB_DEV Fp mul_lohi(const Fp& a, const Fp& b) {
     const uint32_t (&A)[8] = a.v;
     const uint32_t P[8] = {M::P0, M::P1, M::P2, M::P3, M::P4, M::P5, M::P6, M::P7};
     uint32_t t[9];
@@ -157,18 +228,81 @@ struct Fp {
     return (*this) * o;
   }
 
-  // a^(p-2): Fermat inverse (0 -> 0), plain square-and-multiply (rarely used: final
-  // affine conversions only).
+  // Montgomery inverse (aR -> a^-1 R; 0 -> 0).  Binary extended Euclid on the integer
+  // x = aR gives x^-1 = a^-1 R^-1; one Montgomery product by R^3 restores a^-1 R.  Used
+  // for the few final affine conversions, where a single thread's latency is what counts.
   CSB_DEV Fp inv() const {
-    const uint32_t E[8] = {M::P0 - 2u, M::P1, M::P2, M::P3, M::P4, M::P5, M::P6, M::P7};
-    Fp acc = one();
+    if (is_zero()) return zero();
+    const uint32_t P[8] = {M::P0, M::P1, M::P2, M::P3, M::P4, M::P5, M::P6, M::P7};
+    uint32_t u[8], v[8], x1[8], x2[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) { u[i] = this->v[i]; v[i] = P[i]; x1[i] = 0; x2[i] = 0; }
+    x1[0] = 1;
 #pragma unroll 1
-    for (int bit = 255; bit >= 0; bit--) {
-      acc = acc.sqr();
-      if ((E[bit >> 5] >> (bit & 31)) & 1u) acc = acc * (*this);
+    for (int guard = 0; guard < 2048; guard++) {
+      const bool u1 = (u[0] == 1) && ((u[1] | u[2] | u[3] | u[4] | u[5] | u[6] | u[7]) == 0);
+      const bool v1 = (v[0] == 1) && ((v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7]) == 0);
+      if (u1 || v1) break;
+      // (a zero u or v only arises from an unreduced input; the bounded loops end anyway)
+#pragma unroll 1
+      for (int k = 0; k < 256 && (u[0] & 1u) == 0; k++) { shr1(u); half_mod(x1, P); }
+#pragma unroll 1
+      for (int k = 0; k < 256 && (v[0] & 1u) == 0; k++) { shr1(v); half_mod(x2, P); }
+      if (geq(u, v)) { sub8(u, v); sub_mod(x1, x2, P); }
+      else { sub8(v, u); sub_mod(x2, x1, P); }
     }
-    return acc;
+    const bool u1 = (u[0] == 1) && ((u[1] | u[2] | u[3] | u[4] | u[5] | u[6] | u[7]) == 0);
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = u1 ? x1[i] : x2[i];
+    return r * r3();
   }
+
+ private:
+  static CSB_DEV void shr1(uint32_t (&a)[8]) {
+#pragma unroll
+    for (int i = 0; i < 7; i++) a[i] = (a[i] >> 1) | (a[i + 1] << 31);
+    a[7] >>= 1;
+  }
+  static CSB_DEV bool geq(const uint32_t (&a)[8], const uint32_t (&b)[8]) {
+#pragma unroll
+    for (int i = 7; i >= 0; i--) {
+      if (a[i] != b[i]) return a[i] > b[i];
+    }
+    return true;
+  }
+  static CSB_DEV void sub8(uint32_t (&a)[8], const uint32_t (&b)[8]) {
+    SUB_CC(a[0], a[0], b[0]); SUBC_CC(a[1], a[1], b[1]); SUBC_CC(a[2], a[2], b[2]);
+    SUBC_CC(a[3], a[3], b[3]); SUBC_CC(a[4], a[4], b[4]); SUBC_CC(a[5], a[5], b[5]);
+    SUBC_CC(a[6], a[6], b[6]); SUBC(a[7], a[7], b[7]);
+  }
+  // x <- x/2 mod p for x < p
+  static CSB_DEV void half_mod(uint32_t (&x)[8], const uint32_t (&P)[8]) {
+    if (x[0] & 1u) {
+      uint32_t c;
+      ADD_CC(x[0], x[0], P[0]); ADDC_CC(x[1], x[1], P[1]); ADDC_CC(x[2], x[2], P[2]);
+      ADDC_CC(x[3], x[3], P[3]); ADDC_CC(x[4], x[4], P[4]); ADDC_CC(x[5], x[5], P[5]);
+      ADDC_CC(x[6], x[6], P[6]); ADDC_CC(x[7], x[7], P[7]); ADDC(c, 0u, 0u);
+      shr1(x);
+      x[7] |= c << 31;
+    } else {
+      shr1(x);
+    }
+  }
+  // x <- x - y mod p for x, y < p
+  static CSB_DEV void sub_mod(uint32_t (&x)[8], const uint32_t (&y)[8], const uint32_t (&P)[8]) {
+    uint32_t br;
+    SUB_CC(x[0], x[0], y[0]); SUBC_CC(x[1], x[1], y[1]); SUBC_CC(x[2], x[2], y[2]);
+    SUBC_CC(x[3], x[3], y[3]); SUBC_CC(x[4], x[4], y[4]); SUBC_CC(x[5], x[5], y[5]);
+    SUBC_CC(x[6], x[6], y[6]); SUBC_CC(x[7], x[7], y[7]); SUBC(br, 0u, 0u);
+    if (br) {
+      ADD_CC(x[0], x[0], P[0]); ADDC_CC(x[1], x[1], P[1]); ADDC_CC(x[2], x[2], P[2]);
+      ADDC_CC(x[3], x[3], P[3]); ADDC_CC(x[4], x[4], P[4]); ADDC_CC(x[5], x[5], P[5]);
+      ADDC_CC(x[6], x[6], P[6]); ADDC(x[7], x[7], P[7]);
+    }
+  }
+
+ public:
 };
 
 using Fq = Fp<ModQ>;

@@ -33,6 +33,8 @@ namespace csb {
 struct MsmConfig {
   int c = 0;          // window bits; 0 = pick from N
   int task = 64;      // max points per accumulation task
+  // optional events recorded around the bucket-accumulation kernels (phase timing)
+  cudaEvent_t acc_start = nullptr, acc_stop = nullptr;
 };
 
 // Bytes of device scratch one MSM of n terms needs (G2 when ec2).

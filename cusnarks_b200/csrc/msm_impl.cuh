@@ -4,6 +4,7 @@
 #include "msm.cuh"
 #include "curve.cuh"
 #include "scan.cuh"
+#include "runtime.cuh"
 
 namespace csb {
 namespace msm_detail {
@@ -117,48 +118,86 @@ struct Multi {
   uint32_t bucket, pbase, count, pad;
 };
 
-// One thread per bucket: emit its tasks; empty buckets are set to infinity here.
+// Task lengths are in [1, TASK]; tasks are emitted in descending length (a counting sort
+// over TASK+1 bins) so the 32 lanes of a warp walk buckets of nearly equal size.
+constexpr int kMaxTask = 64;
+
+// Pass 1: per bucket, histogram of its task lengths; empty buckets become infinity.
 template <class F>
-__global__ void k_tasks(const uint32_t* __restrict__ offsets, uint32_t nb, uint32_t task_len,
-                        Task* __restrict__ tasks, uint32_t* __restrict__ counters,
-                        Multi* __restrict__ multi, uint32_t* __restrict__ buckets) {
+__global__ void k_task_hist(const uint32_t* __restrict__ offsets, uint32_t nb, uint32_t task_len,
+                            uint32_t* __restrict__ hist, uint32_t* __restrict__ buckets) {
+  __shared__ uint32_t sh[kMaxTask + 1];
+  for (int i = threadIdx.x; i <= kMaxTask; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t lane = threadIdx.x & 31;
-  uint32_t start = 0, cnt = 0, nt = 0;
+  if (b < nb) {
+    const uint32_t cnt = offsets[b + 1] - offsets[b];
+    if (cnt == 0) {
+      constexpr int XW = 4 * FieldWords<F>::value;
+      st_xyzz<F>(buckets + (size_t)b * XW, XYZZ<F>::inf());
+    } else {
+      const uint32_t nfull = (cnt - 1) / task_len;
+      if (nfull) atomicAdd(&sh[task_len], nfull);
+      atomicAdd(&sh[cnt - nfull * task_len], 1u);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i <= kMaxTask; i += blockDim.x)
+    if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+// Bin cursors in descending length order; counters[0] = number of tasks.
+static __global__ void k_task_bins(const uint32_t* __restrict__ hist, uint32_t task_len,
+                            uint32_t* __restrict__ cursor, uint32_t* __restrict__ counters) {
+  if (threadIdx.x != 0) return;
+  uint32_t run = 0;
+  for (int l = (int)task_len; l >= 1; l--) {
+    cursor[l] = run;
+    run += hist[l];
+  }
+  counters[0] = run;
+}
+
+// Pass 2: emit task records at their sorted positions.  Each block reserves a range per
+// length bin with one global atomic, then ranks its tasks inside it.
+template <class F>
+__global__ void k_task_emit(const uint32_t* __restrict__ offsets, uint32_t nb, uint32_t task_len,
+                            uint32_t* __restrict__ cursor, Task* __restrict__ tasks,
+                            uint32_t* __restrict__ counters, Multi* __restrict__ multi) {
+  __shared__ uint32_t cnt_s[kMaxTask + 1], base_s[kMaxTask + 1];
+  for (int i = threadIdx.x; i <= kMaxTask; i += blockDim.x) cnt_s[i] = 0;
+  __syncthreads();
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t start = 0, cnt = 0, nfull = 0, last = 0;
   if (b < nb) {
     start = offsets[b];
     cnt = offsets[b + 1] - start;
-    nt = (cnt + task_len - 1) / task_len;
+    if (cnt) {
+      nfull = (cnt - 1) / task_len;
+      last = cnt - nfull * task_len;
+      if (nfull) atomicAdd(&cnt_s[task_len], nfull);
+      atomicAdd(&cnt_s[last], 1u);
+    }
   }
-  // warp-aggregated slot allocation for tasks
-  uint32_t incl = nt;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
-    if (lane >= (uint32_t)d) incl += v;
+  __syncthreads();
+  for (int i = threadIdx.x; i <= kMaxTask; i += blockDim.x)
+    base_s[i] = cnt_s[i] ? atomicAdd(&cursor[i], cnt_s[i]) : 0u;
+  __syncthreads();
+  for (int i = threadIdx.x; i <= kMaxTask; i += blockDim.x) cnt_s[i] = 0;
+  __syncthreads();
+  if (cnt == 0) return;
+  const uint32_t nt = nfull + 1;
+  uint32_t pbase = 0;
+  if (nt > 1) {
+    pbase = atomicAdd(&counters[1], nt);
+    const uint32_t mslot = atomicAdd(&counters[2], 1u);
+    multi[mslot] = {b, pbase, nt, 0u};
   }
-  const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-  uint32_t base = 0;
-  if (lane == 31 && total) base = atomicAdd(&counters[0], total);
-  base = __shfl_sync(0xffffffffu, base, 31);
-  if (b >= nb) return;
-  uint32_t slot = base + incl - nt;
-  if (nt == 0) {
-    constexpr int PW = 4 * FieldWords<F>::value;
-    st_xyzz<F>(buckets + (size_t)b * PW, XYZZ<F>::inf());
-    return;
-  }
-  if (nt == 1) {
-    tasks[slot] = {start, cnt, b, 0u};
-    return;
-  }
-  const uint32_t pbase = atomicAdd(&counters[1], nt);
-  const uint32_t mslot = atomicAdd(&counters[2], 1u);
-  multi[mslot] = {b, pbase, nt, 0u};
+#pragma unroll 1
   for (uint32_t t = 0; t < nt; t++) {
-    const uint32_t s = start + t * task_len;
-    const uint32_t l = min(task_len, cnt - t * task_len);
-    tasks[slot + t] = {s, l, nb + pbase + t, 0u};
+    const uint32_t len = t < nfull ? task_len : last;
+    const uint32_t slot = base_s[len] + atomicAdd(&cnt_s[len], 1u);
+    tasks[slot] = {start + t * task_len, len, nt == 1 ? b : nb + pbase + t, 0u};
   }
 }
 
@@ -201,7 +240,7 @@ __global__ void __launch_bounds__(128) k_combine(const Multi* __restrict__ multi
     XYZZ<F> acc = XYZZ<F>::inf();
 #pragma unroll 1
     for (uint32_t i = threadIdx.x; i < mu.count; i += blockDim.x)
-      acc = xyzz_add(acc, ld_xyzz<F>(partials + (size_t)(mu.pbase + i) * XW));
+      acc = xyzz_add_cold(acc, ld_xyzz<F>(partials + (size_t)(mu.pbase + i) * XW));
     // warp tree
 #pragma unroll 1
     for (int d = 16; d > 0; d >>= 1) {
@@ -210,7 +249,7 @@ __global__ void __launch_bounds__(128) k_combine(const Multi* __restrict__ multi
       const uint32_t* aw = reinterpret_cast<const uint32_t*>(&acc);
 #pragma unroll
       for (int w = 0; w < XW; w++) ow[w] = __shfl_down_sync(0xffffffffu, aw[w], d);
-      acc = xyzz_add(acc, o);
+      acc = xyzz_add_cold(acc, o);
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (lane == 0) {
@@ -225,7 +264,7 @@ __global__ void __launch_bounds__(128) k_combine(const Multi* __restrict__ multi
         XYZZ<F> o;
         uint32_t* ow = reinterpret_cast<uint32_t*>(&o);
         for (int w = 0; w < XW; w++) ow[w] = red[k][w];
-        s = xyzz_add(s, o);
+        s = xyzz_add_cold(s, o);
       }
       st_xyzz<F>(buckets + (size_t)mu.bucket * XW, s);
     }
@@ -271,19 +310,127 @@ __global__ void __launch_bounds__(128) k_reduce_level(const uint32_t* __restrict
   st_xyzz<F>(zout + ((size_t)j * nout + t) * XW, s);
 }
 
-// Window sums S_j = y_j + z_j, then sum_j 2^(c j) S_j and the affine result.
 template <class F>
-__global__ void k_finish(const uint32_t* __restrict__ y, const uint32_t* __restrict__ z, int W,
-                         int c, uint32_t* __restrict__ out) {
+CSB_DEV XYZZ<F> shfl_down_xyzz(const XYZZ<F>& v, int d) {
+  constexpr int XW = 4 * FieldWords<F>::value;
+  XYZZ<F> o;
+  uint32_t* ow = reinterpret_cast<uint32_t*>(&o);
+  const uint32_t* vw = reinterpret_cast<const uint32_t*>(&v);
+#pragma unroll
+  for (int w = 0; w < XW; w++) ow[w] = __shfl_down_sync(0xffffffffu, vw[w], d);
+  return o;
+}
+
+// Per-window sum after level 0.  With y_t the segment totals and z_t the in-segment
+// weighted sums of level 0, S_j = sum_t (y_t + z_t) + 8 * sum_t t * y_t.  One block per
+// window, E consecutive segments per thread u:
+//   V_u = Y_u + Z_u + 8 * sum_i i*y_{uE+i}      (Y_u, Z_u: the thread's totals)
+//   sum_t t*y_t = sum_u [sum_i i*y_{uE+i}] + E * sum_{u>=1} Suf(u),  Suf(u) = sum_{v>=u} Y_v
+// so S_j = sum_u (V_u + 8E * Suf(u) [u >= 1]): a block suffix scan and a block reduction,
+// about 2E + 25 dependent point operations instead of a serial pass over the segments.
+template <class F, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restrict__ y,
+                                                        const uint32_t* __restrict__ z, uint32_t n1,
+                                                        uint32_t* __restrict__ wsum) {
+  constexpr int XW = 4 * FieldWords<F>::value;
+  constexpr int NW = THREADS / 32;
+  __shared__ uint32_t sh[NW][XW];
+  const int j = blockIdx.x;
+  const uint32_t* yj = y + (size_t)j * n1 * XW;
+  const uint32_t* zj = z + (size_t)j * n1 * XW;
+  const uint32_t E = (n1 + THREADS - 1) / THREADS;  // n1 is a power of two
+  const uint32_t u = threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  XYZZ<F> acc = XYZZ<F>::inf(), ws = XYZZ<F>::inf(), zs = XYZZ<F>::inf();
+#pragma unroll 1
+  for (int i = (int)E - 1; i >= 0; i--) {
+    const uint32_t idx = u * E + i;
+    if (idx < n1) {
+      acc = xyzz_add_cold(acc, ld_xyzz<F>(yj + (size_t)idx * XW));
+      zs = xyzz_add_cold(zs, ld_xyzz<F>(zj + (size_t)idx * XW));
+    }
+    if (i > 0) ws = xyzz_add_cold(ws, acc);
+  }
+  // V = acc + zs + 8 ws
+  ws = xyzz_dbl_cold(xyzz_dbl_cold(xyzz_dbl_cold(ws)));
+  XYZZ<F> V = xyzz_add_cold(xyzz_add_cold(acc, zs), ws);
+  // inclusive suffix scan of acc across the block
+  XYZZ<F> suf = acc;
+#pragma unroll 1
+  for (int d = 1; d < 32; d <<= 1) {
+    const XYZZ<F> o = shfl_down_xyzz(suf, d);
+    if (lane + d < 32) suf = xyzz_add_cold(suf, o);
+  }
+  if (lane == 0) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(&suf);
+    for (int k = 0; k < XW; k++) sh[warp][k] = w[k];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    XYZZ<F> t = XYZZ<F>::inf();
+    if (lane < NW) {
+      uint32_t* w = reinterpret_cast<uint32_t*>(&t);
+      for (int k = 0; k < XW; k++) w[k] = sh[lane][k];
+    }
+    // exclusive suffix over warp totals: lane w gets sum of totals of warps > w
+#pragma unroll 1
+    for (int d = 1; d < 32; d <<= 1) {
+      const XYZZ<F> o = shfl_down_xyzz(t, d);
+      if (lane + d < 32) t = xyzz_add_cold(t, o);
+    }
+    XYZZ<F> excl = shfl_down_xyzz(t, 1);
+    if (lane == 31) excl = XYZZ<F>::inf();
+    __syncwarp();
+    if (lane < NW) {
+      const uint32_t* w = reinterpret_cast<const uint32_t*>(&excl);
+      for (int k = 0; k < XW; k++) sh[lane][k] = w[k];
+    }
+  }
+  __syncthreads();
+  {
+    XYZZ<F> off;
+    uint32_t* w = reinterpret_cast<uint32_t*>(&off);
+    for (int k = 0; k < XW; k++) w[k] = sh[warp][k];
+    suf = xyzz_add_cold(suf, off);
+  }
+  __syncthreads();
+  // C_u = V_u + 8E * Suf(u) for u >= 1 (8E is a power of two)
+  if (u >= 1 && u * E < n1) {
+#pragma unroll 1
+    for (uint32_t m = 8 * E; m > 1; m >>= 1) suf = xyzz_dbl_cold(suf);
+    V = xyzz_add_cold(V, suf);
+  }
+  // block reduction of V
+#pragma unroll 1
+  for (int d = 16; d > 0; d >>= 1) V = xyzz_add_cold(V, shfl_down_xyzz(V, d));
+  if (lane == 0) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(&V);
+    for (int k = 0; k < XW; k++) sh[warp][k] = w[k];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    XYZZ<F> t = XYZZ<F>::inf();
+    if (lane < NW) {
+      uint32_t* w = reinterpret_cast<uint32_t*>(&t);
+      for (int k = 0; k < XW; k++) w[k] = sh[lane][k];
+    }
+#pragma unroll 1
+    for (int d = 16; d > 0; d >>= 1) t = xyzz_add_cold(t, shfl_down_xyzz(t, d));
+    if (lane == 0) st_xyzz<F>(wsum + (size_t)j * XW, t);
+  }
+}
+
+// sum_j 2^(c j) S_j (Horner over the windows) and the affine result.
+template <class F>
+__global__ void k_finish(const uint32_t* __restrict__ wsum, int W, int c, uint32_t* __restrict__ out) {
   constexpr int XW = 4 * FieldWords<F>::value;
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  XYZZ<F> r = XYZZ<F>::inf();
+  XYZZ<F> r = ld_xyzz<F>(wsum + (size_t)(W - 1) * XW);
 #pragma unroll 1
-  for (int j = W - 1; j >= 0; j--) {
+  for (int j = W - 2; j >= 0; j--) {
 #pragma unroll 1
-    for (int d = 0; d < c && j != W - 1; d++) r = xyzz_dbl(r);
-    r = xyzz_add(r, ld_xyzz<F>(y + (size_t)j * XW));
-    r = xyzz_add(r, ld_xyzz<F>(z + (size_t)j * XW));
+    for (int d = 0; d < c; d++) r = xyzz_dbl_cold(r);
+    r = xyzz_add_cold(r, ld_xyzz<F>(wsum + (size_t)j * XW));
   }
   st_affine<F>(out, xyzz_to_affine(r));
 }
@@ -294,8 +441,12 @@ __global__ void k_store_inf(uint32_t* out) {
 }
 
 // --------------------------------------------------------------- workspace layout ----
+// counters block: [0] tasks, [1] partial slots, [2] split buckets; hist at +16 and
+// bin cursors at +96 (kMaxTask + 1 words each).
+constexpr int kCtrHist = 16, kCtrCursor = 96, kCtrWords = 192;
+
 struct Layout {
-  size_t counts, offsets, entries, tasks, multi, partials, buckets, lv_a, lv_b, counters, total;
+  size_t counts, offsets, entries, tasks, multi, partials, buckets, lv_y, lv_z, wsum, counters, total;
 };
 
 static inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -306,9 +457,10 @@ inline Layout make_layout(uint32_t n, int c, int xyzz_bytes, uint32_t task_len) 
   const size_t ne = (size_t)n * W;
   const size_t max_tasks = nb + ne / task_len + 1;
   const size_t max_partials = 2 * (ne / task_len) + 1;
+  const size_t n1 = ((size_t)1 << (c - 1)) / 8 + 1;
   Layout L{};
   size_t o = 0;
-  L.counters = o; o = align256(o + 4 * sizeof(uint32_t));
+  L.counters = o; o = align256(o + kCtrWords * sizeof(uint32_t));
   L.counts = o;   o = align256(o + (nb + 1) * sizeof(uint32_t));
   L.offsets = o;  o = align256(o + (nb + 1) * sizeof(uint32_t));
   L.entries = o;  o = align256(o + ne * sizeof(uint32_t));
@@ -316,11 +468,23 @@ inline Layout make_layout(uint32_t n, int c, int xyzz_bytes, uint32_t task_len) 
   L.multi = o;    o = align256(o + (ne / (task_len + 1) + 1) * sizeof(Multi));
   L.partials = o; o = align256(o + max_partials * (size_t)xyzz_bytes);
   L.buckets = o;  o = align256(o + nb * (size_t)xyzz_bytes);
-  const size_t lv = ((nb / 8) + W) * (size_t)xyzz_bytes;
-  L.lv_a = o;     o = align256(o + 2 * lv);
-  L.lv_b = o;     o = align256(o + 2 * lv);
+  L.lv_y = o;     o = align256(o + (size_t)W * n1 * xyzz_bytes);
+  L.lv_z = o;     o = align256(o + (size_t)W * n1 * xyzz_bytes);
+  L.wsum = o;     o = align256(o + (size_t)W * xyzz_bytes);
   L.total = o + scan_workspace_bytes(nb + 1);
   return L;
+}
+
+template <class F>
+int accumulate_grid(int sms) {
+  static int blocks_per_sm = 0;
+  if (blocks_per_sm == 0) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_accumulate<F>, 128, 0) != cudaSuccess || b < 1)
+      b = 1;
+    blocks_per_sm = b;
+  }
+  return blocks_per_sm * sms;
 }
 
 template <class F>
@@ -329,13 +493,17 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
                      cudaStream_t st) {
   constexpr bool EC2 = FieldWords<F>::value == 16;
   constexpr int XB = 4 * FieldWords<F>::value * 4;  // bytes per XYZZ point
+  constexpr int XWD = XB / 4;                       // words per XYZZ point
   if (n == 0) {
     k_store_inf<F><<<1, 32, 0, st>>>(d_out);
+    note_launch();
     return cudaGetLastError();
   }
   const int c = cfg.c > 0 ? cfg.c : msm_default_window(n, EC2);
   if (c < 4 || c > 24) return cudaErrorInvalidValue;
-  const uint32_t task_len = cfg.task >= (int)kMinTask ? (uint32_t)cfg.task : 64u;
+  uint32_t task_len = cfg.task > 0 ? (uint32_t)cfg.task : 64u;
+  if (task_len < kMinTask) task_len = kMinTask;
+  if (task_len > (uint32_t)kMaxTask) task_len = kMaxTask;
   const int W = num_windows(c);
   const uint32_t nb = (uint32_t)W << (c - 1);
   const Layout L = make_layout(n, c, XB, kMinTask);
@@ -349,46 +517,52 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   Multi* multi = reinterpret_cast<Multi*>(base + L.multi);
   uint32_t* partials = reinterpret_cast<uint32_t*>(base + L.partials);
   uint32_t* buckets = reinterpret_cast<uint32_t*>(base + L.buckets);
-  uint32_t* lva = reinterpret_cast<uint32_t*>(base + L.lv_a);
-  uint32_t* lvb = reinterpret_cast<uint32_t*>(base + L.lv_b);
+  uint32_t* lv_y = reinterpret_cast<uint32_t*>(base + L.lv_y);
+  uint32_t* lv_z = reinterpret_cast<uint32_t*>(base + L.lv_z);
+  uint32_t* wsum = reinterpret_cast<uint32_t*>(base + L.wsum);
   void* scan_tmp = base + (L.total - scan_workspace_bytes(nb + 1));
 
   cudaError_t e;
-  if ((e = cudaMemsetAsync(counters, 0, 4 * sizeof(uint32_t), st)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(counters, 0, kCtrWords * sizeof(uint32_t), st)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(counts, 0, (nb + 1) * sizeof(uint32_t), st)) != cudaSuccess) return e;
   const int T = 256;
   k_count<F><<<(n + T - 1) / T, T, 0, st>>>(d_scalars, d_points, n, c, W, counts);
+  note_launch();
   if ((e = scan_exclusive_u32(counts, offsets, nb + 1, scan_tmp, st)) != cudaSuccess) return e;
   // counts is reused as the scatter cursor
   if ((e = cudaMemcpyAsync(counts, offsets, nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
     return e;
   k_scatter<F><<<(n + T - 1) / T, T, 0, st>>>(d_scalars, d_points, n, c, W, counts, entries);
-  k_tasks<F><<<(nb + T - 1) / T, T, 0, st>>>(offsets, nb, task_len, tasks, counters, multi, buckets);
+  note_launch();
+  k_task_hist<F><<<(nb + T - 1) / T, T, 0, st>>>(offsets, nb, task_len, counters + kCtrHist, buckets);
+  note_launch();
+  k_task_bins<<<1, 32, 0, st>>>(counters + kCtrHist, task_len, counters + kCtrCursor, counters);
+  note_launch();
+  k_task_emit<F><<<(nb + T - 1) / T, T, 0, st>>>(offsets, nb, task_len, counters + kCtrCursor, tasks,
+                                                  counters, multi);
+  note_launch();
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_accumulate<F><<<sms * 8, 128, 0, st>>>(tasks, counters, entries, d_points, nb, buckets, partials);
+  if (cfg.acc_start) cudaEventRecord(cfg.acc_start, st);
+  k_accumulate<F><<<accumulate_grid<F>(sms), 128, 0, st>>>(tasks, counters, entries, d_points, nb,
+                                                           buckets, partials);
+  note_launch();
   k_combine<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);
-  // hierarchical bucket reduction
-  const uint32_t* y = buckets;
-  const uint32_t* z = nullptr;
-  uint32_t len = 1u << (c - 1);
-  uint32_t* bufs[2][2] = {{lva, lva + ((size_t)(nb / 8) + W) * (XB / 4)},
-                          {lvb, lvb + ((size_t)(nb / 8) + W) * (XB / 4)}};
-  int level = 0, pp = 0;
-  while (len > 1) {
-    const uint32_t nout = (len + 7) / 8;
-    uint32_t* yo = bufs[pp][0];
-    uint32_t* zo = bufs[pp][1];
-    const uint32_t threads = (uint32_t)W * nout;
-    k_reduce_level<F><<<(threads + 127) / 128, 128, 0, st>>>(y, z, len, nout, W, level, yo, zo);
-    y = yo; z = zo; len = nout; level++; pp ^= 1;
-  }
-  if (z == nullptr) {
-    // c == 1 is excluded above, so at least one level always runs
-    return cudaErrorInvalidValue;
-  }
-  k_finish<F><<<1, 32, 0, st>>>(y, z, W, c, d_out);
+  note_launch();
+  if (cfg.acc_stop) cudaEventRecord(cfg.acc_stop, st);
+  // level 0: segments of 8 buckets -> totals y and in-segment weighted sums z
+  const uint32_t B = 1u << (c - 1);
+  const uint32_t n1 = (B + 7) / 8;
+  const uint32_t threads0 = (uint32_t)W * n1;
+  k_reduce_level<F><<<(threads0 + 127) / 128, 128, 0, st>>>(buckets, nullptr, B, n1, W, 0, lv_y, lv_z);
+  note_launch();
+  constexpr int WT = 256;
+  k_window_sum<F, WT><<<W, WT, 0, st>>>(lv_y, lv_z, n1, wsum);
+  note_launch();
+  k_finish<F><<<1, 32, 0, st>>>(wsum, W, c, d_out);
+  note_launch();
+  (void)XWD;
   return cudaGetLastError();
 }
 

@@ -68,12 +68,17 @@ struct cs_ctx {
   csb::DeviceBuffer in;        // device copies of host inputs
   csb::DeviceBuffer out;       // device results
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  cudaEvent_t ev_phase0 = nullptr, ev_phase1 = nullptr;  // bucket accumulation of the last MSM
   float last_ms = 0.f;
+  float last_phase_ms = 0.f;
+  bool phase_valid = false;
   std::string err;
   std::mutex mu;               // one call at a time per context
 };
 
 namespace csb {
+// Counts kernel launches made by this library (cs_kernel_launches()).
+void note_launch(unsigned n = 1);
 // Records a CUDA error on the context and maps it to the C ABI status code.
 int fail(cs_ctx* ctx, cudaError_t e, const char* where);
 int fail_msg(cs_ctx* ctx, int code, const std::string& msg);

@@ -1,6 +1,7 @@
 // scan.cu -- multi-level exclusive scan: every block scans 4096 elements (1024 threads x
 // 4), block totals are scanned recursively, then added back.
 #include "scan.cuh"
+#include "runtime.cuh"
 
 namespace csb {
 
@@ -75,6 +76,7 @@ cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, void
   if (n == 0) return cudaSuccess;
   if (n <= kTile) {
     k_scan_tile<<<1, kThreads, 0, st>>>(in, out, n, nullptr);
+    note_launch();
     return cudaGetLastError();
   }
   const size_t tiles = (n + kTile - 1) / kTile;
@@ -82,9 +84,11 @@ cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, void
   uint32_t* sums_scan = reinterpret_cast<uint32_t*>(static_cast<char*>(tmp) + align256(tiles * 4));
   void* rest = static_cast<char*>(tmp) + 2 * align256(tiles * 4);
   k_scan_tile<<<(unsigned)tiles, kThreads, 0, st>>>(in, out, n, sums);
+  note_launch();
   cudaError_t e = scan_exclusive_u32(sums, sums_scan, tiles, rest, st);
   if (e != cudaSuccess) return e;
   k_add_tile_offsets<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(out, n, sums_scan);
+  note_launch();
   return cudaGetLastError();
 }
 

@@ -59,6 +59,24 @@ typedef struct {
   char *filename;
 } jacadd_reduced_t;
 
+/* ntt_interpolandmul_t, reference src/cuda/types.h:530-546. */
+typedef struct {
+  uint32_t *A;
+  uint32_t *B;
+  uint32_t *roots;
+  uint32_t Nrows;
+  uint32_t Ncols;
+  uint32_t mNrows;
+  uint32_t mNcols;
+  uint32_t nroots;
+  uint32_t rstride;
+  uint32_t pidx;
+  uint32_t max_threads;
+  uint32_t start_idx;
+  uint32_t last_idx;
+  uint32_t thread_id;
+} ntt_interpolandmul_t;
+
 /* ------------------------------------------------ drop-in reference entry points --- */
 /* Replaces ec_jacreduce_server_h, reference src/cuda/ec.cpp:1536 (bound at
  * src/cython/_utils_host.pxd:139).  out_ep <- sum_i scl[i] * x[i] as affine Montgomery
@@ -69,6 +87,46 @@ typedef struct {
 void ec_jacreduce_server_h(jacadd_reduced_t *args);
 /* Replaces ec2_jacreduce_server_h, reference src/cuda/ec.cpp:1530 (same as above). */
 void ec2_jacreduce_server_h(jacadd_reduced_t *args);
+
+/* Field arithmetic, reference src/cuda/ff.cpp (bound at src/cython/_utils_host.pxd:41-65):
+ * single-element Montgomery product, square, modular add/sub and Montgomery inverse
+ * (replacing montmult_h ff.cpp:225, montsquare_h :423, addm_h :679, subm_h :713,
+ * montinv_h :745), and the batched conversions to_montgomeryN_h :658 and
+ * from_montgomeryN_h :503 (strip_last 0 only; other values report CS_ERR_UNSUPPORTED).
+ * Results go to host memory; status in cs_field_last_status(). */
+void montmult_h(uint32_t *U, const uint32_t *A, const uint32_t *B, uint32_t pidx);
+void montsquare_h(uint32_t *U, const uint32_t *A, uint32_t pidx);
+void addm_h(uint32_t *U, const uint32_t *A, const uint32_t *B, uint32_t pidx);
+void subm_h(uint32_t *U, const uint32_t *A, const uint32_t *B, uint32_t pidx);
+void montinv_h(uint32_t *y, uint32_t *x, uint32_t pidx);
+void to_montgomeryN_h(uint32_t *z, const uint32_t *x, uint32_t n, uint32_t pidx);
+void from_montgomeryN_h(uint32_t *z, const uint32_t *x, uint32_t n, uint32_t pidx, uint32_t strip_last);
+int cs_field_last_status(void);
+
+/* Number-theoretic transforms over Fr (pidx must be 1, MOD_FIELD).
+ * Replaces ntt_h, reference src/cuda/ntt.cpp:453 (bound at _utils_host.pxd:70):
+ *   A[k*astride] <- sum_j A[j*astride] roots[(rstride*j*k*direction) mod (rstride*2^levels)],
+ *   natural order, in place.
+ * Replaces intt_h, reference src/cuda/ntt.cpp:583 (_utils_host.pxd:72): the inverse
+ *   transform (direction -1 on the same table) scaled by 2^-levels, output Montgomery
+ *   (fmat 1) or normal form (fmat 0).
+ * Replaces find_roots_h, reference src/cuda/ntt.cpp:1164: roots[i] = primitive_root^i.
+ * Status in cs_ntt_last_status(). */
+void ntt_h(uint32_t *A, const uint32_t *roots, uint32_t levels, unsigned long long astride,
+           unsigned long long rstride, int32_t direction, uint32_t pidx);
+void intt_h(uint32_t *A, const uint32_t *roots, uint32_t fmat, uint32_t levels,
+            unsigned long long rstride, uint32_t pidx);
+void find_roots_h(uint32_t *roots, uint32_t *primitive_root, uint32_t nroots, uint32_t pidx);
+/* Replaces ntt_interpolandmul_server_h, reference src/cuda/ntt.cpp:672 (_utils_host.pxd:89):
+ * A, B = evaluations (Montgomery) on the m = 2^(Nrows+Ncols) roots; returns a pointer to
+ * the 2m coefficients of A(x)B(x) in normal form, held in a library buffer that stays
+ * valid until the next call (the reference returns its global M_transpose the same way).
+ * roots is the caller's concatenated table whose first 2m entries are powers of the 2m-th
+ * root; rstride as in the reference (2).  A and B are left unmodified.  NULL on error. */
+uint32_t *ntt_interpolandmul_server_h(ntt_interpolandmul_t *args);
+/* Replaces get_Mtranspose_h, reference src/cuda/ntt.cpp:659: the last H-step result. */
+uint32_t *get_Mtranspose_h(void);
+int cs_ntt_last_status(void);
 
 /* Status of the last drop-in call made by this thread, and its message. */
 int cs_last_status(void);
@@ -87,6 +145,8 @@ int cs_ctx_sync(cs_ctx *ctx);
 const char *cs_ctx_error(cs_ctx *ctx);
 /* Device time in milliseconds of the kernels of the last cs_* call (CUDA events). */
 float cs_ctx_last_ms(cs_ctx *ctx);
+/* Device time in milliseconds of the bucket-accumulation kernels of the last MSM. */
+float cs_ctx_last_phase_ms(cs_ctx *ctx);
 
 /* Multi-exponentiation with host pointers: copies in, computes, copies the affine result
  * out, synchronises.  ec2 selects G2.  window = Pippenger window bits (0 = automatic). */
@@ -98,6 +158,63 @@ int cs_msm_device(cs_ctx *ctx, int ec2, const uint32_t *d_scalars, const uint32_
                   uint32_t n, uint32_t *d_out_affine, int window);
 /* Scratch bytes one MSM of n terms needs (window 0 = automatic). */
 size_t cs_msm_workspace_bytes(uint32_t n, int ec2, int window);
+/* Window bits the automatic choice uses for n terms, and the resulting window count. */
+int cs_msm_default_window(uint32_t n, int ec2);
+int cs_msm_num_windows(int window);
+
+/* Elementwise field operation on n elements of device arrays (8 words each; 16 for
+ * CS_FOP_FQ2_MUL, which multiplies in Fq2 = Fq[u]/(u^2+1) regardless of pidx).
+ * d_b is ignored by the unary operations.  Asynchronous on the context stream. */
+#define CS_FOP_MUL 0       /* Montgomery product a*b*R^-1 */
+#define CS_FOP_ADD 1
+#define CS_FOP_SUB 2
+#define CS_FOP_SQR 3
+#define CS_FOP_INV 4       /* Montgomery inverse (aR)^-1 R, 0 -> 0 */
+#define CS_FOP_TO_MONT 5   /* a -> aR */
+#define CS_FOP_FROM_MONT 6 /* aR -> a */
+#define CS_FOP_MUL_LOHI 7  /* Montgomery product, mad.lo/mad.hi variant (cross-check) */
+#define CS_FOP_FQ2_MUL 8
+int cs_field_op_device(cs_ctx *ctx, int op, int pidx, const uint32_t *d_a, const uint32_t *d_b,
+                       uint32_t *d_out, uint32_t n);
+
+/* Batched scalar multiplication out[i] = scalars[i] * points[i] (affine Montgomery in and
+ * out, like the reference's ec_jacscmul_h + ec_jac2aff_h, src/cuda/ec.cpp:833, :963).
+ * point_stride_words = words between consecutive base points; 0 = one shared base
+ * (fixed-base, as the reference's proving-key generation kernel sc1mulecjac_kernel,
+ * src/cuda/ecbn128_device.cu:326).  Device pointers, asynchronous on the context stream. */
+int cs_scmul_device(cs_ctx *ctx, int ec2, const uint32_t *d_scalars, const uint32_t *d_points,
+                    uint32_t point_stride_words, uint32_t n, uint32_t *d_out_affine);
+
+/* Transform of 2^log_n Fr elements (Montgomery) with the context's resident twiddles
+ * (primitive roots 5^((r-1)/2^k), the reference's proots_field chain).  direction >= 0:
+ * forward; < 0: inverse scaled by 2^-log_n, Montgomery (fmat 1) or normal (fmat 0) out.
+ * d_in may equal d_out.  Asynchronous on the context stream. */
+int cs_ntt_device(cs_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uint32_t log_n, int direction,
+                  int fmat);
+/* H step on device arrays of m = 2^log_m evaluations (Montgomery):
+ *   CS_HSTEP_REFERENCE: d_out (2m) = coefficients of A(x)B(x), normal form (d_C unused),
+ *                       as ntt_interpolandmul_server_h;
+ *   CS_HSTEP_COSET:     d_out (m) = coefficients of (A B - C)/(x^m - 1) evaluated on the
+ *                       coset 5*<w>, normal form.
+ * Both give the Groth16 quotient H in d_out[m .. 2m-2] / d_out[0 .. m-2] when A B - C
+ * vanishes on the domain. */
+#define CS_HSTEP_REFERENCE 0
+#define CS_HSTEP_COSET 1
+int cs_hstep_device(cs_ctx *ctx, int variant, const uint32_t *d_A, const uint32_t *d_B,
+                    const uint32_t *d_C, uint32_t log_m, uint32_t *d_out);
+
+/* ------------------------------------------------------------ measurement ----------- */
+/* Sustained 32-bit integer multiply-add instruction rate of the context's device
+ * (instructions per second, all SMs), the ceiling for the integer-bound kernels. */
+int cs_bench_imad_peak(cs_ctx *ctx, double *imad_per_s);
+/* Instruction-rate probes (ops per second, all SMs): mode 1 mad.lo.u32, 2 mad.hi.u32,
+ * 3 mad.wide.u32, 4 fma.rn.f64, 5 carry-chained mad.lo.cc/madc.hi.cc. */
+int cs_bench_pipe(cs_ctx *ctx, int mode, double *ops_per_s);
+/* Montgomery products per second (variant 0: mad.lo/mad.hi CIOS, 1: wide-product CIOS;
+ * variant 2 reports 32-bit add-with-carry instructions per second instead). */
+int cs_bench_mulmod(cs_ctx *ctx, int variant, double *rate);
+/* Number of kernels this library has launched in the process so far. */
+unsigned long long cs_kernel_launches(void);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,99 @@
+"""GPU field arithmetic (both multiplication variants) against the oracle, bit-exact."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle.oracle import random_field, ints_to_limbs, Q, R, MOD
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from cusnarks_b200 import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def _edge(p):
+    vals = [0, 1, 2, p - 1, p - 2, (1 << 256) % p, p >> 1, (p >> 1) + 1, 0xFFFFFFFF, 1 << 224]
+    return ints_to_limbs(vals)
+
+
+def _run(ctx, op, pidx, a, b=None, words=8):
+    import torch
+    da = torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
+    db = torch.from_numpy(np.ascontiguousarray(b).view(np.int32)).cuda() if b is not None else None
+    dout = torch.zeros_like(da)
+    ctx.field_op_device(op, pidx, da.data_ptr(), db.data_ptr() if db is not None else 0,
+                        dout.data_ptr(), a.shape[0])
+    ctx.sync()
+    return dout.cpu().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize("pidx", [0, 1])
+def test_binary_ops(ctx, oracle, pidx):
+    rng = np.random.Generator(np.random.PCG64(31 + pidx))
+    a = np.concatenate([random_field(rng, 4000, pidx), _edge(MOD[pidx])])
+    b = np.concatenate([random_field(rng, 4000, pidx), _edge(MOD[pidx])[::-1]])
+    want_mul = oracle.montmult(a, b, pidx)
+    assert np.array_equal(_run(ctx, "mul", pidx, a, b), want_mul)
+    assert np.array_equal(_run(ctx, "mul_lohi", pidx, a, b), want_mul)
+    z_add = np.zeros_like(a); z_sub = np.zeros_like(a)
+    P = ctypes.POINTER(ctypes.c_uint32)
+    for i in range(a.shape[0]):
+        oracle.lib.or_addm(z_add[i].ctypes.data_as(P), a[i].ctypes.data_as(P), b[i].ctypes.data_as(P), pidx)
+        oracle.lib.or_subm(z_sub[i].ctypes.data_as(P), a[i].ctypes.data_as(P), b[i].ctypes.data_as(P), pidx)
+    assert np.array_equal(_run(ctx, "add", pidx, a, b), z_add)
+    assert np.array_equal(_run(ctx, "sub", pidx, a, b), z_sub)
+
+
+@pytest.mark.parametrize("pidx", [0, 1])
+def test_unary_ops(ctx, oracle, pidx):
+    rng = np.random.Generator(np.random.PCG64(41 + pidx))
+    a = np.concatenate([random_field(rng, 1000, pidx), _edge(MOD[pidx])])
+    assert np.array_equal(_run(ctx, "sqr", pidx, a), oracle.montmult(a, a, pidx))
+    assert np.array_equal(_run(ctx, "to_mont", pidx, a), oracle.to_mont(a, pidx))
+    assert np.array_equal(_run(ctx, "from_mont", pidx, a), oracle.from_mont(a, pidx))
+    inv = np.zeros_like(a)
+    P = ctypes.POINTER(ctypes.c_uint32)
+    for i in range(a.shape[0]):
+        oracle.lib.or_montinv(inv[i].ctypes.data_as(P), a[i].ctypes.data_as(P), pidx)
+    assert np.array_equal(_run(ctx, "inv", pidx, a), inv)
+
+
+def test_field_known_answers(ctx, golden):
+    kat = golden("field_kat.npz")
+    # test_mul (reference test_utils_host.cpp:7160): montmult_h(A, B, MOD_FIELD) == C
+    assert np.array_equal(_run(ctx, "mul", 1, kat["A"], kat["B"]), kat["C"])
+
+
+def test_fq2_mul(ctx, oracle):
+    rng = np.random.Generator(np.random.PCG64(51))
+    a = random_field(rng, 2000, 0).reshape(-1, 16)
+    b = random_field(rng, 2000, 0).reshape(-1, 16)
+    want = np.zeros_like(a)
+    P = ctypes.POINTER(ctypes.c_uint32)
+    for i in range(a.shape[0]):
+        oracle.lib.or_montmult_ext(want[i].ctypes.data_as(P), a[i].ctypes.data_as(P), b[i].ctypes.data_as(P), 0)
+    assert np.array_equal(_run(ctx, "fq2_mul", 0, a, b), want)
+
+
+def test_dropin_field_entry_points(oracle):
+    from cusnarks_b200 import lib
+    L = lib()
+    rng = np.random.Generator(np.random.PCG64(61))
+    a = random_field(rng, 64, 1); b = random_field(rng, 64, 1)
+    out = np.zeros(8, np.uint32)
+    L.montmult_h(out.ctypes.data, a[0].ctypes.data, b[0].ctypes.data, 1)
+    assert L.cs_field_last_status() == 0
+    assert np.array_equal(out, oracle.montmult(a[:1], b[:1], 1)[0])
+    z = np.zeros_like(a)
+    L.to_montgomeryN_h(z.ctypes.data, a.ctypes.data, 64, 1)
+    assert np.array_equal(z, oracle.to_mont(a, 1))
+    L.from_montgomeryN_h(z.ctypes.data, a.ctypes.data, 64, 1, 0)
+    assert np.array_equal(z, oracle.from_mont(a, 1))
+    L.from_montgomeryN_h(z.ctypes.data, a.ctypes.data, 64, 1, 2)
+    assert L.cs_field_last_status() == 4  # unsupported option reported, no exit

@@ -131,3 +131,26 @@ def test_msm_device_pointers_torch(ctx, oracle, pts_g1):
     ctx.sync()
     got = dout.cpu().numpy().view(np.uint32)
     assert np.array_equal(got, oracle.msm(s, pts_g1[:2048]))
+
+
+@pytest.mark.parametrize("ec2", [0, 1])
+def test_scmul_matches_oracle(ctx, oracle, golden, ec2):
+    """Batched k_i * P_i (golden scalars include full 256-bit values) and fixed base."""
+    import torch
+    g = golden("g2_msm_1024.npz" if ec2 else "g1_msm_1024.npz")
+    n = 256
+    s = np.ascontiguousarray(g["scalars"][:n])
+    p = np.ascontiguousarray(g["points"][:n])
+    pw = p.shape[1]
+    ds = torch.from_numpy(s.view(np.int32)).cuda()
+    dp = torch.from_numpy(p.view(np.int32)).cuda()
+    dout = torch.zeros((n, pw), dtype=torch.int32, device="cuda")
+    ctx.scmul_device(ds.data_ptr(), dp.data_ptr(), n, dout.data_ptr(), ec2=bool(ec2))
+    ctx.sync()
+    assert np.array_equal(dout.cpu().numpy().view(np.uint32), oracle.scmul(s, p, ec2))
+    # fixed base: every scalar times point 3
+    dout.zero_()
+    ctx.scmul_device(ds.data_ptr(), dp[3].data_ptr(), n, dout.data_ptr(), ec2=bool(ec2),
+                     point_stride_words=0)
+    ctx.sync()
+    assert np.array_equal(dout.cpu().numpy().view(np.uint32), oracle.scmul(s, p[3:4], ec2))
