@@ -88,6 +88,10 @@ _SIGNATURES = [
     ("cs_ntt_last_status", ctypes.c_int, []),
     ("cs_ntt_device", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint32, ctypes.c_int, ctypes.c_int]),
     ("cs_hstep_device", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, ctypes.c_uint32, _vp]),
+    ("cs_msm_g1_noalloc", ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, _vp]),
+    ("cs_msm_noalloc_scratch_bytes", ctypes.c_size_t, []),
+    ("cs_msm_g1_noalloc_max_terms", ctypes.c_uint32, []),
+    ("cs_msm_g1_noalloc_error", ctypes.c_char_p, []),
     ("ec_jacreduce_server_h", None, [ctypes.POINTER(JacaddReduced)]),
     ("ec2_jacreduce_server_h", None, [ctypes.POINTER(JacaddReduced)]),
 ]

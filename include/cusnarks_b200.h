@@ -203,6 +203,24 @@ int cs_ntt_device(cs_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uint32_t l
 int cs_hstep_device(cs_ctx *ctx, int variant, const uint32_t *d_A, const uint32_t *d_B,
                     const uint32_t *d_C, uint32_t log_m, uint32_t *d_out);
 
+/* G1 multi-exponentiation that allocates nothing (no counterpart in the reference).
+ * For callers whose device memory is owned by a host framework's pool and who may not
+ * call cudaMalloc themselves, or cannot afford its implicit synchronisation on a
+ * latency-critical path.  Inputs and output are the caller's device pointers (same
+ * layout as cs_msm_device, automatic window); scratch is a fixed file-scope device array
+ * of cs_msm_noalloc_scratch_bytes() bytes (32 MiB) that every GPU loading this library
+ * keeps reserved until exit, which bounds n to cs_msm_g1_noalloc_max_terms() (2^16);
+ * larger n is rejected with CS_ERR_ARG and a message in cs_msm_g1_noalloc_error().
+ * Runs asynchronously on `stream` (a cudaStream_t, NULL = legacy default stream).  The
+ * first call on a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.  Every call shares
+ * the array: calls that overlap on the GPU race, so order them on one stream. */
+int cs_msm_g1_noalloc(const uint32_t *d_scalars, const uint32_t *d_points, uint32_t n,
+                      uint32_t *d_out_affine, void *stream);
+size_t cs_msm_noalloc_scratch_bytes(void);
+uint32_t cs_msm_g1_noalloc_max_terms(void);
+const char *cs_msm_g1_noalloc_error(void);
+
 /* ------------------------------------------------------------ measurement ----------- */
 /* Sustained 32-bit integer multiply-add instruction rate of the context's device
  * (instructions per second, all SMs), the ceiling for the integer-bound kernels. */
