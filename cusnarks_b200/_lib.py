@@ -29,6 +29,21 @@ class CsError(RuntimeError):
         self.code = code
 
 
+class MpolyEval(ctypes.Structure):
+    """mpoly_eval_t (reference src/cuda/types.h:516-528)."""
+    _fields_ = [("pout", _vp), ("scalar", _vp), ("pin", _vp), ("reduce_coeff", ctypes.c_uint32),
+                ("start_idx", ctypes.c_uint32), ("last_idx", ctypes.c_uint32),
+                ("max_threads", ctypes.c_uint32), ("thread_id", ctypes.c_uint32), ("pidx", ctypes.c_uint32)]
+
+
+class PkDesc(ctypes.Structure):
+    """cs_pk_desc (include/cusnarks_b200.h)."""
+    _fields_ = [("n_vars", ctypes.c_uint32), ("n_public", ctypes.c_uint32), ("domain_size", ctypes.c_uint32),
+                ("polsA", _vp), ("polsA_words", ctypes.c_size_t), ("polsA_entries", ctypes.c_uint32),
+                ("polsB", _vp), ("polsB_words", ctypes.c_size_t), ("polsB_entries", ctypes.c_uint32),
+                ("A", _vp), ("B1", _vp), ("B2", _vp), ("C", _vp), ("hExps", _vp), ("delta_1", _vp)]
+
+
 class InterpolAndMul(ctypes.Structure):
     """ntt_interpolandmul_t (reference src/cuda/types.h:530-546)."""
     _fields_ = [("A", _vp), ("B", _vp), ("roots", _vp), ("Nrows", ctypes.c_uint32),
@@ -92,6 +107,19 @@ _SIGNATURES = [
     ("cs_msm_noalloc_scratch_bytes", ctypes.c_size_t, []),
     ("cs_msm_g1_noalloc_max_terms", ctypes.c_uint32, []),
     ("cs_msm_g1_noalloc_error", ctypes.c_char_p, []),
+    ("mpoly_eval_server_h", None, [_vp]),
+    ("mpoly_eval_h", _vp, [_vp]),
+    ("cs_qap_last_status", ctypes.c_int, []),
+    ("cs_pk_create", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("cs_pk_destroy", None, [_vp]),
+    ("cs_prove_workspace_bytes", ctypes.c_size_t, [_vp]),
+    ("cs_prove", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    ("cs_prove_device", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    ("cs_setup_lagrange", ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp]),
+    ("cs_setup_wire_eval", ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32, _vp]),
+    ("cs_setup_c_scalars", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_uint32, _vp]),
+    ("cs_setup_pow_scalars", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint32, _vp]),
+    ("cs_r1cs_layer_eval", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_uint32, _vp, _vp]),
     ("ec_jacreduce_server_h", None, [ctypes.POINTER(JacaddReduced)]),
     ("ec2_jacreduce_server_h", None, [ctypes.POINTER(JacaddReduced)]),
 ]

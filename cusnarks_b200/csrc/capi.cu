@@ -15,6 +15,17 @@ void domain_release(cs_ctx* ctx);  // hstep.cu
 static std::atomic<unsigned long long> g_launches{0};
 void note_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+cudaError_t ctx_aux_init(cs_ctx* ctx) {
+  if (ctx->aux_ready) return cudaSuccess;
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 4 && e == cudaSuccess; i++)
+    if (!ctx->aux[i]) e = cudaStreamCreateWithFlags(&ctx->aux[i], cudaStreamNonBlocking);
+  for (int i = 0; i < 8 && e == cudaSuccess; i++)
+    if (!ctx->aux_ev[i]) e = cudaEventCreateWithFlags(&ctx->aux_ev[i], cudaEventDisableTiming);
+  if (e == cudaSuccess) ctx->aux_ready = true;
+  return e;
+}
+
 int fail(cs_ctx* ctx, cudaError_t e, const char* where) {
   if (ctx) ctx->err = std::string(where) + ": " + cudaGetErrorString(e);
   cudaGetLastError();  // clear the sticky-free error state
@@ -138,6 +149,10 @@ void cs_ctx_destroy(cs_ctx* ctx) {
   if (ctx->ev_phase0) cudaEventDestroy(ctx->ev_phase0);
   if (ctx->ev_phase1) cudaEventDestroy(ctx->ev_phase1);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  for (int i = 0; i < 4; i++)
+    if (ctx->aux[i]) { cudaStreamSynchronize(ctx->aux[i]); cudaStreamDestroy(ctx->aux[i]); }
+  for (int i = 0; i < 8; i++)
+    if (ctx->aux_ev[i]) cudaEventDestroy(ctx->aux_ev[i]);
   delete ctx;
 }
 

@@ -132,6 +132,10 @@ cudaError_t domain_get(cs_ctx* ctx, uint32_t L, Domain** out) {
   return cudaSuccess;
 }
 
+const uint32_t* domain_wf(const Domain* d) { return d->Wf; }
+const uint32_t* domain_wi(const Domain* d) { return d->Wi; }
+const uint32_t* domain_consts(const Domain* d) { return d->consts; }
+
 // ----------------------------------------------------------------- H step cores -----
 // Reference semantics (src/cuda/ntt.cpp:778 interpol_and_mul_h): A, B evaluations on the
 // m-th roots (Montgomery) -> the 2m coefficients of A(x)B(x) in normal form.

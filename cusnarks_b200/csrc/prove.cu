@@ -1,0 +1,329 @@
+// prove.cu -- device-resident proving key and the Groth16 prove pipeline.
+//
+// Follows the reference's CPU proving sequence (src/python/groth_prover.py:575-790
+// pysnarkP_CPU and :1414-1453 in gen_proof):
+//   pA = A.w, pB = B.w on the domain (mpoly_eval)       -> QAP rows (qap.cu)
+//   M  = coefficients of A(x)B(x)                       -> H step, reference variant
+//   polH = M[m .. 2m-2]
+//   pi_A  = MSM(w ++ [1, r], A ++ [alpha_1, delta_1])   (G1)
+//   pi_B  = MSM(w ++ [1, s], B2 ++ [beta_2, delta_2])   (G2)
+//   pi_B1 = MSM(w ++ [1, s], B1 ++ [beta_1, delta_1])   (G1)
+//   pi_C  = MSM(w[nPub+1 : nVars], C[nPub+1 : nVars])   (G1)
+//   pi_C2 = MSM(polH ++ [-r s], hExps[0 .. m-2] ++ [delta_1])
+//   pi_C <- pi_C2 + pi_C + s pi_A + r pi_B1
+// The four witness MSMs run on separate streams and overlap the QAP/H-step chain; the
+// scalings s pi_A and r pi_B1 start as soon as their MSM finishes.
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/cusnarks_b200.h"
+#include "curve.cuh"
+#include "msm.cuh"
+#include "ntt.cuh"
+#include "qap.cuh"
+#include "runtime.cuh"
+
+namespace csb {
+struct Domain;
+cudaError_t domain_get(cs_ctx* ctx, uint32_t L, Domain** out);
+cudaError_t hstep_reference_core(const uint32_t* A, const uint32_t* B, uint32_t L, const uint32_t* Wf2,
+                                 const uint32_t* Wi2, const uint32_t* shift, const uint32_t* minv_R,
+                                 const uint32_t* m2inv, uint32_t* out, uint32_t* scratch, cudaStream_t st);
+// accessors into the opaque Domain (hstep.cu)
+const uint32_t* domain_wf(const Domain* d);
+const uint32_t* domain_wi(const Domain* d);
+const uint32_t* domain_consts(const Domain* d);
+}  // namespace csb
+
+using namespace csb;
+
+struct cs_pk {
+  int device = 0;
+  uint32_t n_vars = 0, n_public = 0, m = 0, log_m = 0;
+  QapRows rows_a, rows_b;
+  uint32_t* a_ext = nullptr;   // nVars+2 G1
+  uint32_t* b1_ext = nullptr;  // nVars+2 G1
+  uint32_t* b2_ext = nullptr;  // nVars+2 G2
+  uint32_t* c = nullptr;       // nVars G1
+  uint32_t* h_ext = nullptr;   // m G1: hExps[0..m-2] ++ delta_1
+  std::vector<void*> owned;
+  ~cs_pk() {
+    for (void* p : owned) cudaFree(p);
+  }
+  cudaError_t alloc(void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 256);
+    if (e == cudaSuccess) owned.push_back(*p);
+    return e;
+  }
+};
+
+namespace {
+
+inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// scalars[n] = 1, scalars[n+1] = x (normal form)
+__global__ void k_set_tail(uint32_t* __restrict__ scalars, uint32_t n, const uint32_t* __restrict__ x) {
+  const int t = threadIdx.x;
+  if (t < 8) {
+    scalars[(size_t)n * 8 + t] = t == 0 ? 1u : 0u;
+    scalars[(size_t)(n + 1) * 8 + t] = x[t];
+  }
+}
+
+// dst = -(r s) mod r_field, normal form (the reference's montmult_neg_h(r_mont, s))
+__global__ void k_neg_rs(const uint32_t* __restrict__ r, const uint32_t* __restrict__ s, uint32_t* __restrict__ dst) {
+  if (threadIdx.x != 0) return;
+  const Fr rm = ld_fp<ModR>(r).to_mont();
+  st_fp<ModR>(dst, Fr::zero() - rm * ld_fp<ModR>(s));
+}
+
+// out (XYZZ) = k * P (affine), left-to-right double-and-add over 256 bits
+template <class F>
+__global__ void k_scale_point(const uint32_t* __restrict__ P, const uint32_t* __restrict__ k,
+                              uint32_t* __restrict__ out) {
+  if (threadIdx.x != 0) return;
+  uint32_t kk[8];
+  for (int i = 0; i < 8; i++) kk[i] = k[i];
+  const Affine<F> p = ld_affine<F>(P);
+  XYZZ<F> acc = XYZZ<F>::inf();
+  if (!affine_is_inf(p)) {
+    for (int b = 255; b >= 0; b--) {
+      acc = xyzz_dbl_cold(acc);
+      if ((kk[b >> 5] >> (b & 31)) & 1u) acc = xyzz_add_cold(acc, XYZZ<F>::from_affine(p));
+    }
+  }
+  st_xyzz<F>(out, acc);
+}
+
+// pi_C = C2 + C + sA + rB1 (C2, C affine; sA, rB1 XYZZ) -> affine
+__global__ void k_final_c(const uint32_t* __restrict__ c2, const uint32_t* __restrict__ c,
+                          const uint32_t* __restrict__ sa, const uint32_t* __restrict__ rb1,
+                          uint32_t* __restrict__ out) {
+  if (threadIdx.x != 0) return;
+  XYZZ<Fq> acc = XYZZ<Fq>::inf();
+  const Affine<Fq> a = ld_affine<Fq>(c2), b = ld_affine<Fq>(c);
+  if (!affine_is_inf(a)) acc = xyzz_madd(acc, a);
+  if (!affine_is_inf(b)) acc = xyzz_madd(acc, b);
+  acc = xyzz_add(acc, ld_xyzz<Fq>(sa));
+  acc = xyzz_add(acc, ld_xyzz<Fq>(rb1));
+  st_affine<Fq>(out, xyzz_to_affine(acc));
+}
+
+cudaError_t copy_in(void* dst, const void* src, size_t bytes, int on_device, cudaStream_t st) {
+  if (!bytes) return cudaSuccess;
+  return cudaMemcpyAsync(dst, src, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st);
+}
+
+uint32_t ilog2_exact(uint32_t m) {
+  uint32_t l = 0;
+  while ((1u << l) < m) l++;
+  return (1u << l) == m ? l : 0xffffffffu;
+}
+
+// Layout of the per-call prove scratch.
+struct ProvePlan {
+  size_t wA, wB, pA, pB, M, hscr, ms_a, ms_b1, ms_b2, ms_c, ms_h, pts, rs, total;
+  size_t bytes_a, bytes_b1, bytes_b2, bytes_c, bytes_h;
+};
+
+ProvePlan plan_prove(const cs_pk* pk) {
+  ProvePlan P{};
+  const size_t nv = pk->n_vars, m = pk->m;
+  const uint32_t nc = pk->n_vars - pk->n_public - 1;
+  P.bytes_a = msm_workspace_bytes(pk->n_vars + 2, 0, false);
+  P.bytes_b1 = P.bytes_a;
+  P.bytes_b2 = msm_workspace_bytes(pk->n_vars + 2, 0, true);
+  P.bytes_c = msm_workspace_bytes(nc, 0, false);
+  P.bytes_h = msm_workspace_bytes(pk->m, 0, false);
+  size_t o = 0;
+  P.wA = o; o += al256((nv + 2) * 32);
+  P.wB = o; o += al256((nv + 2) * 32);
+  P.pA = o; o += al256(m * 32);
+  P.pB = o; o += al256(m * 32);
+  P.M = o; o += al256(2 * m * 32);
+  P.hscr = o; o += al256(4 * m * 32);
+  P.ms_a = o; o += al256(P.bytes_a);
+  P.ms_b1 = o; o += al256(P.bytes_b1);
+  P.ms_b2 = o; o += al256(P.bytes_b2);
+  P.ms_c = o; o += al256(P.bytes_c);
+  P.ms_h = o; o += al256(P.bytes_h);
+  P.pts = o; o += 2048;   // outA 64, outB1 64, outB2 128, outC 64, outH 64, sA 128, rB1 128, piC 64
+  P.rs = o; o += 256;     // r, s, -rs
+  P.total = o;
+  return P;
+}
+
+}  // namespace
+
+namespace csb {
+size_t prove_workspace_bytes(const cs_pk* pk) { return plan_prove(pk).total; }
+}  // namespace csb
+
+extern "C" {
+
+int cs_pk_create(cs_ctx* ctx, const cs_pk_desc* d, int on_device, cs_pk** out) {
+  if (!ctx || !d || !out) return CS_ERR_ARG;
+  *out = nullptr;
+  if (d->n_vars < d->n_public + 2 || !d->polsA || !d->polsB || !d->A || !d->B1 || !d->B2 || !d->C ||
+      !d->hExps || !d->delta_1)
+    return fail_msg(ctx, CS_ERR_ARG, "cs_pk_create: incomplete proving key description");
+  const uint32_t L = ilog2_exact(d->domain_size);
+  if (L == 0xffffffffu || L < 2 || L > 26) return fail_msg(ctx, CS_ERR_ARG, "cs_pk_create: domain size must be 2^k, 4 <= 2^k <= 2^26");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  std::unique_ptr<cs_pk> pk(new cs_pk());
+  pk->device = ctx->device;
+  pk->n_vars = d->n_vars;
+  pk->n_public = d->n_public;
+  pk->m = d->domain_size;
+  pk->log_m = L;
+  const size_t nv = d->n_vars, m = d->domain_size;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  // points
+  if ((e = pk->alloc((void**)&pk->a_ext, (nv + 2) * 64)) != cudaSuccess ||
+      (e = pk->alloc((void**)&pk->b1_ext, (nv + 2) * 64)) != cudaSuccess ||
+      (e = pk->alloc((void**)&pk->b2_ext, (nv + 2) * 128)) != cudaSuccess ||
+      (e = pk->alloc((void**)&pk->c, nv * 64)) != cudaSuccess ||
+      (e = pk->alloc((void**)&pk->h_ext, m * 64)) != cudaSuccess)
+    return fail(ctx, e, "cs_pk_create: point buffers");
+  if ((e = copy_in(pk->a_ext, d->A, (nv + 2) * 64, on_device, st)) != cudaSuccess ||
+      (e = copy_in(pk->b1_ext, d->B1, (nv + 2) * 64, on_device, st)) != cudaSuccess ||
+      (e = copy_in(pk->b2_ext, d->B2, (nv + 2) * 128, on_device, st)) != cudaSuccess ||
+      (e = copy_in(pk->c, d->C, nv * 64, on_device, st)) != cudaSuccess ||
+      (e = copy_in(pk->h_ext, d->hExps, (m - 1) * 64, on_device, st)) != cudaSuccess ||
+      (e = copy_in(pk->h_ext + (m - 1) * 16, d->delta_1, 64, on_device, st)) != cudaSuccess)
+    return fail(ctx, e, "cs_pk_create: point upload");
+  // QAP matrices: reference mpoly layout -> constraint rows
+  for (int which = 0; which < 2; which++) {
+    const uint32_t* pm = which == 0 ? d->polsA : d->polsB;
+    const size_t words = which == 0 ? d->polsA_words : d->polsB_words;
+    const uint32_t n_entries = which == 0 ? d->polsA_entries : d->polsB_entries;
+    QapRows& R = which == 0 ? pk->rows_a : pk->rows_b;
+    uint32_t* dm = nullptr;
+    if ((e = cudaMalloc(&dm, words * 4)) != cudaSuccess) return fail(ctx, e, "cs_pk_create: mpoly");
+    e = copy_in(dm, pm, words * 4, on_device, st);
+    if (e == cudaSuccess) e = pk->alloc((void**)&R.row_off, (m + 1) * 4);
+    if (e == cudaSuccess) e = pk->alloc((void**)&R.wire, (size_t)n_entries * 4);
+    if (e == cudaSuccess) e = pk->alloc((void**)&R.coeff, (size_t)n_entries * 32);
+    void* scratch = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&scratch, qap_transpose_scratch_bytes(d->n_vars, (uint32_t)m, n_entries));
+    if (e == cudaSuccess) e = qap_transpose(dm, d->n_vars, n_entries, 0, d->n_vars, (uint32_t)m, R, scratch, st);
+    R.n_entries = n_entries;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(scratch);
+    cudaFree(dm);
+    if (e != cudaSuccess) return fail(ctx, e, "cs_pk_create: QAP transpose");
+  }
+  Domain* dom = nullptr;
+  if ((e = domain_get(ctx, L + 1, &dom)) != cudaSuccess) return fail(ctx, e, "cs_pk_create: NTT tables");
+  if ((e = domain_get(ctx, L, &dom)) != cudaSuccess) return fail(ctx, e, "cs_pk_create: NTT tables");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(ctx, e, "cs_pk_create: sync");
+  *out = pk.release();
+  return CS_OK;
+}
+
+void cs_pk_destroy(cs_pk* pk) { delete pk; }
+
+size_t cs_prove_workspace_bytes(const cs_pk* pk) { return pk ? plan_prove(pk).total : 0; }
+
+int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t* r, const uint32_t* s,
+                    uint32_t* d_proof) {
+  if (!ctx || !pk || !d_w || !r || !s || !d_proof) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaError_t e = ctx_aux_init(ctx);
+  if (e != cudaSuccess) return fail(ctx, e, "prove streams");
+  const ProvePlan P = plan_prove(pk);
+  if ((e = ctx->work.reserve(P.total, ctx->stream)) != cudaSuccess) return fail(ctx, e, "prove workspace");
+  char* base = static_cast<char*>(ctx->work.ptr);
+  auto at = [&](size_t off) { return reinterpret_cast<uint32_t*>(base + off); };
+  uint32_t *wA = at(P.wA), *wB = at(P.wB), *pA = at(P.pA), *pB = at(P.pB), *M = at(P.M), *hscr = at(P.hscr);
+  uint32_t* pts = at(P.pts);
+  uint32_t *outA = pts, *outB1 = pts + 16, *outB2 = pts + 32, *outC = pts + 64, *outH = pts + 80;
+  uint32_t *sA = pts + 96, *rB1 = pts + 128, *piC = pts + 160;
+  uint32_t* rs = at(P.rs);
+  const uint32_t nv = pk->n_vars, m = pk->m, np1 = pk->n_public + 1;
+  cudaStream_t s0 = ctx->stream;
+  cudaEvent_t ev_w = ctx->aux_ev[0];
+  Domain *dom2 = nullptr, *dom1 = nullptr;
+  if ((e = domain_get(ctx, pk->log_m + 1, &dom2)) != cudaSuccess || (e = domain_get(ctx, pk->log_m, &dom1)) != cudaSuccess)
+    return fail(ctx, e, "prove tables");
+  MsmConfig cfg;
+  cudaEventRecord(ctx->ev_start, s0);
+  // scalars: w ++ [1, r] and w ++ [1, s]; r, s, -rs
+  bool ok = (e = cudaMemcpyAsync(rs, r, 32, cudaMemcpyHostToDevice, s0)) == cudaSuccess &&
+            (e = cudaMemcpyAsync(rs + 8, s, 32, cudaMemcpyHostToDevice, s0)) == cudaSuccess &&
+            (e = cudaMemcpyAsync(wA, d_w, (size_t)nv * 32, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess &&
+            (e = cudaMemcpyAsync(wB, d_w, (size_t)nv * 32, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess;
+  if (!ok) return fail(ctx, e, "prove inputs");
+  k_set_tail<<<1, 32, 0, s0>>>(wA, nv, rs);
+  k_set_tail<<<1, 32, 0, s0>>>(wB, nv, rs + 8);
+  k_neg_rs<<<1, 32, 0, s0>>>(rs, rs + 8, rs + 16);
+  note_launch(3);
+  cudaEventRecord(ev_w, s0);
+  // witness MSMs on the auxiliary streams
+  cudaStream_t sa = ctx->aux[0], sb1 = ctx->aux[1], sb2 = ctx->aux[2], sc = ctx->aux[3];
+  for (int i = 0; i < 4; i++) cudaStreamWaitEvent(ctx->aux[i], ev_w, 0);
+  ok = (e = msm_g1(wA, pk->a_ext, nv + 2, outA, at(P.ms_a), P.bytes_a, cfg, sa)) == cudaSuccess &&
+       (e = msm_g1(wB, pk->b1_ext, nv + 2, outB1, at(P.ms_b1), P.bytes_b1, cfg, sb1)) == cudaSuccess &&
+       (e = msm_g2(wB, pk->b2_ext, nv + 2, outB2, at(P.ms_b2), P.bytes_b2, cfg, sb2)) == cudaSuccess &&
+       (e = msm_g1(wA + (size_t)np1 * 8, pk->c + (size_t)np1 * 16, nv - np1, outC, at(P.ms_c), P.bytes_c, cfg, sc)) ==
+           cudaSuccess;
+  if (!ok) return fail(ctx, e, "prove witness MSMs");
+  k_scale_point<Fq><<<1, 32, 0, sa>>>(outA, rs + 8, sA);   // s * pi_A
+  k_scale_point<Fq><<<1, 32, 0, sb1>>>(outB1, rs, rB1);    // r * pi_B1
+  note_launch(2);
+  // QAP evaluation and H step on the main stream
+  ok = (e = qap_eval(pk->rows_a, d_w, pA, 0, s0)) == cudaSuccess &&
+       (e = qap_eval(pk->rows_b, d_w, pB, 0, s0)) == cudaSuccess &&
+       (e = hstep_reference_core(pA, pB, pk->log_m, domain_wf(dom2), domain_wi(dom2), domain_wf(dom2),
+                                 domain_consts(dom1) + 16, domain_consts(dom2) + 24, M, hscr, s0)) == cudaSuccess &&
+       // polH = M[m .. 2m-2]; M[2m-1] (always zero) becomes the -rs term for delta_1
+       (e = cudaMemcpyAsync(M + (size_t)(2 * m - 1) * 8, rs + 16, 32, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess &&
+       (e = msm_g1(M + (size_t)m * 8, pk->h_ext, m, outH, at(P.ms_h), P.bytes_h, cfg, s0)) == cudaSuccess;
+  if (!ok) return fail(ctx, e, "prove QAP/H");
+  for (int i = 0; i < 4; i++) {
+    cudaEventRecord(ctx->aux_ev[1 + i], ctx->aux[i]);
+    cudaStreamWaitEvent(s0, ctx->aux_ev[1 + i], 0);
+  }
+  k_final_c<<<1, 32, 0, s0>>>(outH, outC, sA, rB1, piC);
+  note_launch();
+  // proof = pi_A (16) | pi_B (32) | pi_C (16), affine Montgomery
+  ok = (e = cudaMemcpyAsync(d_proof, outA, 64, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess &&
+       (e = cudaMemcpyAsync(d_proof + 16, outB2, 128, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess &&
+       (e = cudaMemcpyAsync(d_proof + 48, piC, 64, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess;
+  cudaEventRecord(ctx->ev_stop, s0);
+  if (!ok) return fail(ctx, e, "prove output");
+  if ((e = cudaGetLastError()) != cudaSuccess) return fail(ctx, e, "prove launch");
+  return CS_OK;
+}
+
+int cs_prove(cs_ctx* ctx, cs_pk* pk, const uint32_t* w, const uint32_t* r, const uint32_t* s, uint32_t* proof) {
+  if (!ctx || !pk || !w || !proof) return CS_ERR_ARG;
+  cudaError_t e;
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if ((e = ctx->in.reserve((size_t)pk->n_vars * 32 + 512, ctx->stream)) != cudaSuccess)
+      return fail(ctx, e, "prove witness buffer");
+    if ((e = cudaMemcpyAsync(ctx->in.ptr, w, (size_t)pk->n_vars * 32, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+      return fail(ctx, e, "prove witness upload");
+  }
+  uint32_t* d_w = static_cast<uint32_t*>(ctx->in.ptr);
+  uint32_t* d_proof = d_w + (size_t)pk->n_vars * 8;
+  int st = cs_prove_device(ctx, pk, d_w, r, s, d_proof);
+  if (st != CS_OK) return st;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if ((e = cudaMemcpyAsync(proof, d_proof, 64 * 4, cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess)
+    return fail(ctx, e, "prove download");
+  if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(ctx, e, "prove sync");
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
+  return CS_OK;
+}
+
+}  // extern "C"

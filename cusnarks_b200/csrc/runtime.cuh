@@ -74,9 +74,15 @@ struct cs_ctx {
   bool phase_valid = false;
   std::string err;
   std::mutex mu;               // one call at a time per context
+  // auxiliary streams / events for fork-join pipelines (prove), created on first use
+  cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t aux_ev[8] = {nullptr};
+  bool aux_ready = false;
 };
 
 namespace csb {
+// Creates the context's auxiliary streams and events (idempotent).
+cudaError_t ctx_aux_init(cs_ctx* ctx);
 // Counts kernel launches made by this library (cs_kernel_launches()).
 void note_launch(unsigned n = 1);
 // Records a CUDA error on the context and maps it to the C ABI status code.

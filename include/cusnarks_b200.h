@@ -77,6 +77,19 @@ typedef struct {
   uint32_t thread_id;
 } ntt_interpolandmul_t;
 
+/* mpoly_eval_t, reference src/cuda/types.h:516-528. */
+typedef struct {
+  uint32_t *pout;
+  const uint32_t *scalar;
+  uint32_t *pin;
+  uint32_t reduce_coeff;
+  uint32_t start_idx;
+  uint32_t last_idx;
+  uint32_t max_threads;
+  uint32_t thread_id;
+  uint32_t pidx;
+} mpoly_eval_t;
+
 /* ------------------------------------------------ drop-in reference entry points --- */
 /* Replaces ec_jacreduce_server_h, reference src/cuda/ec.cpp:1536 (bound at
  * src/cython/_utils_host.pxd:139).  out_ep <- sum_i scl[i] * x[i] as affine Montgomery
@@ -127,6 +140,15 @@ uint32_t *ntt_interpolandmul_server_h(ntt_interpolandmul_t *args);
 /* Replaces get_Mtranspose_h, reference src/cuda/ntt.cpp:659: the last H-step result. */
 uint32_t *get_Mtranspose_h(void);
 int cs_ntt_last_status(void);
+
+/* QAP evaluation.  Replaces mpoly_eval_server_h, reference src/cuda/mpoly.cpp:67
+ * (_utils_host.pxd:207), and mpoly_eval_h, mpoly.cpp:125: pout[c] += toMont(scalar[i]) *
+ * coeff for every (c, coeff) of the polynomials i in [start_idx, last_idx) of the
+ * reference mpoly layout pin (mpoly.cpp:195).  Deterministic (no racing threads); pidx
+ * must be 1.  Status in cs_qap_last_status(). */
+void mpoly_eval_server_h(mpoly_eval_t *args);
+void *mpoly_eval_h(void *args);
+int cs_qap_last_status(void);
 
 /* Status of the last drop-in call made by this thread, and its message. */
 int cs_last_status(void);
@@ -220,6 +242,62 @@ int cs_msm_g1_noalloc(const uint32_t *d_scalars, const uint32_t *d_points, uint3
 size_t cs_msm_noalloc_scratch_bytes(void);
 uint32_t cs_msm_g1_noalloc_max_terms(void);
 const char *cs_msm_g1_noalloc_error(void);
+
+/* --------------------------------------------------------------- Groth16 prove ----- */
+/* Proving key as the reference stores it (src/python/pysnarks_utils.py pkvars_to_bin with
+ * the extension of :653-657), Montgomery affine points:
+ *   A, B1: n_vars + 2 G1 points (A ++ alpha_1 ++ delta_1, B1 ++ beta_1 ++ delta_1),
+ *   B2: n_vars + 2 G2 points (B2 ++ beta_2 ++ delta_2), C: n_vars G1 points (entries below
+ *   n_public + 1 unused), hExps: domain_size - 1 G1 points, delta_1: one G1 point,
+ *   polsA / polsB: QAP matrices in the mpoly layout (polsA extended with the public rows). */
+typedef struct {
+  uint32_t n_vars, n_public, domain_size;
+  const uint32_t *polsA; size_t polsA_words; uint32_t polsA_entries;
+  const uint32_t *polsB; size_t polsB_words; uint32_t polsB_entries;
+  const uint32_t *A, *B1, *B2, *C, *hExps, *delta_1;
+} cs_pk_desc;
+typedef struct cs_pk cs_pk;
+
+/* Uploads (on_device = 0: host pointers) or copies (1: device pointers) the key into HBM,
+ * transposes the QAP matrices into constraint rows and builds the NTT tables; the key
+ * then serves any number of proofs. */
+int cs_pk_create(cs_ctx *ctx, const cs_pk_desc *desc, int on_device, cs_pk **out);
+void cs_pk_destroy(cs_pk *pk);
+size_t cs_prove_workspace_bytes(const cs_pk *pk);
+/* Groth16 proof for witness w (n_vars normal-form elements, w[0] = 1), blinding r and s
+ * (normal form, host pointers): proof = pi_A (16 words) | pi_B (32) | pi_C (16), affine
+ * Montgomery, the reference prover's pi_a_eccf1 / pi_b_eccf2 / pi_c_eccf1
+ * (groth_prover.py:1245 gen_proof; CPU sequence :575-790 and :1414-1453).
+ * cs_prove: host witness and proof, synchronous.  cs_prove_device: device witness and
+ * proof buffers, asynchronous on the context stream (r and s are read at call time). */
+int cs_prove(cs_ctx *ctx, cs_pk *pk, const uint32_t *w, const uint32_t *r, const uint32_t *s,
+             uint32_t *proof);
+int cs_prove_device(cs_ctx *ctx, cs_pk *pk, const uint32_t *d_w, const uint32_t *r, const uint32_t *s,
+                    uint32_t *d_proof);
+
+/* ------------------------------------------- proving-key generation (setup) -------- */
+/* Device kernels for building proving keys (the quantities of the reference's
+ * groth_setup.py calculateValuesAtT :771 / calculateEncryptedValuesAtT :488); all Fr
+ * values Montgomery unless noted, device pointers, asynchronous on the context stream.
+ *   cs_setup_lagrange:   out[c] = L_c(t) = w^c (t^m - 1) / (m (t - w^c)), c < m = 2^log_m.
+ *   cs_setup_wire_eval:  out[i] = sum_c M[i][c] L[c] for the mpoly-layout matrix M (rows of
+ *                        index >= n_rows ignored), i.e. u_i(t) / v_i(t) / w_i(t).
+ *   cs_setup_c_scalars:  out[i] = (beta u_i + alpha v_i + w_i) k, normal form (k = 1/delta
+ *                        for C, 1/gamma for the verifying key's IC).
+ *   cs_setup_pow_scalars: out[j] = t^j k, j < n, normal form (k = Z(t)/delta: hExps).
+ *   cs_r1cs_layer_eval:  out[c] = (A_c . w)(B_c . w), normal form, for CSR rows with
+ *                        Montgomery coefficients and a normal-form witness (evaluates the
+ *                        outputs of one layer of a synthetic circuit). */
+int cs_setup_lagrange(cs_ctx *ctx, uint32_t log_m, const uint32_t *d_t, uint32_t *d_out);
+int cs_setup_wire_eval(cs_ctx *ctx, const uint32_t *d_mpoly, uint32_t n_wires, const uint32_t *d_L,
+                       uint32_t n_rows, uint32_t *d_out);
+int cs_setup_c_scalars(cs_ctx *ctx, const uint32_t *d_u, const uint32_t *d_v, const uint32_t *d_w,
+                       const uint32_t *d_alpha, const uint32_t *d_beta, const uint32_t *d_k, uint32_t n,
+                       uint32_t *d_out);
+int cs_setup_pow_scalars(cs_ctx *ctx, const uint32_t *d_t, const uint32_t *d_k, uint32_t n, uint32_t *d_out);
+int cs_r1cs_layer_eval(cs_ctx *ctx, const uint32_t *a_off, const uint32_t *a_wire, const uint32_t *a_coeff,
+                       const uint32_t *b_off, const uint32_t *b_wire, const uint32_t *b_coeff, uint32_t n_rows,
+                       const uint32_t *d_w, uint32_t *d_out);
 
 /* ------------------------------------------------------------ measurement ----------- */
 /* Sustained 32-bit integer multiply-add instruction rate of the context's device

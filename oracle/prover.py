@@ -1,0 +1,68 @@
+"""CPU restatement of the reference's Groth16 proving sequence, and proof verification.
+
+TEST INFRASTRUCTURE ONLY.  ``cpu_prove`` follows src/python/groth_prover.py pysnarkP_CPU
+(:575-790: mpoly_eval of A and B, ntt_interpolandmul, the five multi-exponentiations with
+the extension scalars [1, r], [1, s], [-rs]) and the final combination of gen_proof
+(:1414-1453: pi_C = pi_C2 + pi_C + s pi_A + r pi_B1), calling the oracle's restatements of
+the reference routines (cs_oracle.c).  ``verify`` checks the Groth16 pairing equation
+with oracle/bn254.py.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .oracle import Oracle, ints_to_limbs, limbs_to_int, from_mont_int, R
+from . import bn254
+
+
+def _ext(a: np.ndarray, rows) -> np.ndarray:
+    return np.concatenate([np.asarray(a, dtype=np.uint32).reshape(-1, 8), ints_to_limbs(rows)])
+
+
+def cpu_prove(o: Oracle, pk: dict, w: np.ndarray, r: int, s: int, order: int = 6) -> np.ndarray:
+    """pk: host arrays as cusnarks_b200.groth.pk_to_host returns them.  Returns 64 words:
+    pi_A | pi_B | pi_C, affine Montgomery."""
+    nv, npub, m = pk["n_vars"], pk["n_public"], pk["domain_size"]
+    L = m.bit_length() - 1
+    w = np.ascontiguousarray(w, dtype=np.uint32).reshape(-1, 8)
+    pA = o.mpoly_eval(w[:nv], pk["polsA"], m, 0, nv, 1)
+    pB = o.mpoly_eval(w[:nv], pk["polsB"], m, 0, nv, 1)
+    roots = o.find_roots(L + 1)
+    M = o.interpolandmul(pA, pB, roots, L, 2)
+    polH = M[m:2 * m - 1]
+    neg_rs = (-(r * s)) % R
+    pi_a = o.msm(_ext(w[:nv], [1, r]), pk["A"][:nv + 2], 0, order)
+    pi_b = o.msm(_ext(w[:nv], [1, s]), pk["B2"][:nv + 2], 1, order)
+    pi_b1 = o.msm(_ext(w[:nv], [1, s]), pk["B1"][:nv + 2], 0, order)
+    pi_c = o.msm(w[npub + 1:nv], pk["C"][npub + 1:nv], 0, order)
+    hpts = np.concatenate([pk["hExps"][:m - 1].reshape(-1, 16), pk["delta_1"].reshape(-1, 16)])
+    pi_c2 = o.msm(_ext(polH, [neg_rs]), hpts, 0, order)
+    fin_s = ints_to_limbs([1, 1, s, r])
+    fin_p = np.stack([pi_c2, pi_c, pi_a, pi_b1])
+    pi_c = o.msm(fin_s, fin_p, 0, 2)
+    return np.concatenate([pi_a, pi_b, pi_c]).astype(np.uint32)
+
+
+def _g1(words):
+    x, y = (from_mont_int(limbs_to_int(words[i * 8:(i + 1) * 8]), 0) for i in range(2))
+    one = from_mont_int((1 << 256) % bn254.Q, 0)
+    if x == 0 and y == 1:
+        return None
+    return (x, y)
+
+
+def _g2(words):
+    v = [from_mont_int(limbs_to_int(words[i * 8:(i + 1) * 8]), 0) for i in range(4)]
+    if v[0] == 0 and v[1] == 0 and v[2] == 1 and v[3] == 0:
+        return None
+    return ((v[0], v[1]), (v[2], v[3]))
+
+
+def verify(vk: dict, proof: np.ndarray, public_inputs) -> bool:
+    """vk with affine Montgomery arrays (alpha_1, beta_2, gamma_2, delta_2, IC rows);
+    proof = 64 words pi_A | pi_B | pi_C; public_inputs: normal-form limbs (n_public x 8)."""
+    vkp = {"alpha_1": _g1(vk["alpha_1"]), "beta_2": _g2(vk["beta_2"]), "gamma_2": _g2(vk["gamma_2"]),
+           "delta_2": _g2(vk["delta_2"]), "IC": [_g1(row) for row in np.asarray(vk["IC"]).reshape(-1, 16)]}
+    pr = {"A": _g1(proof[:16]), "B": _g2(proof[16:48]), "C": _g1(proof[48:64])}
+    pub = [1] + [limbs_to_int(row) for row in np.asarray(public_inputs).reshape(-1, 8)]
+    return bn254.groth16_verify(vkp, pr, pub)
