@@ -1,21 +1,29 @@
 #!/usr/bin/env python
 """Benchmark of the Groth16/BN128 prover hot path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload msm|prove]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--no-cpu]
 
 Prints ONE JSON line (rank 0).  Under torchrun (N > 1) every rank runs its own replica of
-the workload (proofs and multi-exponentiations are independent: no data-path
-collective); the timed region is bracketed by barriers, device time is the max over
-ranks, and ``value`` is the total over all ranks.
+the workload (proofs are independent: no data-path collective); the timed region is
+bracketed by barriers, device time is the max over ranks, and ``value`` is the total over
+all ranks (weak scaling).
 
-Workload "msm": BN128 G1 multi-exponentiation, N = 2^20 terms, scalars uniform in Fr
-(seeded), base points k_i * G1 (seeded k_i, generated on the GPU), inputs resident in HBM.
-One step = one MSM.  value = MSMs per second (all GPUs); g1_msm_2^20_ms = device ms.
+Workload (the configuration the headline metric is quoted on): full Groth16 prove for a
+synthetic R1CS of 2^20 constraints (nConstraints = 2^20 - 2, one public input, A and B rows
+with 3 nonzeros at random wires with uniform random Fr coefficients, C row = one output wire
+set to (A.w)(B.w)); proving key from seeded toxic waste, resident in HBM; fixed r, s.
+One step = one proof from a device-resident witness; device time from CUDA events around
+the whole proof.  Also reported: one BN128 G1 MSM of 2^20 terms (``g1_msm_2^20_ms``), whose
+bucket-accumulation kernel -- the dominant kernel of every proof -- carries the roofline.
 
-``--impl reference`` times the reference's own CPU multi-exp (oracle/_ref, built from
-the reference sources; the C restatement in oracle/ when that library is absent) on all
-host cores, on bounded 2^16-term samples scaled to the same unit.
+``e2e`` goes through the public C ABI (cs_prove) with the witness in pinned host memory and
+the proof copied back, wall clock per proof.
+
+``cpu_baseline`` / ``--impl reference``: the reference's own CPU library (oracle/_ref,
+built from the reference sources; the C restatement when that library is absent) runs the
+reference's proving sequence on all host cores for a 2^16-constraint sample of the same
+circuit family; the time is scaled x16 to the 2^20 unit (every step of the sequence is
+linear or N log N in the size; the scale is stated in the line).
 """
 from __future__ import annotations
 
@@ -34,19 +42,11 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 METRIC = "Groth16 proofs/s + p50/p99 latency, 2^20 G1 MSM ms; served vs plain, 1 B200"
-IMAD_PER_MONT = 264   # CIOS, 8x32-bit limbs: 8 rows x (16 a*b + 16 m*p + 1 m) mad.lo/mad.hi
+UNIT = "proofs/s (2^20 constraints)"
+IMAD_PER_MONT = 264   # CIOS, 8x32-bit limbs: 8 rows x (16 a*b + 16 m*p + 1 m) multiply-adds
 L2_BYTES = 126 * 1024 * 1024
-
-
-def survey_msm_mults(n: int, ec2: bool = False) -> float:
-    """Implementation-independent Montgomery-product count of one MSM:
-    c = max(8, log2 N - 4), w = ceil(256/c), B = 2^(c-1), w*(11 N + 32 B); x3 for G2."""
-    import math
-    c = max(8, int(math.log2(max(n, 2))) - 4)
-    w = -(-256 // c)
-    B = 1 << (c - 1)
-    m = w * (11 * n + 16 * 2 * B)
-    return 3.0 * m if ec2 else float(m)
+LOG_M = 20
+CPU_SAMPLE_LOG_M = 16
 
 
 # ----------------------------------------------------------------- clocks sampler ---
@@ -61,7 +61,6 @@ class ClockSampler:
         self.dev = device_index
         self.proc = None
         self.lines = []
-        self.t = None
 
     def start(self):
         try:
@@ -72,8 +71,7 @@ class ClockSampler:
         except Exception:
             self.proc = None
             return
-        self.t = threading.Thread(target=self._read, daemon=True)
-        self.t.start()
+        threading.Thread(target=self._read, daemon=True).start()
 
     def _read(self):
         for line in self.proc.stdout:
@@ -116,7 +114,7 @@ def dist_setup():
         import torch.distributed as dist
         from datetime import timedelta
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     return world, rank, local
 
@@ -137,36 +135,78 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
+def pct(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = min(len(xs) - 1, max(0, int(round(q / 100.0 * (len(xs) - 1)))))
+    return xs[k]
+
+
 # ---------------------------------------------------------------- CPU reference ------
-def cpu_reference_msm(n: int, seed: int, repeats: int = 1):
-    """Time the reference CPU multi-exp on n terms (all host threads).  Returns
-    (seconds per MSM, kind, threads).  Inputs: same generators, computed on the CPU."""
+def cpu_reference_prove_sample(ctx, log_m: int, seed: int, repeats: int = 1):
+    """Seconds per proof of the reference's CPU proving sequence (oracle/_ref on all host
+    threads) on a 2^log_m-constraint circuit of the benchmark family.  The circuit and key
+    are generated with this library; only the CPU proving is timed."""
+    from cusnarks_b200.groth import SyntheticCircuit, setup_pk, pk_to_host
     from oracle.oracle import Oracle, RefLib
+    from oracle.prover import cpu_prove
+    circ = SyntheticCircuit(ctx, log_m, seed=seed)
+    pk = pk_to_host(setup_pk(ctx, circ, seed=seed + 1))
     o = Oracle()
-    rng = np.random.Generator(np.random.PCG64(seed))
-    from cusnarks_b200.synth import random_field, g1_generator
-    k = random_field(rng, n)
-    pts = o.scmul(k, g1_generator().reshape(1, -1), 0)
-    s = random_field(rng, n)
-    threads = os.cpu_count() or 1
-    if RefLib.available():
-        ref = RefLib.get()
-        fn = lambda: ref.msm(s, pts, 0, 6, 0)  # noqa: E731  reference defaults: order 6
-        kind = "reference"
-    else:
-        fn = lambda: o.msm(s, pts, 0, 6, 0)  # noqa: E731
-        kind = "port"
-    fn()
+    ref = RefLib.get() if RefLib.available() else None
+    cpu_prove(o, pk, circ.w, 1234567, 7654321, ref=ref)  # warm the caches / thread pools
     t0 = time.perf_counter()
     for _ in range(repeats):
-        fn()
-    return (time.perf_counter() - t0) / repeats, kind, threads
+        cpu_prove(o, pk, circ.w, 1234567, 7654321, ref=ref)
+    sec = (time.perf_counter() - t0) / repeats
+    return sec, ("reference" if ref else "port"), (os.cpu_count() or 1)
 
 
-# ----------------------------------------------------------------------- workload ---
+# ----------------------------------------------------------------------- workloads ---
+class ProveWorkload:
+    def __init__(self, ctx, log_m: int, seed: int):
+        import torch
+        from cusnarks_b200.groth import SyntheticCircuit, setup_pk, Prover
+        from cusnarks_b200.synth import to_limbs
+        self.torch = torch
+        self.ctx = ctx
+        self.circ = SyntheticCircuit(ctx, log_m, seed=seed)
+        self.pk = setup_pk(ctx, self.circ, seed=seed + 1)
+        self.prover = Prover(ctx, self.pk)
+        self.r, self.s = to_limbs(0x1234567890abcdef), to_limbs(0xfedcba0987654321)
+        dev = torch.device("cuda", ctx.device)
+        self.d_w = self.circ.d_w
+        self.d_proof = torch.zeros(64, dtype=torch.int32, device=dev)
+        self.h_w = torch.from_numpy(self.circ.w.view(np.int32)).pin_memory()
+        self.h_proof = torch.zeros(64, dtype=torch.int32).pin_memory()
+        self.flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()
+
+    def l2_flush(self):
+        self.flush.add_(1)
+        self.torch.cuda.synchronize()
+
+    def step(self) -> float:
+        self.prover.prove_device(self.d_w.data_ptr(), self.r, self.s, self.d_proof.data_ptr())
+        self.ctx.sync()
+        return self.ctx.last_ms
+
+    def e2e_step(self) -> float:
+        from cusnarks_b200._lib import lib, check
+        t0 = time.perf_counter()
+        check(lib().cs_prove(self.ctx.handle, self.prover.handle, self.h_w.data_ptr(), self.r.ctypes.data,
+                             self.s.ctypes.data, self.h_proof.data_ptr()), self.ctx.handle)
+        return (time.perf_counter() - t0) * 1e3
+
+    @property
+    def h2d_bytes(self):
+        return self.circ.n_vars * 32 + 64
+
+    d2h_bytes = 256
+
+
 class MsmWorkload:
-    name = "msm"
-
     def __init__(self, ctx, log_n: int, seed: int):
         import torch
         from cusnarks_b200.synth import random_field, g1_generator
@@ -174,26 +214,16 @@ class MsmWorkload:
         self.ctx = ctx
         self.n = 1 << log_n
         rng = np.random.Generator(np.random.PCG64(seed))
-        k = random_field(rng, self.n)
-        s = random_field(rng, self.n)
         dev = torch.device("cuda", ctx.device)
-        self.d_k = torch.from_numpy(k.view(np.int32)).to(dev)
-        self.d_s = torch.from_numpy(s.view(np.int32)).to(dev)
+        self.d_k = torch.from_numpy(random_field(rng, self.n).view(np.int32)).to(dev)
+        self.d_s = torch.from_numpy(random_field(rng, self.n).view(np.int32)).to(dev)
         g = torch.from_numpy(g1_generator().view(np.int32)).to(dev)
         self.d_p = torch.empty((self.n, 16), dtype=torch.int32, device=dev)
         self.d_out = torch.zeros(16, dtype=torch.int32, device=dev)
         torch.cuda.synchronize()
         ctx.scmul_device(self.d_k.data_ptr(), g.data_ptr(), self.n, self.d_p.data_ptr(), point_stride_words=0)
         ctx.sync()
-        # pinned host copies for the end-to-end leg
-        self.h_s = torch.from_numpy(s.view(np.int32)).pin_memory()
-        self.h_p = self.d_p.cpu().pin_memory()
-        self.h_out = torch.zeros(16, dtype=torch.int32).pin_memory()
-        self.flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=dev)
-
-    def l2_flush(self):
-        self.flush.add_(1)
-        self.torch.cuda.synchronize()
+        self.keep = g
 
     def step(self):
         self.ctx.msm_device(self.d_s.data_ptr(), self.d_p.data_ptr(), self.n, self.d_out.data_ptr())
@@ -201,30 +231,9 @@ class MsmWorkload:
         return self.ctx.last_ms, self.ctx.last_phase_ms
 
     def dominant_units(self):
-        """(window, bucket) entries one accumulation launch processes: N * W."""
         from cusnarks_b200._lib import lib
         c = lib().cs_msm_default_window(self.n, 0)
         return self.n * lib().cs_msm_num_windows(c), c
-
-    def e2e_step(self) -> float:
-        t0 = time.perf_counter()
-        from cusnarks_b200._lib import lib, check
-        L = lib()
-        check(L.cs_msm(self.ctx.handle, 0, self.h_s.data_ptr(), self.h_p.data_ptr(), self.n,
-                       self.h_out.data_ptr(), 0), self.ctx.handle)
-        return (time.perf_counter() - t0) * 1e3
-
-    @property
-    def h2d_bytes(self):
-        return self.n * (32 + 64)
-
-    d2h_bytes = 64
-
-    def algorithmic_mults(self):
-        return survey_msm_mults(self.n)
-
-    def hbm_bytes(self):
-        return self.n * 96
 
 
 def run_ours(args, world, rank, local):
@@ -232,8 +241,8 @@ def run_ours(args, world, rank, local):
     from cusnarks_b200 import Context
     from cusnarks_b200.context import kernel_launches
     ctx = Context(local)
-    wl = MsmWorkload(ctx, 20, seed=1234 + rank)
     peak_imad = ctx.imad_peak()
+    wl = ProveWorkload(ctx, LOG_M, seed=100 + rank)
     for _ in range(args.warmup):
         wl.step()
     wl.l2_flush()
@@ -243,11 +252,9 @@ def run_ours(args, world, rank, local):
     if sampler:
         sampler.start()
     l0 = kernel_launches()
-    dev_ms, acc_ms = [], []
+    dev_ms = []
     for _ in range(args.steps):
-        t, a = wl.step()
-        dev_ms.append(t)
-        acc_ms.append(a)
+        dev_ms.append(wl.step())
         wl.l2_flush()
     launches = kernel_launches() - l0
     torch.cuda.synchronize()
@@ -255,81 +262,90 @@ def run_ours(args, world, rank, local):
     clocks = sampler.stop() if sampler else None
     total_ms = max_over_ranks(sum(dev_ms), world)
     ms_per_step = total_ms / args.steps
-    # end-to-end through the C ABI with pinned host buffers
-    e2e = [wl.e2e_step() for _ in range(max(2, args.steps // 2))]
-    e2e_ms = max_over_ranks(statistics.median(e2e), world)
     value = world * 1e3 / ms_per_step
-    mults = wl.algorithmic_mults()
-    achieved_imad_msm = mults * IMAD_PER_MONT / (ms_per_step * 1e-3)
-    # dominant kernel: bucket accumulation, 11 Montgomery products (mixed add) per entry
-    units, window = wl.dominant_units()
+    # end-to-end through the C ABI with host buffers
+    e2e = [wl.e2e_step() for _ in range(max(3, args.steps // 2))]
+    e2e_ms = max_over_ranks(statistics.median(e2e), world)
+    # the 2^20 G1 MSM and its dominant kernel
+    mw = MsmWorkload(ctx, 20, seed=7 + rank)
+    for _ in range(3):
+        mw.step()
+    msm_ms, acc_ms = [], []
+    for _ in range(max(3, args.steps)):
+        t, a = mw.step()
+        msm_ms.append(t)
+        acc_ms.append(a)
+        wl.l2_flush()
+    units, window = mw.dominant_units()
     acc = statistics.mean(acc_ms)
-    achieved_imad = units * 11 * IMAD_PER_MONT / (acc * 1e-3)
+    achieved = units * 11 * IMAD_PER_MONT / (acc * 1e-3)
     line = {
         "metric": METRIC,
         "value": round(value, 3),
-        "unit": "G1 MSM (2^20) / s",
+        "unit": UNIT,
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": round(ms_per_step, 4),
+        "ms_per_step": round(ms_per_step, 3),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "u32x8 (256-bit Montgomery integers)",
-        "data": "synthetic: seeded uniform Fr scalars, base points k_i*G1 generated on GPU",
-        "config": {"workload": "BN128 G1 MSM N=2^20, single instance, inputs resident in HBM",
-                   "l2": "flushed between timed steps (2x L2 write)", "window": "auto"},
-        "g1_msm_2^20_ms": round(ms_per_step, 4),
-        "roofline": {"bound": "int (IMAD pipe)", "kernel": "k_accumulate+k_combine (bucket accumulation)",
-                     "achieved": round(achieved_imad / 1e12, 4),
-                     "peak": round(peak_imad / 1e12, 4), "unit": "T IMAD/s",
-                     "frac": round(achieved_imad / peak_imad, 4), "traffic": None,
+        "data": "synthetic: seeded R1CS (3 nonzeros per A/B row), seeded toxic waste, GPU-generated key",
+        "config": {"workload": "Groth16 prove, synthetic R1CS 2^20 constraints (domain 2^20), "
+                               "proving key resident in HBM, fixed r,s",
+                   "n_vars": wl.circ.n_vars, "domain": 1 << LOG_M, "path": "plain (one proof per call)",
+                   "l2": "flushed between timed steps (2x L2 write)"},
+        "latency_ms": {"p50": round(pct(dev_ms, 50), 3), "p99": round(pct(dev_ms, 99), 3),
+                       "basis": "device time per proof, plain per-call path"},
+        "g1_msm_2^20_ms": round(statistics.median(msm_ms), 3),
+        "roofline": {"bound": "int (IMAD pipe)", "kernel": "k_accumulate+k_combine (MSM bucket accumulation)",
+                     "achieved": round(achieved / 1e12, 4), "peak": round(peak_imad / 1e12, 4),
+                     "unit": "T IMAD/s", "frac": round(achieved / peak_imad, 4), "traffic": None,
                      "kernel_ms": round(acc, 4), "units_per_launch": units, "window": window,
-                     "basis": "N*W entries x 11 Montgomery products (mixed add) x 264 IMAD / "
-                              "accumulation ms; peak = live IMAD microbenchmark (cs_bench_imad_peak)",
-                     "whole_msm": {"achieved": round(achieved_imad_msm / 1e12, 4),
-                                   "frac": round(achieved_imad_msm / peak_imad, 4),
-                                   "basis": "survey count w(11N+32B) Montgomery products x 264 IMAD"}},
-        "e2e": {"value": round(world * 1e3 / e2e_ms, 3), "unit": "G1 MSM (2^20) / s",
-                "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes,
-                "ms": round(e2e_ms, 3)},
+                     "basis": "2^20 G1 MSM: N*W entries x 11 Montgomery products x 264 IMAD / kernel ms "
+                              "(CUDA events around the kernels); peak = live IMAD microbenchmark"},
+        "e2e": {"value": round(world * 1e3 / e2e_ms, 3), "unit": UNIT, "ms": round(e2e_ms, 3),
+                "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes},
         "gpu_launches": launches,
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        sec, kind, threads = cpu_reference_msm(1 << 16, seed=99)
-        line["cpu_baseline"] = {"value": round(1.0 / (sec * 16), 5), "unit": "G1 MSM (2^20) / s",
-                                "cores": threads, "kind": kind,
-                                "sample": "one 2^16-term G1 MSM (reference defaults: order 6, pippen 0), "
-                                          "time x16 to the 2^20 unit",
-                                "ms_2^20_scaled": round(sec * 16e3, 1)}
+        sec, kind, threads = cpu_reference_prove_sample(ctx, CPU_SAMPLE_LOG_M, seed=55)
+        scaled = sec * (1 << (LOG_M - CPU_SAMPLE_LOG_M))
+        line["cpu_baseline"] = {"value": round(1.0 / scaled, 6), "unit": UNIT, "cores": threads, "kind": kind,
+                                "sample": f"one Groth16 proof of a 2^{CPU_SAMPLE_LOG_M}-constraint circuit of the "
+                                          f"same family ({sec:.2f} s), x{1 << (LOG_M - CPU_SAMPLE_LOG_M)} to 2^20",
+                                "s_per_proof_scaled": round(scaled, 2)}
     if rank == 0:
         print(json.dumps(line), flush=True)
+    wl.prover.close()
     ctx.close()
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    times = []
-    kind, threads = "reference", os.cpu_count() or 1
+    from cusnarks_b200 import Context
+    ctx = Context(0)
+    times, kind, threads = [], "reference", os.cpu_count() or 1
     for i in range(args.warmup + args.steps):
-        sec, kind, threads = cpu_reference_msm(1 << 16, seed=500 + i)
+        sec, kind, threads = cpu_reference_prove_sample(ctx, CPU_SAMPLE_LOG_M, seed=500 + i)
         if i >= args.warmup:
-            times.append(sec * 16)
+            times.append(sec * (1 << (LOG_M - CPU_SAMPLE_LOG_M)))
     per = statistics.mean(times)
     val = 1.0 / per
-    line = {"metric": METRIC, "impl": "reference", "value": round(val, 5), "unit": "G1 MSM (2^20) / s",
+    line = {"metric": METRIC, "impl": "reference", "value": round(val, 6), "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(per * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": round(per * 1e3, 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32x8 (256-bit Montgomery integers)", "data": "synthetic",
-            "config": {"workload": "BN128 G1 MSM N=2^20, single instance (timed on 2^16-term samples x16)"},
-            "cpu_baseline": {"value": round(val, 5), "unit": "G1 MSM (2^20) / s", "cores": threads,
-                             "kind": kind, "sample": "2^16-term G1 MSM per step, scaled x16"},
-            "e2e": {"value": round(val, 5), "unit": "G1 MSM (2^20) / s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+            "config": {"workload": "Groth16 prove, synthetic R1CS 2^20 constraints (timed on 2^16-constraint "
+                                   "samples of the same family, x16)"},
+            "cpu_baseline": {"value": round(val, 6), "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"one 2^{CPU_SAMPLE_LOG_M}-constraint proof per step, x16 to 2^20"},
+            "e2e": {"value": round(val, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    ctx.close()
 
 
 def main():
@@ -338,16 +354,12 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["msm"], default="msm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    world, rank, local = (1, 0, 0)
     if args.impl == "reference":
-        world = int(os.environ.get("WORLD_SIZE", "1"))
-        rank = int(os.environ.get("RANK", "0"))
-        run_reference(args, world, rank)
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
         return
     world, rank, local = dist_setup()
     run_ours(args, world, rank, local)

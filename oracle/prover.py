@@ -19,27 +19,33 @@ def _ext(a: np.ndarray, rows) -> np.ndarray:
     return np.concatenate([np.asarray(a, dtype=np.uint32).reshape(-1, 8), ints_to_limbs(rows)])
 
 
-def cpu_prove(o: Oracle, pk: dict, w: np.ndarray, r: int, s: int, order: int = 6) -> np.ndarray:
+def cpu_prove(o: Oracle, pk: dict, w: np.ndarray, r: int, s: int, order: int = 6, ref=None) -> np.ndarray:
     """pk: host arrays as cusnarks_b200.groth.pk_to_host returns them.  Returns 64 words:
-    pi_A | pi_B | pi_C, affine Montgomery."""
+    pi_A | pi_B | pi_C, affine Montgomery.  With ref (an oracle.RefLib), the QAP evaluation,
+    H step and multi-exponentiations run in the reference's own library instead of the
+    restatement (same sequence, same results)."""
     nv, npub, m = pk["n_vars"], pk["n_public"], pk["domain_size"]
     L = m.bit_length() - 1
     w = np.ascontiguousarray(w, dtype=np.uint32).reshape(-1, 8)
-    pA = o.mpoly_eval(w[:nv], pk["polsA"], m, 0, nv, 1)
-    pB = o.mpoly_eval(w[:nv], pk["polsB"], m, 0, nv, 1)
-    roots = o.find_roots(L + 1)
-    M = o.interpolandmul(pA, pB, roots, L, 2)
+    eng = ref if ref is not None else o
+    pA = eng.mpoly_eval(w[:nv], pk["polsA"], m, 0, nv, 1)
+    pB = eng.mpoly_eval(w[:nv], pk["polsB"], m, 0, nv, 1)
+    if ref is not None:
+        from .oracle import hstep_roots_table
+        M = ref.interpolandmul(pA, pB, hstep_roots_table(o, L), L, 2)
+    else:
+        M = o.interpolandmul(pA, pB, o.find_roots(L + 1), L, 2)
     polH = M[m:2 * m - 1]
     neg_rs = (-(r * s)) % R
-    pi_a = o.msm(_ext(w[:nv], [1, r]), pk["A"][:nv + 2], 0, order)
-    pi_b = o.msm(_ext(w[:nv], [1, s]), pk["B2"][:nv + 2], 1, order)
-    pi_b1 = o.msm(_ext(w[:nv], [1, s]), pk["B1"][:nv + 2], 0, order)
-    pi_c = o.msm(w[npub + 1:nv], pk["C"][npub + 1:nv], 0, order)
+    pi_a = eng.msm(_ext(w[:nv], [1, r]), pk["A"][:nv + 2], 0, order)
+    pi_b = eng.msm(_ext(w[:nv], [1, s]), pk["B2"][:nv + 2], 1, order)
+    pi_b1 = eng.msm(_ext(w[:nv], [1, s]), pk["B1"][:nv + 2], 0, order)
+    pi_c = eng.msm(w[npub + 1:nv], pk["C"][npub + 1:nv], 0, order)
     hpts = np.concatenate([pk["hExps"][:m - 1].reshape(-1, 16), pk["delta_1"].reshape(-1, 16)])
-    pi_c2 = o.msm(_ext(polH, [neg_rs]), hpts, 0, order)
+    pi_c2 = eng.msm(_ext(polH, [neg_rs]), hpts, 0, order)
     fin_s = ints_to_limbs([1, 1, s, r])
     fin_p = np.stack([pi_c2, pi_c, pi_a, pi_b1])
-    pi_c = o.msm(fin_s, fin_p, 0, 2)
+    pi_c = eng.msm(fin_s, fin_p, 0, 2)
     return np.concatenate([pi_a, pi_b, pi_c]).astype(np.uint32)
 
 
