@@ -81,6 +81,11 @@ _SIGNATURES = [
     ("cs_msm_workspace_bytes", ctypes.c_size_t, [ctypes.c_uint32, ctypes.c_int, ctypes.c_int]),
     ("cs_msm_default_window", ctypes.c_int, [ctypes.c_uint32, ctypes.c_int]),
     ("cs_msm_num_windows", ctypes.c_int, [ctypes.c_int]),
+    ("cs_msm_fixed_window", ctypes.c_int, [ctypes.c_uint32, ctypes.c_int]),
+    ("cs_msm_fixed_table_points", ctypes.c_size_t, [ctypes.c_uint32, ctypes.c_int]),
+    ("cs_msm_fixed_workspace_bytes", ctypes.c_size_t, [ctypes.c_uint32, ctypes.c_int, ctypes.c_int]),
+    ("cs_msm_fixed_table_device", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_uint32, ctypes.c_int, _vp]),
+    ("cs_msm_fixed_device", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, ctypes.c_int, _vp]),
     ("cs_scmul_device", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, ctypes.c_uint32, _vp]),
     ("cs_bench_imad_peak", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     ("cs_bench_pipe", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
@@ -113,6 +118,9 @@ _SIGNATURES = [
     ("cs_pk_create", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.POINTER(_vp)]),
     ("cs_pk_destroy", None, [_vp]),
     ("cs_prove_workspace_bytes", ctypes.c_size_t, [_vp]),
+    ("cs_pk_fixed_base", ctypes.c_int, [_vp, _vp, ctypes.c_int]),
+    ("cs_pk_device_bytes", ctypes.c_size_t, [_vp]),
+    ("cs_pk_fixed_window", ctypes.c_int, [_vp, ctypes.c_int]),
     ("cs_prove", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     ("cs_prove_device", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     ("cs_setup_lagrange", ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp]),

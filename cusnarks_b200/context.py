@@ -86,6 +86,26 @@ class Context:
     def msm_workspace_bytes(n: int, ec2: bool = False, window: int = 0) -> int:
         return int(lib().cs_msm_workspace_bytes(n, int(bool(ec2)), window))
 
+    # ---------------------------------------------------- fixed-base (resident) MSM ----
+    @staticmethod
+    def msm_fixed_window(n: int, ec2: bool = False) -> int:
+        return int(lib().cs_msm_fixed_window(n, int(bool(ec2))))
+
+    @staticmethod
+    def msm_fixed_table_points(n: int, window: int) -> int:
+        return int(lib().cs_msm_fixed_table_points(n, window))
+
+    def msm_fixed_table_device(self, d_points: int, n: int, window: int, d_table: int, ec2: bool = False):
+        """d_table (msm_fixed_table_points(n, window) affine points) <- 2^(window j) P_i."""
+        check(self._lib.cs_msm_fixed_table_device(self.handle, int(bool(ec2)), ctypes.c_void_p(d_points), n,
+                                                  window, ctypes.c_void_p(d_table)), self.handle)
+
+    def msm_fixed_device(self, d_scalars: int, d_table: int, n: int, window: int, d_out: int,
+                         ec2: bool = False):
+        check(self._lib.cs_msm_fixed_device(self.handle, int(bool(ec2)), ctypes.c_void_p(d_scalars),
+                                            ctypes.c_void_p(d_table), n, window, ctypes.c_void_p(d_out)),
+              self.handle)
+
     # -------------------------------------------------------------- field ops -----
     FOP = {"mul": 0, "add": 1, "sub": 2, "sqr": 3, "inv": 4, "to_mont": 5, "from_mont": 6,
            "mul_lohi": 7, "fq2_mul": 8}

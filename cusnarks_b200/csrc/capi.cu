@@ -235,6 +235,51 @@ int cs_msm(cs_ctx* ctx, int ec2, const uint32_t* scalars, const uint32_t* points
   return CS_OK;
 }
 
+int cs_msm_fixed_window(uint32_t n, int ec2) { return csb::msm_fixed_window(n, ec2 != 0); }
+
+size_t cs_msm_fixed_table_points(uint32_t n, int window) {
+  return window >= 4 && window <= 24 ? csb::msm_fixed_table_points(n, window) : 0;
+}
+
+size_t cs_msm_fixed_workspace_bytes(uint32_t n, int ec2, int window) {
+  return csb::msm_fixed_workspace_bytes(n, window, ec2 != 0);
+}
+
+int cs_msm_fixed_table_device(cs_ctx* ctx, int ec2, const uint32_t* d_points, uint32_t n, int window,
+                              uint32_t* d_table) {
+  if (!ctx || window < 4 || window > 24 || (n && (!d_points || !d_table))) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaError_t e = ctx->work.reserve(csb::msm_fixed_table_work_bytes(n, ec2 != 0), ctx->stream);
+  if (e != cudaSuccess) return fail(ctx, e, "fixed-base table scratch");
+  EventScope ev(ctx);
+  e = ec2 ? csb::msm_fixed_table_g2(d_points, n, window, d_table, ctx->work.ptr, ctx->work.bytes, ctx->stream)
+          : csb::msm_fixed_table_g1(d_points, n, window, d_table, ctx->work.ptr, ctx->work.bytes, ctx->stream);
+  ev.stop();
+  if (e != cudaSuccess) return fail(ctx, e, "fixed-base table launch");
+  return CS_OK;
+}
+
+int cs_msm_fixed_device(cs_ctx* ctx, int ec2, const uint32_t* d_scalars, const uint32_t* d_table, uint32_t n,
+                        int window, uint32_t* d_out) {
+  if (!ctx || !d_out || window < 4 || window > 24 || (n && (!d_scalars || !d_table))) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaError_t e = ctx->work.reserve(csb::msm_fixed_workspace_bytes(n, window, ec2 != 0), ctx->stream);
+  if (e != cudaSuccess) return fail(ctx, e, "fixed-base msm workspace");
+  csb::MsmConfig cfg;
+  cfg.c = window;
+  cfg.acc_start = ctx->ev_phase0;
+  cfg.acc_stop = ctx->ev_phase1;
+  ctx->phase_valid = true;
+  EventScope ev(ctx);
+  e = ec2 ? csb::msm_fixed_g2(d_scalars, d_table, n, d_out, ctx->work.ptr, ctx->work.bytes, cfg, ctx->stream)
+          : csb::msm_fixed_g1(d_scalars, d_table, n, d_out, ctx->work.ptr, ctx->work.bytes, cfg, ctx->stream);
+  ev.stop();
+  if (e != cudaSuccess) return fail(ctx, e, "fixed-base msm launch");
+  return CS_OK;
+}
+
 int cs_scmul_device(cs_ctx* ctx, int ec2, const uint32_t* d_scalars, const uint32_t* d_points,
                     uint32_t stride, uint32_t n, uint32_t* d_out) {
   if (!ctx || (n && (!d_scalars || !d_points || !d_out))) return CS_ERR_ARG;

@@ -22,4 +22,28 @@ size_t msm_workspace_bytes(uint32_t n, int c, bool ec2) {
   return msm_detail::make_layout(n, c, xb, msm_detail::kMinTask).total;
 }
 
+int msm_fixed_window(uint32_t n, bool ec2) {
+  // one bucket set: W * n * madd + 2 * 2^(c-1) * add
+  int best = 8;
+  double best_cost = 1e300;
+  for (int c = 6; c <= 22; c++) {
+    const double W = msm_detail::num_windows(c);
+    const double cost = W * (double)n * 10.0 + 2.0 * (double)(1u << (c - 1)) * 14.0;
+    if (cost < best_cost) { best_cost = cost; best = c; }
+  }
+  (void)ec2;
+  return best;
+}
+
+size_t msm_fixed_table_points(uint32_t n, int c) { return (size_t)msm_detail::num_windows(c) * n; }
+
+size_t msm_fixed_table_work_bytes(uint32_t n, bool ec2) {
+  return msm_detail::fixed_table_work_bytes(n, ec2 ? 256 : 128, ec2 ? 64 : 32);
+}
+
+size_t msm_fixed_workspace_bytes(uint32_t n, int c, bool ec2) {
+  if (c <= 0) c = msm_fixed_window(n, ec2);
+  return msm_detail::make_layout(n, c, ec2 ? 256 : 128, msm_detail::kMinTask, true).total;
+}
+
 }  // namespace csb

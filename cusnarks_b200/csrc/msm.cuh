@@ -23,6 +23,12 @@
 //                the segment total for the next level).
 //   6. finish:   level results are combined with 3-bit Horner steps, windows with c-bit
 //                Horner steps, and the result is converted to affine.
+//
+// Fixed-base variant, for bases that stay resident (a proving key): a table
+// T[j*N + i] = 2^(c j) P_i of W*N affine points is built once, every digit of every
+// scalar goes into ONE set of 2^(c-1) buckets, and steps 5-6 reduce a single window
+// (more 8-bucket levels, no window Horner).  With the per-window tail gone a wider
+// window (c ~ 20 at N = 2^20: 13 instead of 16 windows) also cuts the accumulation.
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
@@ -50,5 +56,21 @@ cudaError_t msm_g1(const uint32_t* d_scalars, const uint32_t* d_points, uint32_t
 cudaError_t msm_g2(const uint32_t* d_scalars, const uint32_t* d_points, uint32_t n,
                    uint32_t* d_out, void* d_work, size_t work_bytes, const MsmConfig& cfg,
                    cudaStream_t stream);
+
+// Fixed-base MSM.  Window for a table of n bases; table points (W*n); scratch bytes to
+// build a table (table_work) and to run one MSM (workspace).  cfg.c must equal the c the
+// table was built with.
+int msm_fixed_window(uint32_t n, bool ec2);
+size_t msm_fixed_table_points(uint32_t n, int c);
+size_t msm_fixed_table_work_bytes(uint32_t n, bool ec2);
+size_t msm_fixed_workspace_bytes(uint32_t n, int c, bool ec2);
+cudaError_t msm_fixed_table_g1(const uint32_t* d_points, uint32_t n, int c, uint32_t* d_table, void* d_work,
+                               size_t work_bytes, cudaStream_t stream);
+cudaError_t msm_fixed_table_g2(const uint32_t* d_points, uint32_t n, int c, uint32_t* d_table, void* d_work,
+                               size_t work_bytes, cudaStream_t stream);
+cudaError_t msm_fixed_g1(const uint32_t* d_scalars, const uint32_t* d_table, uint32_t n, uint32_t* d_out,
+                         void* d_work, size_t work_bytes, const MsmConfig& cfg, cudaStream_t stream);
+cudaError_t msm_fixed_g2(const uint32_t* d_scalars, const uint32_t* d_table, uint32_t n, uint32_t* d_out,
+                         void* d_work, size_t work_bytes, const MsmConfig& cfg, cudaStream_t stream);
 
 }  // namespace csb

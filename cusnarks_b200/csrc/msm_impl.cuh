@@ -81,7 +81,10 @@ CSB_DEV bool load_scalar(const uint32_t* scalars, const uint32_t* points, uint32
   return !point_is_inf<F>(points + (size_t)i * PW);
 }
 
-template <class F>
+// Entry placement.  Generic: bucket (window j, |d|-1) of W*B, entry = point index i.
+// Fixed-base (tables T[j*n + i] = 2^(c j) P_i): one set of B buckets, bucket |d|-1,
+// entry = table index j*n + i, so no per-window sums and no Horner step remain.
+template <class F, bool FIXED>
 __global__ void k_count(const uint32_t* __restrict__ scalars, const uint32_t* __restrict__ points,
                         uint32_t n, int c, int W, uint32_t* __restrict__ counts) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -90,11 +93,11 @@ __global__ void k_count(const uint32_t* __restrict__ scalars, const uint32_t* __
   if (!load_scalar<F>(scalars, points, i, k)) return;
   const uint32_t B = 1u << (c - 1);
   for_each_digit(k, c, W, [&](int j, uint32_t mag, bool) {
-    atomicAdd(&counts[(size_t)j * B + (mag - 1)], 1u);
+    atomicAdd(&counts[(FIXED ? 0 : (size_t)j * B) + (mag - 1)], 1u);
   });
 }
 
-template <class F>
+template <class F, bool FIXED>
 __global__ void k_scatter(const uint32_t* __restrict__ scalars, const uint32_t* __restrict__ points,
                           uint32_t n, int c, int W, uint32_t* __restrict__ cursor,
                           uint32_t* __restrict__ entries) {
@@ -104,8 +107,8 @@ __global__ void k_scatter(const uint32_t* __restrict__ scalars, const uint32_t* 
   if (!load_scalar<F>(scalars, points, i, k)) return;
   const uint32_t B = 1u << (c - 1);
   for_each_digit(k, c, W, [&](int j, uint32_t mag, bool neg) {
-    const uint32_t pos = atomicAdd(&cursor[(size_t)j * B + (mag - 1)], 1u);
-    entries[pos] = i | (neg ? NEG_BIT : 0u);
+    const uint32_t pos = atomicAdd(&cursor[(FIXED ? 0 : (size_t)j * B) + (mag - 1)], 1u);
+    entries[pos] = (FIXED ? (uint32_t)j * n + i : i) | (neg ? NEG_BIT : 0u);
   });
 }
 
@@ -321,17 +324,17 @@ CSB_DEV XYZZ<F> shfl_down_xyzz(const XYZZ<F>& v, int d) {
   return o;
 }
 
-// Per-window sum after level 0.  With y_t the segment totals and z_t the in-segment
-// weighted sums of level 0, S_j = sum_t (y_t + z_t) + 8 * sum_t t * y_t.  One block per
-// window, E consecutive segments per thread u:
-//   V_u = Y_u + Z_u + 8 * sum_i i*y_{uE+i}      (Y_u, Z_u: the thread's totals)
+// Per-window sum after levels 0..L-1.  With y_t the segment totals and z_t the weighted
+// carries of the last level, S_j = sum_t (y_t + z_t) + G * sum_t t * y_t with G = 8^L =
+// 2^shift.  One block per window, E consecutive segments per thread u:
+//   V_u = Y_u + Z_u + G * sum_i i*y_{uE+i}      (Y_u, Z_u: the thread's totals)
 //   sum_t t*y_t = sum_u [sum_i i*y_{uE+i}] + E * sum_{u>=1} Suf(u),  Suf(u) = sum_{v>=u} Y_v
-// so S_j = sum_u (V_u + 8E * Suf(u) [u >= 1]): a block suffix scan and a block reduction,
+// so S_j = sum_u (V_u + G E * Suf(u) [u >= 1]): a block suffix scan and a block reduction,
 // about 2E + 25 dependent point operations instead of a serial pass over the segments.
 template <class F, int THREADS>
 __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restrict__ y,
                                                         const uint32_t* __restrict__ z, uint32_t n1,
-                                                        uint32_t* __restrict__ wsum) {
+                                                        int shift, uint32_t* __restrict__ wsum) {
   constexpr int XW = 4 * FieldWords<F>::value;
   constexpr int NW = THREADS / 32;
   __shared__ uint32_t sh[NW][XW];
@@ -351,8 +354,9 @@ __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restri
     }
     if (i > 0) ws = xyzz_add_cold(ws, acc);
   }
-  // V = acc + zs + 8 ws
-  ws = xyzz_dbl_cold(xyzz_dbl_cold(xyzz_dbl_cold(ws)));
+  // V = acc + zs + 2^shift ws
+#pragma unroll 1
+  for (int d = 0; d < shift; d++) ws = xyzz_dbl_cold(ws);
   XYZZ<F> V = xyzz_add_cold(xyzz_add_cold(acc, zs), ws);
   // inclusive suffix scan of acc across the block
   XYZZ<F> suf = acc;
@@ -394,10 +398,12 @@ __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restri
     suf = xyzz_add_cold(suf, off);
   }
   __syncthreads();
-  // C_u = V_u + 8E * Suf(u) for u >= 1 (8E is a power of two)
+  // C_u = V_u + 2^shift E * Suf(u) for u >= 1 (E is a power of two)
   if (u >= 1 && u * E < n1) {
 #pragma unroll 1
-    for (uint32_t m = 8 * E; m > 1; m >>= 1) suf = xyzz_dbl_cold(suf);
+    for (uint32_t m = E; m > 1; m >>= 1) suf = xyzz_dbl_cold(suf);
+#pragma unroll 1
+    for (int d = 0; d < shift; d++) suf = xyzz_dbl_cold(suf);
     V = xyzz_add_cold(V, suf);
   }
   // block reduction of V
@@ -444,20 +450,25 @@ __global__ void k_store_inf(uint32_t* out) {
 // counters block: [0] tasks, [1] partial slots, [2] split buckets; hist at +16 and
 // bin cursors at +96 (kMaxTask + 1 words each).
 constexpr int kCtrHist = 16, kCtrCursor = 96, kCtrWords = 192;
+// fixed-base reduction stops adding levels once a window has at most this many segments
+constexpr uint32_t kFixedTopSegments = 1024;
 
 struct Layout {
-  size_t counts, offsets, entries, tasks, multi, partials, buckets, lv_y, lv_z, wsum, counters, total;
+  size_t counts, offsets, entries, tasks, multi, partials, buckets, lv_y, lv_z, lv_y2, lv_z2, wsum,
+      counters, total;
 };
 
 static inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
-inline Layout make_layout(uint32_t n, int c, int xyzz_bytes, uint32_t task_len) {
+inline Layout make_layout(uint32_t n, int c, int xyzz_bytes, uint32_t task_len, bool fixed = false) {
   const int W = num_windows(c);
-  const size_t nb = (size_t)W << (c - 1);
+  const size_t nb = fixed ? ((size_t)1 << (c - 1)) : (size_t)W << (c - 1);
+  const int WR = fixed ? 1 : W;  // bucket sets reduced
   const size_t ne = (size_t)n * W;
   const size_t max_tasks = nb + ne / task_len + 1;
   const size_t max_partials = 2 * (ne / task_len) + 1;
   const size_t n1 = ((size_t)1 << (c - 1)) / 8 + 1;
+  const size_t n2 = fixed ? n1 / 8 + 1 : 0;
   Layout L{};
   size_t o = 0;
   L.counters = o; o = align256(o + kCtrWords * sizeof(uint32_t));
@@ -468,9 +479,11 @@ inline Layout make_layout(uint32_t n, int c, int xyzz_bytes, uint32_t task_len) 
   L.multi = o;    o = align256(o + (ne / (task_len + 1) + 1) * sizeof(Multi));
   L.partials = o; o = align256(o + max_partials * (size_t)xyzz_bytes);
   L.buckets = o;  o = align256(o + nb * (size_t)xyzz_bytes);
-  L.lv_y = o;     o = align256(o + (size_t)W * n1 * xyzz_bytes);
-  L.lv_z = o;     o = align256(o + (size_t)W * n1 * xyzz_bytes);
-  L.wsum = o;     o = align256(o + (size_t)W * xyzz_bytes);
+  L.lv_y = o;     o = align256(o + (size_t)WR * n1 * xyzz_bytes);
+  L.lv_z = o;     o = align256(o + (size_t)WR * n1 * xyzz_bytes);
+  L.lv_y2 = o;    o = align256(o + n2 * xyzz_bytes);
+  L.lv_z2 = o;    o = align256(o + n2 * xyzz_bytes);
+  L.wsum = o;     o = align256(o + (size_t)WR * xyzz_bytes);
   L.total = o + scan_workspace_bytes(nb + 1);
   return L;
 }
@@ -487,26 +500,29 @@ int accumulate_grid(int sms) {
   return blocks_per_sm * sms;
 }
 
-template <class F>
+// One MSM.  Generic: d_points holds n points.  FIXED: d_points is a table of W*n points,
+// T[j*n + i] = 2^(c j) P_i, built with the same c (fixed_table_impl).
+template <class F, bool FIXED>
 cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32_t n,
                      uint32_t* d_out, void* d_work, size_t work_bytes, const MsmConfig& cfg,
                      cudaStream_t st) {
   constexpr bool EC2 = FieldWords<F>::value == 16;
   constexpr int XB = 4 * FieldWords<F>::value * 4;  // bytes per XYZZ point
-  constexpr int XWD = XB / 4;                       // words per XYZZ point
   if (n == 0) {
     k_store_inf<F><<<1, 32, 0, st>>>(d_out);
     note_launch();
     return cudaGetLastError();
   }
+  if (FIXED && cfg.c <= 0) return cudaErrorInvalidValue;  // the table fixes the window
   const int c = cfg.c > 0 ? cfg.c : msm_default_window(n, EC2);
   if (c < 4 || c > 24) return cudaErrorInvalidValue;
   uint32_t task_len = cfg.task > 0 ? (uint32_t)cfg.task : 64u;
   if (task_len < kMinTask) task_len = kMinTask;
   if (task_len > (uint32_t)kMaxTask) task_len = kMaxTask;
   const int W = num_windows(c);
-  const uint32_t nb = (uint32_t)W << (c - 1);
-  const Layout L = make_layout(n, c, XB, kMinTask);
+  if (FIXED && (uint64_t)W * n >= (uint64_t)NEG_BIT) return cudaErrorInvalidValue;
+  const uint32_t nb = FIXED ? (1u << (c - 1)) : (uint32_t)W << (c - 1);
+  const Layout L = make_layout(n, c, XB, kMinTask, FIXED);
   if (work_bytes < L.total || d_work == nullptr) return cudaErrorInvalidValue;
   char* base = static_cast<char*>(d_work);
   uint32_t* counters = reinterpret_cast<uint32_t*>(base + L.counters);
@@ -519,6 +535,8 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   uint32_t* buckets = reinterpret_cast<uint32_t*>(base + L.buckets);
   uint32_t* lv_y = reinterpret_cast<uint32_t*>(base + L.lv_y);
   uint32_t* lv_z = reinterpret_cast<uint32_t*>(base + L.lv_z);
+  uint32_t* lv_y2 = reinterpret_cast<uint32_t*>(base + L.lv_y2);
+  uint32_t* lv_z2 = reinterpret_cast<uint32_t*>(base + L.lv_z2);
   uint32_t* wsum = reinterpret_cast<uint32_t*>(base + L.wsum);
   void* scan_tmp = base + (L.total - scan_workspace_bytes(nb + 1));
 
@@ -526,13 +544,13 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   if ((e = cudaMemsetAsync(counters, 0, kCtrWords * sizeof(uint32_t), st)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(counts, 0, (nb + 1) * sizeof(uint32_t), st)) != cudaSuccess) return e;
   const int T = 256;
-  k_count<F><<<(n + T - 1) / T, T, 0, st>>>(d_scalars, d_points, n, c, W, counts);
+  k_count<F, FIXED><<<(n + T - 1) / T, T, 0, st>>>(d_scalars, d_points, n, c, W, counts);
   note_launch();
   if ((e = scan_exclusive_u32(counts, offsets, nb + 1, scan_tmp, st)) != cudaSuccess) return e;
   // counts is reused as the scatter cursor
   if ((e = cudaMemcpyAsync(counts, offsets, nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
     return e;
-  k_scatter<F><<<(n + T - 1) / T, T, 0, st>>>(d_scalars, d_points, n, c, W, counts, entries);
+  k_scatter<F, FIXED><<<(n + T - 1) / T, T, 0, st>>>(d_scalars, d_points, n, c, W, counts, entries);
   note_launch();
   k_task_hist<F><<<(nb + T - 1) / T, T, 0, st>>>(offsets, nb, task_len, counters + kCtrHist, buckets);
   note_launch();
@@ -552,17 +570,119 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   note_launch();
   if (cfg.acc_stop) cudaEventRecord(cfg.acc_stop, st);
   // level 0: segments of 8 buckets -> totals y and in-segment weighted sums z
+  const int WR = FIXED ? 1 : W;
   const uint32_t B = 1u << (c - 1);
-  const uint32_t n1 = (B + 7) / 8;
-  const uint32_t threads0 = (uint32_t)W * n1;
-  k_reduce_level<F><<<(threads0 + 127) / 128, 128, 0, st>>>(buckets, nullptr, B, n1, W, 0, lv_y, lv_z);
+  uint32_t nseg = (B + 7) / 8;
+  k_reduce_level<F><<<((uint32_t)WR * nseg + 127) / 128, 128, 0, st>>>(buckets, nullptr, B, nseg, WR, 0,
+                                                                      lv_y, lv_z);
   note_launch();
+  int levels = 1;
+  uint32_t *y = lv_y, *z = lv_z, *y2 = lv_y2, *z2 = lv_z2;
+  // fixed-base: one bucket set of 2^(c-1); more levels keep the single top block short
+  while (FIXED && nseg > kFixedTopSegments) {
+    const uint32_t nnext = (nseg + 7) / 8;
+    k_reduce_level<F><<<(nnext + 127) / 128, 128, 0, st>>>(y, z, nseg, nnext, 1, levels, y2, z2);
+    note_launch();
+    uint32_t* ty = y; y = y2; y2 = ty;
+    uint32_t* tz = z; z = z2; z2 = tz;
+    nseg = nnext;
+    levels++;
+  }
   constexpr int WT = 256;
-  k_window_sum<F, WT><<<W, WT, 0, st>>>(lv_y, lv_z, n1, wsum);
+  k_window_sum<F, WT><<<WR, WT, 0, st>>>(y, z, nseg, 3 * levels, wsum);
   note_launch();
-  k_finish<F><<<1, 32, 0, st>>>(wsum, W, c, d_out);
+  k_finish<F><<<1, 32, 0, st>>>(wsum, WR, c, d_out);
   note_launch();
-  (void)XWD;
+  return cudaGetLastError();
+}
+
+// Fixed-base tables.  table[0..n) = points; table[j n + i] = 2^c table[(j-1) n + i],
+// computed in XYZZ and brought back to affine with one inversion per run of kAffRun
+// points (Montgomery's simultaneous inversion).  Points at infinity stay infinity.
+constexpr int kAffRun = 16;
+
+template <class F>
+__global__ void __launch_bounds__(128) k_table_double(const uint32_t* __restrict__ src, uint32_t n, int c,
+                                                      uint32_t* __restrict__ xyzz) {
+  constexpr int XW = 4 * FieldWords<F>::value;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Affine<F> p = ld_affine<F>(src + (size_t)i * 2 * FieldWords<F>::value);
+  XYZZ<F> r = XYZZ<F>::inf();
+  if (!affine_is_inf(p)) {
+    r = xyzz_mdbl(p);
+#pragma unroll 1
+    for (int d = 1; d < c; d++) r = xyzz_dbl(r);
+  }
+  st_xyzz<F>(xyzz + (size_t)i * XW, r);
+}
+
+// Thread t converts points [t R, t R + R): prefix products of ZZ*ZZZ, one inverse, and
+// the back substitution; `pref` holds the prefix products (n field elements).
+template <class F>
+__global__ void __launch_bounds__(128) k_batch_affine(const uint32_t* __restrict__ xyzz, uint32_t n,
+                                                      uint32_t* __restrict__ pref, uint32_t* __restrict__ dst) {
+  constexpr int FW = FieldWords<F>::value;
+  constexpr int XW = 4 * FW;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t lo = t * kAffRun;
+  if (lo >= n) return;
+  const uint32_t hi = min(n, lo + kAffRun);
+  F acc = F::one();
+  for (uint32_t i = lo; i < hi; i++) {
+    const XYZZ<F> p = ld_xyzz<F>(xyzz + (size_t)i * XW);
+    if (!p.is_inf()) acc = acc * (p.ZZ * p.ZZZ);
+    st_field(pref + (size_t)i * FW, acc);
+  }
+  F inv = acc.inv();
+  for (uint32_t i = hi; i-- > lo;) {
+    const XYZZ<F> p = ld_xyzz<F>(xyzz + (size_t)i * XW);
+    uint32_t* o = dst + (size_t)i * 2 * FW;
+    if (p.is_inf()) {
+      st_affine<F>(o, Affine<F>{F::zero(), F::one()});
+      continue;
+    }
+    F before = F::one();
+    if (i > lo) {  // written above by this thread: a plain (coherent) load, not __ldg
+      uint32_t* bw = reinterpret_cast<uint32_t*>(&before);
+      const uint4* src = reinterpret_cast<const uint4*>(pref + (size_t)(i - 1) * FW);
+#pragma unroll
+      for (int q = 0; q < FW / 4; q++) {
+        const uint4 v = src[q];
+        bw[4 * q] = v.x; bw[4 * q + 1] = v.y; bw[4 * q + 2] = v.z; bw[4 * q + 3] = v.w;
+      }
+    }
+    const F ip = inv * before;          // 1 / (ZZ ZZZ)
+    inv = inv * (p.ZZ * p.ZZZ);
+    st_affine<F>(o, Affine<F>{p.X * (p.ZZZ * ip), p.Y * (p.ZZ * ip)});
+  }
+}
+
+inline size_t fixed_table_work_bytes(uint32_t n, int xyzz_bytes, int field_bytes) {
+  return align256((size_t)n * xyzz_bytes) + align256((size_t)n * field_bytes);
+}
+
+template <class F>
+cudaError_t fixed_table_impl(const uint32_t* d_points, uint32_t n, int c, uint32_t* d_table, void* d_work,
+                             size_t work_bytes, cudaStream_t st) {
+  constexpr int FW = FieldWords<F>::value;
+  constexpr int XB = 16 * FW, PB = 8 * FW;
+  if (c < 4 || c > 24) return cudaErrorInvalidValue;
+  if (n == 0) return cudaSuccess;
+  if (!d_work || work_bytes < fixed_table_work_bytes(n, XB, 4 * FW)) return cudaErrorInvalidValue;
+  uint32_t* xyzz = static_cast<uint32_t*>(d_work);
+  uint32_t* pref = reinterpret_cast<uint32_t*>(static_cast<char*>(d_work) + align256((size_t)n * XB));
+  const int W = num_windows(c);
+  cudaError_t e = cudaMemcpyAsync(d_table, d_points, (size_t)n * PB, cudaMemcpyDeviceToDevice, st);
+  if (e != cudaSuccess) return e;
+  const uint32_t runs = (n + kAffRun - 1) / kAffRun;
+  for (int j = 1; j < W; j++) {
+    const uint32_t* src = d_table + (size_t)(j - 1) * n * 2 * FW;
+    uint32_t* dst = d_table + (size_t)j * n * 2 * FW;
+    k_table_double<F><<<(n + 127) / 128, 128, 0, st>>>(src, n, c, xyzz);
+    k_batch_affine<F><<<(runs + 127) / 128, 128, 0, st>>>(xyzz, n, pref, dst);
+    note_launch(2);
+  }
   return cudaGetLastError();
 }
 

@@ -49,13 +49,33 @@ struct cs_pk {
   uint32_t* b2_ext = nullptr;  // nVars+2 G2
   uint32_t* c = nullptr;       // nVars G1
   uint32_t* h_ext = nullptr;   // m G1: hExps[0..m-2] ++ delta_1
+  // Fixed-base tables of the five MSMs (msm.cuh), in one allocation; c == 0: none.
+  struct Fixed {
+    uint32_t* table = nullptr;
+    uint32_t n = 0;
+    int c = 0;
+  };
+  Fixed fa, fb1, fb2, fc, fh;
+  void* fixed_block = nullptr;
+  size_t fixed_bytes = 0, base_bytes = 0;
   std::vector<void*> owned;
+  bool has_fixed() const { return fixed_block != nullptr; }
+  void drop_fixed() {
+    if (fixed_block) cudaFree(fixed_block);
+    fixed_block = nullptr;
+    fixed_bytes = 0;
+    fa = fb1 = fb2 = fc = fh = Fixed{};
+  }
   ~cs_pk() {
+    drop_fixed();
     for (void* p : owned) cudaFree(p);
   }
   cudaError_t alloc(void** p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes ? bytes : 256);
-    if (e == cudaSuccess) owned.push_back(*p);
+    if (e == cudaSuccess) {
+      owned.push_back(*p);
+      base_bytes += bytes ? bytes : 256;
+    }
     return e;
   }
 };
@@ -133,11 +153,19 @@ ProvePlan plan_prove(const cs_pk* pk) {
   ProvePlan P{};
   const size_t nv = pk->n_vars, m = pk->m;
   const uint32_t nc = pk->n_vars - pk->n_public - 1;
-  P.bytes_a = msm_workspace_bytes(pk->n_vars + 2, 0, false);
-  P.bytes_b1 = P.bytes_a;
-  P.bytes_b2 = msm_workspace_bytes(pk->n_vars + 2, 0, true);
-  P.bytes_c = msm_workspace_bytes(nc, 0, false);
-  P.bytes_h = msm_workspace_bytes(pk->m, 0, false);
+  if (pk->has_fixed()) {
+    P.bytes_a = msm_fixed_workspace_bytes(pk->fa.n, pk->fa.c, false);
+    P.bytes_b1 = msm_fixed_workspace_bytes(pk->fb1.n, pk->fb1.c, false);
+    P.bytes_b2 = msm_fixed_workspace_bytes(pk->fb2.n, pk->fb2.c, true);
+    P.bytes_c = msm_fixed_workspace_bytes(pk->fc.n, pk->fc.c, false);
+    P.bytes_h = msm_fixed_workspace_bytes(pk->fh.n, pk->fh.c, false);
+  } else {
+    P.bytes_a = msm_workspace_bytes(pk->n_vars + 2, 0, false);
+    P.bytes_b1 = P.bytes_a;
+    P.bytes_b2 = msm_workspace_bytes(pk->n_vars + 2, 0, true);
+    P.bytes_c = msm_workspace_bytes(nc, 0, false);
+    P.bytes_h = msm_workspace_bytes(pk->m, 0, false);
+  }
   size_t o = 0;
   P.wA = o; o += al256((nv + 2) * 32);
   P.wB = o; o += al256((nv + 2) * 32);
@@ -228,6 +256,73 @@ int cs_pk_create(cs_ctx* ctx, const cs_pk_desc* d, int on_device, cs_pk** out) {
 
 void cs_pk_destroy(cs_pk* pk) { delete pk; }
 
+int cs_pk_fixed_base(cs_ctx* ctx, cs_pk* pk, int window) {
+  if (!ctx || !pk || window > 24 || (window > 0 && window < 4)) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  // tables may be read by proofs still in flight on this context
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  for (int i = 0; i < 4 && e == cudaSuccess; i++)
+    if (ctx->aux[i]) e = cudaStreamSynchronize(ctx->aux[i]);
+  if (e != cudaSuccess) return fail(ctx, e, "cs_pk_fixed_base: sync");
+  pk->drop_fixed();
+  if (window < 0) return CS_OK;
+  const uint32_t nv = pk->n_vars, np1 = pk->n_public + 1;
+  struct Job {
+    cs_pk::Fixed* f;
+    const uint32_t* pts;
+    uint32_t n;
+    bool ec2;
+  } jobs[5] = {{&pk->fa, pk->a_ext, nv + 2, false},
+               {&pk->fb1, pk->b1_ext, nv + 2, false},
+               {&pk->fb2, pk->b2_ext, nv + 2, true},
+               {&pk->fc, pk->c + (size_t)np1 * 16, nv - np1, false},
+               {&pk->fh, pk->h_ext, pk->m, false}};
+  size_t total = 0, scratch = 0;
+  size_t offs[5];
+  for (int k = 0; k < 5; k++) {
+    Job& j = jobs[k];
+    const int c = window > 0 ? window : msm_fixed_window(j.n, j.ec2);
+    offs[k] = total;
+    total += al256(msm_fixed_table_points(j.n, c) * (j.ec2 ? 128 : 64));
+    const size_t sb = msm_fixed_table_work_bytes(j.n, j.ec2);
+    if (sb > scratch) scratch = sb;
+    j.f->n = j.n;
+    j.f->c = c;
+  }
+  if ((e = ctx->work.reserve(scratch, ctx->stream)) != cudaSuccess) {
+    pk->fa = pk->fb1 = pk->fb2 = pk->fc = pk->fh = cs_pk::Fixed{};
+    return fail(ctx, e, "cs_pk_fixed_base: table scratch");
+  }
+  void* block = nullptr;
+  if ((e = cudaMalloc(&block, total)) != cudaSuccess) {
+    pk->fa = pk->fb1 = pk->fb2 = pk->fc = pk->fh = cs_pk::Fixed{};
+    return fail(ctx, e, "cs_pk_fixed_base: tables");
+  }
+  pk->fixed_block = block;
+  pk->fixed_bytes = total;
+  for (int k = 0; k < 5 && e == cudaSuccess; k++) {
+    Job& j = jobs[k];
+    j.f->table = reinterpret_cast<uint32_t*>(static_cast<char*>(block) + offs[k]);
+    e = j.ec2 ? msm_fixed_table_g2(j.pts, j.n, j.f->c, j.f->table, ctx->work.ptr, ctx->work.bytes, ctx->stream)
+              : msm_fixed_table_g1(j.pts, j.n, j.f->c, j.f->table, ctx->work.ptr, ctx->work.bytes, ctx->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    pk->drop_fixed();
+    return fail(ctx, e, "cs_pk_fixed_base: table build");
+  }
+  return CS_OK;
+}
+
+size_t cs_pk_device_bytes(const cs_pk* pk) { return pk ? pk->base_bytes + pk->fixed_bytes : 0; }
+
+int cs_pk_fixed_window(const cs_pk* pk, int which) {
+  if (!pk || !pk->has_fixed() || which < 0 || which > 4) return 0;
+  const cs_pk::Fixed* f[5] = {&pk->fa, &pk->fb1, &pk->fb2, &pk->fc, &pk->fh};
+  return f[which]->c;
+}
+
 size_t cs_prove_workspace_bytes(const cs_pk* pk) { return pk ? plan_prove(pk).total : 0; }
 
 int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t* r, const uint32_t* s,
@@ -268,11 +363,22 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
   // witness MSMs on the auxiliary streams
   cudaStream_t sa = ctx->aux[0], sb1 = ctx->aux[1], sb2 = ctx->aux[2], sc = ctx->aux[3];
   for (int i = 0; i < 4; i++) cudaStreamWaitEvent(ctx->aux[i], ev_w, 0);
-  ok = (e = msm_g1(wA, pk->a_ext, nv + 2, outA, at(P.ms_a), P.bytes_a, cfg, sa)) == cudaSuccess &&
-       (e = msm_g1(wB, pk->b1_ext, nv + 2, outB1, at(P.ms_b1), P.bytes_b1, cfg, sb1)) == cudaSuccess &&
-       (e = msm_g2(wB, pk->b2_ext, nv + 2, outB2, at(P.ms_b2), P.bytes_b2, cfg, sb2)) == cudaSuccess &&
-       (e = msm_g1(wA + (size_t)np1 * 8, pk->c + (size_t)np1 * 16, nv - np1, outC, at(P.ms_c), P.bytes_c, cfg, sc)) ==
-           cudaSuccess;
+  // resident fixed-base tables when the key has them, else the generic MSM over the points
+  auto run_msm = [&](bool ec2, const uint32_t* sc, const uint32_t* pts, const cs_pk::Fixed& f, uint32_t n,
+                     uint32_t* out, size_t off, size_t bytes, cudaStream_t st) {
+    if (pk->has_fixed()) {
+      MsmConfig fcfg;
+      fcfg.c = f.c;
+      return ec2 ? msm_fixed_g2(sc, f.table, n, out, at(off), bytes, fcfg, st)
+                 : msm_fixed_g1(sc, f.table, n, out, at(off), bytes, fcfg, st);
+    }
+    return ec2 ? msm_g2(sc, pts, n, out, at(off), bytes, cfg, st) : msm_g1(sc, pts, n, out, at(off), bytes, cfg, st);
+  };
+  ok = (e = run_msm(false, wA, pk->a_ext, pk->fa, nv + 2, outA, P.ms_a, P.bytes_a, sa)) == cudaSuccess &&
+       (e = run_msm(false, wB, pk->b1_ext, pk->fb1, nv + 2, outB1, P.ms_b1, P.bytes_b1, sb1)) == cudaSuccess &&
+       (e = run_msm(true, wB, pk->b2_ext, pk->fb2, nv + 2, outB2, P.ms_b2, P.bytes_b2, sb2)) == cudaSuccess &&
+       (e = run_msm(false, wA + (size_t)np1 * 8, pk->c + (size_t)np1 * 16, pk->fc, nv - np1, outC, P.ms_c, P.bytes_c,
+                    sc)) == cudaSuccess;
   if (!ok) return fail(ctx, e, "prove witness MSMs");
   k_scale_point<Fq><<<1, 32, 0, sa>>>(outA, rs + 8, sA);   // s * pi_A
   k_scale_point<Fq><<<1, 32, 0, sb1>>>(outB1, rs, rB1);    // r * pi_B1
@@ -284,7 +390,7 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
                                  domain_consts(dom1) + 16, domain_consts(dom2) + 24, M, hscr, s0)) == cudaSuccess &&
        // polH = M[m .. 2m-2]; M[2m-1] (always zero) becomes the -rs term for delta_1
        (e = cudaMemcpyAsync(M + (size_t)(2 * m - 1) * 8, rs + 16, 32, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess &&
-       (e = msm_g1(M + (size_t)m * 8, pk->h_ext, m, outH, at(P.ms_h), P.bytes_h, cfg, s0)) == cudaSuccess;
+       (e = run_msm(false, M + (size_t)m * 8, pk->h_ext, pk->fh, m, outH, P.ms_h, P.bytes_h, s0)) == cudaSuccess;
   if (!ok) return fail(ctx, e, "prove QAP/H");
   for (int i = 0; i < 4; i++) {
     cudaEventRecord(ctx->aux_ev[1 + i], ctx->aux[i]);

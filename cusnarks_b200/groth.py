@@ -239,7 +239,9 @@ def pk_to_host(pk: dict) -> dict:
 class Prover:
     """A proving key resident in HBM and the prove call (cs_pk_create / cs_prove)."""
 
-    def __init__(self, ctx: Context, pk: dict):
+    def __init__(self, ctx: Context, pk: dict, fixed_base: int = 0):
+        """fixed_base: window of the resident fixed-base MSM tables (0 = automatic per MSM,
+        negative = no tables: every proof runs the generic MSM over the key's points)."""
         import torch
         self.ctx = ctx
         self._keep = []
@@ -269,6 +271,19 @@ class Prover:
         self.n_vars = pk["n_vars"]
         self._keep.clear()
         del torch
+        if fixed_base >= 0:
+            self.set_fixed_base(fixed_base)
+
+    def set_fixed_base(self, window: int = 0):
+        """Builds (window >= 0) or drops (window < 0) the key's fixed-base tables."""
+        check(lib().cs_pk_fixed_base(self.ctx.handle, self.handle, window), self.ctx.handle)
+
+    def fixed_windows(self) -> list:
+        """Windows of the A, B1, B2, C, H tables (0 = no table)."""
+        return [int(lib().cs_pk_fixed_window(self.handle, k)) for k in range(5)]
+
+    def device_bytes(self) -> int:
+        return int(lib().cs_pk_device_bytes(self.handle))
 
     def close(self):
         if getattr(self, "handle", None):

@@ -184,6 +184,21 @@ size_t cs_msm_workspace_bytes(uint32_t n, int ec2, int window);
 int cs_msm_default_window(uint32_t n, int ec2);
 int cs_msm_num_windows(int window);
 
+/* Fixed-base multi-exponentiation for bases that stay resident in HBM (a proving key).
+ * The reference re-sends the proving-key points with every proof (groth_prover.py:1563
+ * findECPointsDispatch); here a table of cs_msm_fixed_table_points(n, window) affine points
+ * T[j*n + i] = 2^(window*j) P_i is built once by cs_msm_fixed_table_device, and every
+ * cs_msm_fixed_device call over those bases sums all windows in one bucket set (no
+ * per-window reduction, no window Horner step).  Same result as cs_msm_device on the
+ * original points.  window in [4, 24]; cs_msm_fixed_window picks one for n bases. */
+int cs_msm_fixed_window(uint32_t n, int ec2);
+size_t cs_msm_fixed_table_points(uint32_t n, int window);
+size_t cs_msm_fixed_workspace_bytes(uint32_t n, int ec2, int window);
+int cs_msm_fixed_table_device(cs_ctx *ctx, int ec2, const uint32_t *d_points, uint32_t n, int window,
+                              uint32_t *d_table);
+int cs_msm_fixed_device(cs_ctx *ctx, int ec2, const uint32_t *d_scalars, const uint32_t *d_table,
+                        uint32_t n, int window, uint32_t *d_out_affine);
+
 /* Elementwise field operation on n elements of device arrays (8 words each; 16 for
  * CS_FOP_FQ2_MUL, which multiplies in Fq2 = Fq[u]/(u^2+1) regardless of pidx).
  * d_b is ignored by the unary operations.  Asynchronous on the context stream. */
@@ -264,6 +279,14 @@ typedef struct cs_pk cs_pk;
 int cs_pk_create(cs_ctx *ctx, const cs_pk_desc *desc, int on_device, cs_pk **out);
 void cs_pk_destroy(cs_pk *pk);
 size_t cs_prove_workspace_bytes(const cs_pk *pk);
+/* Builds fixed-base tables (cs_msm_fixed_*) for the key's five MSMs (window > 0: that
+ * window for all; 0: chosen per MSM) or drops them (window < 0); cs_prove uses the tables
+ * whenever the key has them.  About 13 x the G1/G2 point bytes at 2^20 (~5 GiB).
+ * Synchronises the context's streams first.  cs_pk_device_bytes: HBM the key holds;
+ * cs_pk_fixed_window: window of table `which` (0 A, 1 B1, 2 B2, 3 C, 4 H; 0 = none). */
+int cs_pk_fixed_base(cs_ctx *ctx, cs_pk *pk, int window);
+size_t cs_pk_device_bytes(const cs_pk *pk);
+int cs_pk_fixed_window(const cs_pk *pk, int which);
 /* Groth16 proof for witness w (n_vars normal-form elements, w[0] = 1), blinding r and s
  * (normal form, host pointers): proof = pi_A (16 words) | pi_B (32) | pi_C (16), affine
  * Montgomery, the reference prover's pi_a_eccf1 / pi_b_eccf2 / pi_c_eccf1

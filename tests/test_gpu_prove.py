@@ -48,10 +48,17 @@ def test_prove_matches_cpu_and_verifies(ctx, oracle, log_m, seed):
     bad = circ.public_inputs.copy()
     bad[0, 0] ^= 1
     assert not verify(host["vk"], proof, bad)
-    # the same key uploaded from host memory gives the same proof; proofs repeat
-    prover2 = Prover(ctx, host)
+    # the default key holds fixed-base tables for all five MSMs
+    assert all(c > 0 for c in prover.fixed_windows())
+    # the same key uploaded from host memory, without tables (generic MSMs), gives the
+    # same proof; proofs repeat; tables rebuilt with another window give it again
+    prover2 = Prover(ctx, host, fixed_base=-1)
+    assert prover2.fixed_windows() == [0] * 5
     assert np.array_equal(prover2.prove(circ.w, ints_to_limbs([r])[0], ints_to_limbs([s])[0]), proof)
     assert np.array_equal(prover.prove(circ.w, ints_to_limbs([r])[0], ints_to_limbs([s])[0]), proof)
+    prover2.set_fixed_base(7)
+    assert prover2.fixed_windows() == [7] * 5
+    assert np.array_equal(prover2.prove(circ.w, ints_to_limbs([r])[0], ints_to_limbs([s])[0]), proof)
     prover.close(); prover2.close()
 
 
