@@ -14,6 +14,9 @@
 namespace csb {
 
 #define CSB_DEV __device__ __forceinline__
+#ifndef CSB_FQ2_MODE
+#define CSB_FQ2_MODE 0  // Fq2 product: 0 CIOS x3, 1 carry-flag-free CIOS x3, 2 lazy reduction
+#endif
 
 // ---------------------------------------------------------------- moduli ------------
 struct ModQ {  // base field q (the reference's MOD_GROUP, pidx 0)
@@ -26,6 +29,14 @@ struct ModQ {  // base field q (the reference's MOD_GROUP, pidx 0)
                             R24 = 0x0a417ff6u, R25 = 0x47ab1effu, R26 = 0xcab8351fu, R27 = 0x06d89f71u;
   static constexpr uint32_t R30 = 0xda1530dfu, R31 = 0xb1cd6dafu, R32 = 0xa7283db6u, R33 = 0x62f210e6u,
                             R34 = 0x0ada0afbu, R35 = 0xef7f0b0cu, R36 = 0x2d592544u, R37 = 0x20fd6e90u;
+  // q^2, 16 limbs (lazy-reduction offset)
+  static CSB_DEV uint32_t P2_LIMB(int i) {
+    constexpr uint32_t k[16] = {0x275d69b1u, 0x3b5458a2u, 0x09eac101u, 0xa602072du,
+                                0x6d96cadcu, 0x4a50189cu, 0x7a1242c8u, 0x04689e95u,
+                                0x34c6b38du, 0x26edfa5cu, 0x16375606u, 0xb00b8551u,
+                                0x0348d21cu, 0x599a6f7cu, 0x763cbf9cu, 0x0925c4b8u};
+    return k[i];
+  }
 };
 struct ModR {  // scalar field r (the reference's MOD_FIELD, pidx 1)
   static constexpr uint32_t P0 = 0xf0000001u, P1 = 0x43e1f593u, P2 = 0x79b97091u, P3 = 0x2833e848u,
@@ -183,6 +194,94 @@ struct Fp {
     return r;
   }
 
+  // CIOS Montgomery product in plain 64-bit C++ arithmetic (no carry flag): independent
+  // products can be interleaved by the compiler.
+  static CSB_DEV Fp mul_c64(const Fp& a, const Fp& b) {
+    const uint32_t P[8] = {M::P0, M::P1, M::P2, M::P3, M::P4, M::P5, M::P6, M::P7};
+    uint32_t t[10];
+#pragma unroll
+    for (int i = 0; i < 10; i++) t[i] = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      uint64_t c = 0;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const uint64_t s = (uint64_t)a.v[j] * b.v[i] + t[j] + c;
+        t[j] = (uint32_t)s;
+        c = s >> 32;
+      }
+      const uint64_t s8 = (uint64_t)t[8] + c;
+      t[8] = (uint32_t)s8;
+      t[9] = (uint32_t)(s8 >> 32);
+      const uint32_t m = t[0] * M::NP0;
+      uint64_t c2 = ((uint64_t)m * P[0] + t[0]) >> 32;
+#pragma unroll
+      for (int j = 1; j < 8; j++) {
+        const uint64_t s = (uint64_t)m * P[j] + t[j] + c2;
+        t[j - 1] = (uint32_t)s;
+        c2 = s >> 32;
+      }
+      const uint64_t s7 = (uint64_t)t[8] + c2;
+      t[7] = (uint32_t)s7;
+      t[8] = t[9] + (uint32_t)(s7 >> 32);
+    }
+    uint32_t r8[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) r8[i] = t[i];
+    reduce_once(r8);
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = r8[i];
+    return r;
+  }
+
+  // Full 512-bit product a*b (16 limbs), 64-bit C++ arithmetic.
+  static CSB_DEV void mul_full(uint32_t (&t)[16], const Fp& a, const Fp& b) {
+#pragma unroll
+    for (int i = 0; i < 16; i++) t[i] = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      uint64_t c = 0;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const uint64_t s = (uint64_t)a.v[j] * b.v[i] + t[i + j] + c;
+        t[i + j] = (uint32_t)s;
+        c = s >> 32;
+      }
+      t[i + 8] = (uint32_t)c;
+    }
+  }
+
+  // Montgomery reduction T * 2^-256 mod p for T < p * 2^256 (16 limbs, consumed).
+  static CSB_DEV Fp redc(uint32_t (&t)[16]) {
+    const uint32_t P[8] = {M::P0, M::P1, M::P2, M::P3, M::P4, M::P5, M::P6, M::P7};
+    uint32_t hi = 0;  // overflow of limb i+8, owed to limb i+9
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const uint32_t m = t[i] * M::NP0;
+      uint64_t c = 0;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const uint64_t s = (uint64_t)m * P[j] + t[i + j] + c;
+        t[i + j] = (uint32_t)s;
+        c = s >> 32;
+      }
+      // row carry into limb i+8; its own overflow goes to limb i+9 with the next row
+      const uint64_t s8 = (uint64_t)t[i + 8] + c + hi;
+      t[i + 8] = (uint32_t)s8;
+      hi = (uint32_t)(s8 >> 32);
+    }
+    // T < p 2^256 keeps the result below 2p < 2^256: hi is 0 here
+    uint32_t r8[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) r8[i] = t[8 + i];
+    reduce_once(r8);
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = r8[i];
+    return r;
+  }
+
   friend CSB_DEV Fp operator*(const Fp& a, const Fp& b) {
 #ifdef CSB_MUL_LOHI
     return mul_lohi(a, b);
@@ -319,10 +418,53 @@ struct Fq2 {
   friend CSB_DEV Fq2 operator-(const Fq2& a, const Fq2& b) { return {a.c0 - b.c0, a.c1 - b.c1}; }
   // Karatsuba, 3 products (src/cuda/ff.cpp montmult_ext_h: same non-residue -1)
   friend CSB_DEV Fq2 operator*(const Fq2& a, const Fq2& b) {
+#if CSB_FQ2_MODE == 1
+    const Fq v0 = Fq::mul_c64(a.c0, b.c0);
+    const Fq v1 = Fq::mul_c64(a.c1, b.c1);
+    const Fq s = Fq::mul_c64(a.c0 + a.c1, b.c0 + b.c1);
+    return {v0 - v1, s - v0 - v1};
+#elif CSB_FQ2_MODE == 2
+    return mul_lazy(a, b);
+#else
     const Fq v0 = a.c0 * b.c0;
     const Fq v1 = a.c1 * b.c1;
     const Fq s = (a.c0 + a.c1) * (b.c0 + b.c1);
     return {v0 - v1, s - v0 - v1};
+#endif
+  }
+  // Karatsuba with lazy reduction: three 512-bit products, two Montgomery reductions.
+  //   c0 = a0 b0 - a1 b1 + p^2 (in [0, 2p^2)),  c1 = (a0+a1)(b0+b1) - a0 b0 - a1 b1 (< 2p^2)
+  // with the sums a0+a1, b0+b1 unreduced (< 2^255); both stay below p 2^256.
+  static CSB_DEV Fq2 mul_lazy(const Fq2& a, const Fq2& b) {
+    uint32_t v0[16], v1[16], s[16];
+    Fq::mul_full(v0, a.c0, b.c0);
+    Fq::mul_full(v1, a.c1, b.c1);
+    Fq sa, sb;
+    {
+      uint64_t ca = 0, cb = 0;
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        ca += (uint64_t)a.c0.v[i] + a.c1.v[i];
+        cb += (uint64_t)b.c0.v[i] + b.c1.v[i];
+        sa.v[i] = (uint32_t)ca;
+        sb.v[i] = (uint32_t)cb;
+        ca >>= 32;
+        cb >>= 32;
+      }
+    }
+    Fq::mul_full(s, sa, sb);
+    // s <- s - v0 - v1 ; v0 <- v0 - v1 + p^2
+    int64_t bs = 0, b0 = 0;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      bs += (int64_t)s[i] - v0[i] - v1[i];
+      b0 += (int64_t)v0[i] - v1[i] + ModQ::P2_LIMB(i);
+      s[i] = (uint32_t)bs;
+      v0[i] = (uint32_t)b0;
+      bs >>= 32;  // arithmetic shift: borrow in -2..0
+      b0 >>= 32;
+    }
+    return {Fq::redc(v0), Fq::redc(s)};
   }
   // (a0 + a1 u)^2 = (a0 + a1)(a0 - a1) + 2 a0 a1 u
   CSB_DEV Fq2 sqr() const {

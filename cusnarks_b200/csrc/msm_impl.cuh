@@ -204,8 +204,16 @@ __global__ void k_task_emit(const uint32_t* __restrict__ offsets, uint32_t nb, u
   }
 }
 
+// Minimum resident blocks per SM asked of the compiler for the accumulation kernel
+// (0 = no register cap).
+#ifndef CSB_ACC_G2_MINB
+#define CSB_ACC_G2_MINB 3  // 168 registers: 12 warps per SM instead of 8 (measured faster)
+#endif
+template <class F> struct AccMinBlocks { static constexpr int value = 0; };
+template <> struct AccMinBlocks<Fq2> { static constexpr int value = CSB_ACC_G2_MINB; };
+
 template <class F>
-__global__ void __launch_bounds__(128) k_accumulate(const Task* __restrict__ tasks,
+__global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate(const Task* __restrict__ tasks,
                                                     const uint32_t* __restrict__ counters,
                                                     const uint32_t* __restrict__ entries,
                                                     const uint32_t* __restrict__ points, uint32_t nb,
@@ -229,7 +237,29 @@ __global__ void __launch_bounds__(128) k_accumulate(const Task* __restrict__ tas
   }
 }
 
-// One block per split bucket: tree-sum its partials.
+// Split buckets with at most kCombineSerial partials: one thread each, a serial sum.
+// (The top window of a scalar has fewer bits, so its digits crowd into fewer buckets and
+// many of those split into two or three tasks.)
+constexpr uint32_t kCombineSerial = 8;
+
+template <class F>
+__global__ void __launch_bounds__(128) k_combine_small(const Multi* __restrict__ multi,
+                                                       const uint32_t* __restrict__ counters,
+                                                       const uint32_t* __restrict__ partials,
+                                                       uint32_t* __restrict__ buckets) {
+  constexpr int XW = 4 * FieldWords<F>::value;
+  const uint32_t nm = counters[2];
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < nm; m += gridDim.x * blockDim.x) {
+    const Multi mu = multi[m];
+    if (mu.count > kCombineSerial) continue;
+    XYZZ<F> acc = ld_xyzz<F>(partials + (size_t)mu.pbase * XW);
+#pragma unroll 1
+    for (uint32_t i = 1; i < mu.count; i++) acc = xyzz_add(acc, ld_xyzz<F>(partials + (size_t)(mu.pbase + i) * XW));
+    st_xyzz<F>(buckets + (size_t)mu.bucket * XW, acc);
+  }
+}
+
+// Split buckets with more partials: one block each, tree sum.
 template <class F>
 __global__ void __launch_bounds__(128) k_combine(const Multi* __restrict__ multi,
                                                  const uint32_t* __restrict__ counters,
@@ -240,6 +270,7 @@ __global__ void __launch_bounds__(128) k_combine(const Multi* __restrict__ multi
   const uint32_t nm = counters[2];
   for (uint32_t m = blockIdx.x; m < nm; m += gridDim.x) {
     const Multi mu = multi[m];
+    if (mu.count <= kCombineSerial) continue;  // k_combine_small
     XYZZ<F> acc = XYZZ<F>::inf();
 #pragma unroll 1
     for (uint32_t i = threadIdx.x; i < mu.count; i += blockDim.x)
@@ -313,6 +344,7 @@ __global__ void __launch_bounds__(128) k_reduce_level(const uint32_t* __restrict
   st_xyzz<F>(zout + ((size_t)j * nout + t) * XW, s);
 }
 
+
 template <class F>
 CSB_DEV XYZZ<F> shfl_down_xyzz(const XYZZ<F>& v, int d) {
   constexpr int XW = 4 * FieldWords<F>::value;
@@ -322,6 +354,50 @@ CSB_DEV XYZZ<F> shfl_down_xyzz(const XYZZ<F>& v, int d) {
 #pragma unroll
   for (int w = 0; w < XW; w++) ow[w] = __shfl_down_sync(0xffffffffu, vw[w], d);
   return o;
+}
+
+// Level k >= 1, warp-cooperative: one thread per element, the 8 lanes 8t..8t+7 hold
+// segment t (segments never straddle a warp).  With suf_i = sum_{i' >= i} y_i' (a 3-step
+// shuffle scan), the segment total is suf_0 and sum_i i*y_i = sum_{i >= 1} suf_i (a 3-step
+// tree), so the dependent chain is about 7 + 3k point operations instead of 26 + 3k.
+// Outputs as k_reduce_level.  Every lane runs the shuffles (no early return).
+template <class F>
+__global__ void __launch_bounds__(128) k_reduce_level_coop(const uint32_t* __restrict__ y,
+                                                           const uint32_t* __restrict__ z, uint32_t n,
+                                                           uint32_t nout, int W, int level,
+                                                           uint32_t* __restrict__ yout,
+                                                           uint32_t* __restrict__ zout) {
+  constexpr int XW = 4 * FieldWords<F>::value;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t per = nout * 8;  // padded elements per window
+  const uint32_t j = g / per, e = g % per, t = e >> 3;
+  const int i = (int)(e & 7);
+  const bool valid = j < (uint32_t)W && e < n;
+  const bool head = j < (uint32_t)W && i == 0;
+  const uint32_t* yj = y + (size_t)j * n * XW;
+  const uint32_t* zj = z + (size_t)j * n * XW;
+  XYZZ<F> suf = valid ? ld_xyzz<F>(yj + (size_t)e * XW) : XYZZ<F>::inf();
+#pragma unroll 1
+  for (int d = 1; d < 8; d <<= 1) {
+    const XYZZ<F> o = shfl_down_xyzz(suf, d);
+    if (i + d < 8) suf = xyzz_add(suf, o);
+  }
+  if (head) st_xyzz<F>(yout + ((size_t)j * nout + t) * XW, suf);
+  XYZZ<F> w = i >= 1 ? suf : XYZZ<F>::inf();
+#pragma unroll 1
+  for (int d = 4; d >= 1; d >>= 1) {
+    const XYZZ<F> o = shfl_down_xyzz(w, d);
+    if (i < d) w = xyzz_add(w, o);
+  }
+#pragma unroll 1
+  for (int k = 0; k < 3 * level; k++) w = xyzz_dbl(w);
+  XYZZ<F> zz = valid ? ld_xyzz<F>(zj + (size_t)e * XW) : XYZZ<F>::inf();
+#pragma unroll 1
+  for (int d = 4; d >= 1; d >>= 1) {
+    const XYZZ<F> o = shfl_down_xyzz(zz, d);
+    if (i < d) zz = xyzz_add(zz, o);
+  }
+  if (head) st_xyzz<F>(zout + ((size_t)j * nout + t) * XW, xyzz_add(zz, w));
 }
 
 // Per-window sum after levels 0..L-1.  With y_t the segment totals and z_t the weighted
@@ -450,8 +526,8 @@ __global__ void k_store_inf(uint32_t* out) {
 // counters block: [0] tasks, [1] partial slots, [2] split buckets; hist at +16 and
 // bin cursors at +96 (kMaxTask + 1 words each).
 constexpr int kCtrHist = 16, kCtrCursor = 96, kCtrWords = 192;
-// fixed-base reduction stops adding levels once a window has at most this many segments
-constexpr uint32_t kFixedTopSegments = 1024;
+// the reduction adds levels until a window has at most this many segments
+constexpr uint32_t kTopSegments = 256;
 
 struct Layout {
   size_t counts, offsets, entries, tasks, multi, partials, buckets, lv_y, lv_z, lv_y2, lv_z2, wsum,
@@ -468,7 +544,7 @@ inline Layout make_layout(uint32_t n, int c, int xyzz_bytes, uint32_t task_len, 
   const size_t max_tasks = nb + ne / task_len + 1;
   const size_t max_partials = 2 * (ne / task_len) + 1;
   const size_t n1 = ((size_t)1 << (c - 1)) / 8 + 1;
-  const size_t n2 = fixed ? n1 / 8 + 1 : 0;
+  const size_t n2 = (size_t)WR * (n1 / 8 + 1);
   Layout L{};
   size_t o = 0;
   L.counters = o; o = align256(o + kCtrWords * sizeof(uint32_t));
@@ -566,8 +642,9 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   k_accumulate<F><<<accumulate_grid<F>(sms), 128, 0, st>>>(tasks, counters, entries, d_points, nb,
                                                            buckets, partials);
   note_launch();
+  k_combine_small<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);
   k_combine<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);
-  note_launch();
+  note_launch(2);
   if (cfg.acc_stop) cudaEventRecord(cfg.acc_stop, st);
   // level 0: segments of 8 buckets -> totals y and in-segment weighted sums z
   const int WR = FIXED ? 1 : W;
@@ -578,10 +655,11 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   note_launch();
   int levels = 1;
   uint32_t *y = lv_y, *z = lv_z, *y2 = lv_y2, *z2 = lv_z2;
-  // fixed-base: one bucket set of 2^(c-1); more levels keep the single top block short
-  while (FIXED && nseg > kFixedTopSegments) {
+  // more (warp-cooperative) levels keep the top block's chain short
+  while (nseg > kTopSegments) {
     const uint32_t nnext = (nseg + 7) / 8;
-    k_reduce_level<F><<<(nnext + 127) / 128, 128, 0, st>>>(y, z, nseg, nnext, 1, levels, y2, z2);
+    const uint32_t threads = (uint32_t)WR * nnext * 8;
+    k_reduce_level_coop<F><<<(threads + 127) / 128, 128, 0, st>>>(y, z, nseg, nnext, WR, levels, y2, z2);
     note_launch();
     uint32_t* ty = y; y = y2; y2 = ty;
     uint32_t* tz = z; z = z2; z2 = tz;

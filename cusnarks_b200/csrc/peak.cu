@@ -122,7 +122,68 @@ __global__ void __launch_bounds__(256) k_alu(uint32_t seed, uint32_t* sink) {
   if (x == 0x9e3779b9u) sink[0] = x;
 }
 
+// Latency probe: one thread runs CHAINS independent dependent chains x <- x * y, with
+// the flag-carry CIOS (VARIANT 0), the wide-product CIOS (1) or the carry-flag-free
+// 64-bit CIOS (2); or XYZZ point additions acc <- acc + p (VARIANT 3: wide, 4: c64).
+template <int VARIANT, int CHAINS>
+__global__ void k_mul_latency(const uint32_t* __restrict__ seed, uint32_t* sink, int iters) {
+  using csb::Fq;
+  Fq x[CHAINS], y;
+#pragma unroll
+  for (int k = 0; k < CHAINS; k++)
+#pragma unroll
+    for (int i = 0; i < 8; i++) x[k].v[i] = (seed[i] ^ (k * 977u)) & (i == 7 ? 0x0fffffffu : 0xffffffffu);
+#pragma unroll
+  for (int i = 0; i < 8; i++) y.v[i] = seed[8 + i] & (i == 7 ? 0x0fffffffu : 0xffffffffu);
+#pragma unroll 1
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int k = 0; k < CHAINS; k++)
+      x[k] = VARIANT == 0 ? Fq::mul_lohi(x[k], y) : VARIANT == 1 ? Fq::mul_wide(x[k], y) : Fq::mul_c64(x[k], y);
+  }
+  uint32_t h = 0;
+#pragma unroll
+  for (int k = 0; k < CHAINS; k++)
+#pragma unroll
+    for (int i = 0; i < 8; i++) h ^= x[k].v[i];
+  if (h == 0x12345u) sink[0] = h;
+}
+
 }  // namespace
+
+// Nanoseconds per Montgomery product for one thread running `chains` (1 or 4) independent
+// chains; variant 0 flag-carry, 1 wide-product, 2 carry-flag-free 64-bit CIOS.
+extern "C" int cs_bench_mul_latency(cs_ctx* ctx, int variant, int chains, double* ns_per_mul) {
+  if (!ctx || !ns_per_mul || variant < 0 || variant > 2 || (chains != 1 && chains != 4)) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaError_t e = ctx->out.reserve(256, ctx->stream);
+  if (e != cudaSuccess) return csb::fail(ctx, e, "latency probe buffer");
+  uint32_t* buf = static_cast<uint32_t*>(ctx->out.ptr);
+  if ((e = cudaMemsetAsync(buf, 0x5a, 256, ctx->stream)) != cudaSuccess) return csb::fail(ctx, e, "latency probe init");
+  const int iters = 2000;
+  float best = 1e30f;
+  for (int rep = 0; rep < 3; rep++) {
+    cudaEventRecord(ctx->ev_start, ctx->stream);
+    if (chains == 1) {
+      if (variant == 0) k_mul_latency<0, 1><<<1, 1, 0, ctx->stream>>>(buf, buf + 32, iters);
+      else if (variant == 1) k_mul_latency<1, 1><<<1, 1, 0, ctx->stream>>>(buf, buf + 32, iters);
+      else k_mul_latency<2, 1><<<1, 1, 0, ctx->stream>>>(buf, buf + 32, iters);
+    } else {
+      if (variant == 0) k_mul_latency<0, 4><<<1, 1, 0, ctx->stream>>>(buf, buf + 32, iters);
+      else if (variant == 1) k_mul_latency<1, 4><<<1, 1, 0, ctx->stream>>>(buf, buf + 32, iters);
+      else k_mul_latency<2, 4><<<1, 1, 0, ctx->stream>>>(buf, buf + 32, iters);
+    }
+    csb::note_launch();
+    cudaEventRecord(ctx->ev_stop, ctx->stream);
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return csb::fail(ctx, e, "latency probe kernel");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+    if (rep > 0 && ms < best) best = ms;
+  }
+  *ns_per_mul = (double)best * 1e6 / ((double)iters * chains);
+  return CS_OK;
+}
 
 extern "C" int cs_bench_mulmod(cs_ctx* ctx, int variant, double* mulmods_per_s) {
   if (!ctx || !mulmods_per_s || variant < 0 || variant > 2) return CS_ERR_ARG;

@@ -80,20 +80,33 @@ class SyntheticCircuit:
         self.n_inputs = n_inputs
         self.n_vars = nv = n_inputs + nc
         rng = np.random.Generator(np.random.PCG64(seed))
-        # layers: constraint c may read wires below the first output of its layer
+        # Layers of S constraints; a constraint reads wires below the first output of its
+        # layer, so the witness is computed layer by layer.  One A index and one B index
+        # of each constraint are forced onto the previous layer's wires (a bijection when
+        # the layers have equal size), so every wire except the last layer's outputs
+        # (S of them) appears in A and in B, as in a real circuit; the other two indices
+        # are uniform over the available wires.
+        S = 1 << max(6, (log_m + 4) // 2)
         bounds = []
-        c0, avail = 0, n_inputs
+        c0, prev0, prev_n = 0, 0, n_inputs
         while c0 < nc:
-            c1 = min(nc, c0 + avail)
-            bounds.append((c0, c1, avail))
-            avail += c1 - c0
+            c1 = min(nc, c0 + S)
+            bounds.append((c0, c1, n_inputs + c0, prev0, prev_n))
+            prev0, prev_n = n_inputs + c0, c1 - c0
             c0 = c1
         self.layers = bounds
         hi = np.empty(nc, dtype=np.int64)
-        for c0, c1, av in bounds:
+        fa = np.empty(nc, dtype=np.int64)
+        fb = np.empty(nc, dtype=np.int64)
+        for c0, c1, av, p0, pn in bounds:
+            j = np.arange(c1 - c0)
             hi[c0:c1] = av
+            fa[c0:c1] = p0 + j % pn
+            fb[c0:c1] = p0 + (7 * j + 3) % pn
         self.a_wire = rng.integers(0, hi[:, None], size=(nc, 3)).astype(np.uint32)
         self.b_wire = rng.integers(0, hi[:, None], size=(nc, 3)).astype(np.uint32)
+        self.a_wire[:, 0] = fa
+        self.b_wire[:, 1] = fb
         L = lib()
         # coefficients: uniform Fr, stored Montgomery (as the reference's mpolys are)
         coeff = synth.random_field(rng, 6 * nc)
@@ -112,7 +125,7 @@ class SyntheticCircuit:
         da_wire, db_wire = _t(self.a_wire.reshape(-1)), _t(self.b_wire.reshape(-1))
         da_coeff, db_coeff = _t(self.a_coeff.reshape(-1)), _t(self.b_coeff.reshape(-1))
         doff = _t(np.arange(0, 3 * nc + 1, 3, dtype=np.uint32))
-        for c0, c1, _ in bounds:
+        for c0, c1, *_ in bounds:
             check(L.cs_r1cs_layer_eval(ctx.handle, _vp(doff.data_ptr() + 4 * c0), _vp(da_wire.data_ptr()),
                                        _vp(da_coeff.data_ptr()), _vp(doff.data_ptr() + 4 * c0),
                                        _vp(db_wire.data_ptr()), _vp(db_coeff.data_ptr()), c1 - c0,

@@ -332,6 +332,9 @@ int cs_bench_pipe(cs_ctx *ctx, int mode, double *ops_per_s);
 /* Montgomery products per second (variant 0: mad.lo/mad.hi CIOS, 1: wide-product CIOS;
  * variant 2 reports 32-bit add-with-carry instructions per second instead). */
 int cs_bench_mulmod(cs_ctx *ctx, int variant, double *rate);
+/* Single-thread latency, ns per Montgomery product, of `chains` (1 or 4) independent
+ * dependent chains: variant 0 flag-carry CIOS, 1 wide-product CIOS, 2 carry-flag-free CIOS. */
+int cs_bench_mul_latency(cs_ctx *ctx, int variant, int chains, double *ns_per_mul);
 /* Number of kernels this library has launched in the process so far. */
 unsigned long long cs_kernel_launches(void);
 
