@@ -10,14 +10,22 @@ all ranks (weak scaling).
 
 Workload (the configuration the headline metric is quoted on): full Groth16 prove for a
 synthetic R1CS of 2^20 constraints (nConstraints = 2^20 - 2, one public input, A and B rows
-with 3 nonzeros at random wires with uniform random Fr coefficients, C row = one output wire
-set to (A.w)(B.w)); proving key from seeded toxic waste, resident in HBM; fixed r, s.
-One step = one proof from a device-resident witness; device time from CUDA events around
-the whole proof.  Also reported: one BN128 G1 MSM of 2^20 terms (``g1_msm_2^20_ms``), whose
-bucket-accumulation kernel -- the dominant kernel of every proof -- carries the roofline.
+with 3 nonzeros with uniform random Fr coefficients over earlier wires -- every wire but the
+last layer's is read in A and in B -- C row = one output wire set to (A.w)(B.w)); proving key
+from seeded toxic waste, resident in HBM with its fixed-base MSM tables; fixed r, s.
 
-``e2e`` goes through the public C ABI (cs_prove) with the witness in pinned host memory and
-the proof copied back, wall clock per proof.
+``value``: the served engine -- one step = one proof from a device-resident witness, K proofs
+overlapped across --slots contexts, device time (CUDA events on a marker stream) around all K.
+``e2e``: the same through the public C ABI prove server (cs_server_*), witness in host
+memory, proof back in host memory, K requests submitted at once, wall clock.
+``latency_ms``: p50/p99 submit -> proof through the server under Poisson arrivals at 70% of
+that saturated rate.  ``single_proof``: one proof per call (cs_prove_device), device time.
+``plain_per_call``: the reference's flow through the drop-in entry points (mpoly_eval_server_h,
+ntt_interpolandmul_server_h, ec_jacreduce_server_h per MSM with the key points copied per
+call), wall clock; ``served_vs_plain`` = e2e / plain.  ``served_mix``: 8 circuits of
+2^12..2^20 constraints (log-uniform, seeded), requests uniform over them, saturation and
+Poisson 50% / 90% with p50/p99.  Also one BN128 G1 MSM of 2^20 terms (``g1_msm_2^20_ms``),
+whose bucket-accumulation kernel -- the dominant kernel of every proof -- carries the roofline.
 
 ``cpu_baseline`` / ``--impl reference``: the reference's own CPU library (oracle/_ref,
 built from the reference sources; the C restatement when that library is absent) runs the
@@ -236,6 +244,110 @@ class MsmWorkload:
         return self.n * lib().cs_msm_num_windows(c), c
 
 
+class ServedDevice:
+    """Proofs from a device-resident witness overlapped across `slots` contexts (each with
+    its own streams and scratch): the served engine without the host copies."""
+
+    def __init__(self, wl, slots: int):
+        import torch
+        from cusnarks_b200 import Context
+        self.wl = wl
+        self.ctxs = [wl.ctx] + [Context(wl.ctx.device) for _ in range(slots - 1)]
+        dev = torch.device("cuda", wl.ctx.device)
+        self.proofs = [torch.zeros(64, dtype=torch.int32, device=dev) for _ in self.ctxs]
+
+    def run(self, k: int):
+        from cusnarks_b200._lib import lib, check
+        wl = self.wl
+        for i in range(k):
+            j = i % len(self.ctxs)
+            c = self.ctxs[j]
+            check(lib().cs_prove_device(c.handle, wl.prover.handle, _vp(wl.d_w.data_ptr()), wl.r.ctypes.data,
+                                        wl.s.ctypes.data, _vp(self.proofs[j].data_ptr())), c.handle)
+        for c in self.ctxs:
+            c.sync()
+
+    def close(self):
+        for c in self.ctxs[1:]:
+            c.close()
+
+
+def _vp(x):
+    import ctypes
+    return ctypes.c_void_p(x)
+
+
+def device_span_ms(fn):
+    """Device time (CUDA events on a marker stream) around fn(), which synchronises."""
+    import torch
+    s = torch.cuda.Stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(s)
+    fn()
+    torch.cuda.synchronize()
+    b.record(s)
+    b.synchronize()
+    return a.elapsed_time(b)
+
+
+def served_run(srv, jobs, rate_hz=None, seed=0):
+    """Submits jobs [(key, w, r, s)] all at once (rate_hz None) or as a Poisson stream;
+    returns (wall seconds first submit -> last proof, latencies ms)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    t0 = time.perf_counter()
+    tickets = []
+    at = 0.0
+    for key, w, r, s in jobs:
+        if rate_hz:
+            at += rng.exponential(1.0 / rate_hz)
+            dt = t0 + at - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+        tickets.append(srv.submit(key, w, r, s))
+    lat = []
+    for t in tickets:
+        _, info = srv.wait(t)
+        lat.append(info["latency_ms"])
+    return time.perf_counter() - t0, lat
+
+
+def served_mix(ctx, slots: int, n_requests: int, seed: int = 5):
+    """Config 5: 8 circuits of 2^12..2^20 constraints (log-uniform, seeded), keys resident,
+    requests over them (uniform) at Poisson rates 50% / 90% of the measured saturation."""
+    from cusnarks_b200.groth import SyntheticCircuit, setup_pk, Prover
+    from cusnarks_b200.server import ProveServer
+    from cusnarks_b200.synth import to_limbs
+    rng = np.random.Generator(np.random.PCG64(seed))
+    logs = sorted(int(x) for x in rng.integers(12, 21, 8))
+    circs, provers = [], []
+    for i, lm in enumerate(logs):
+        c = SyntheticCircuit(ctx, lm, seed=300 + i)
+        circs.append(c)
+        provers.append(Prover(ctx, setup_pk(ctx, c, seed=400 + i)))
+    srv = ProveServer(ctx.device, slots=slots, reserve_bytes=1 << 30)
+    keys = [srv.add_key(p) for p in provers]
+    r, s = to_limbs(0x1234567890abcdef), to_limbs(0xfedcba0987654321)
+    pick = rng.integers(0, 8, n_requests)
+    jobs = [(keys[k], circs[k].w, r, s) for k in pick]
+    served_run(srv, jobs[:16])                    # warm every slot's scratch and twiddles
+    wall, lat = served_run(srv, jobs)
+    sat = len(jobs) / wall
+    out = {"circuits_log2": logs, "slots": slots, "requests": len(jobs),
+           "saturation": {"proofs_per_s": round(sat, 2), "p50_ms": round(pct(lat, 50), 2),
+                          "p99_ms": round(pct(lat, 99), 2), "arrivals": "all at once"}}
+    for frac in (0.5, 0.9):
+        wall, lat = served_run(srv, jobs, rate_hz=frac * sat, seed=seed + int(frac * 10))
+        out[f"poisson_{int(frac * 100)}pct"] = {"rate_hz": round(frac * sat, 2),
+                                                "proofs_per_s": round(len(jobs) / wall, 2),
+                                                "p50_ms": round(pct(lat, 50), 2), "p99_ms": round(pct(lat, 99), 2)}
+    out["max_concurrent"] = srv.stats()["max_concurrent"]
+    srv.close()
+    for p in provers:
+        p.close()
+    return out
+
+
 def run_ours(args, world, rank, local):
     import torch
     from cusnarks_b200 import Context
@@ -243,29 +355,54 @@ def run_ours(args, world, rank, local):
     ctx = Context(local)
     peak_imad = ctx.imad_peak()
     wl = ProveWorkload(ctx, LOG_M, seed=100 + rank)
+    sd = ServedDevice(wl, args.slots)
+    # one proof per call (resident key): lone-proof device latency
     for _ in range(args.warmup):
         wl.step()
-    wl.l2_flush()
+    single = []
+    for _ in range(args.steps):
+        wl.l2_flush()
+        single.append(wl.step())
+    # served engine, device witness: `steps` proofs overlapped across the slots
+    for _ in range(args.warmup):
+        sd.run(args.slots)
     sampler = ClockSampler(local) if rank == 0 else None
     barrier(world)
     torch.cuda.synchronize()
     if sampler:
         sampler.start()
     l0 = kernel_launches()
-    dev_ms = []
-    for _ in range(args.steps):
-        dev_ms.append(wl.step())
-        wl.l2_flush()
+    span = device_span_ms(lambda: sd.run(args.steps))
     launches = kernel_launches() - l0
-    torch.cuda.synchronize()
     barrier(world)
     clocks = sampler.stop() if sampler else None
-    total_ms = max_over_ranks(sum(dev_ms), world)
+    total_ms = max_over_ranks(span, world)
     ms_per_step = total_ms / args.steps
     value = world * 1e3 / ms_per_step
-    # end-to-end through the C ABI with host buffers
-    e2e = [wl.e2e_step() for _ in range(max(3, args.steps // 2))]
-    e2e_ms = max_over_ranks(statistics.median(e2e), world)
+    sd.close()
+    # end to end: the C-ABI server, host witness in, proof out to host
+    from cusnarks_b200.server import ProveServer
+    srv = ProveServer(local, slots=args.slots, reserve_bytes=1 << 30)
+    key = srv.add_key(wl.prover)
+    jobs = [(key, wl.circ.w, wl.r, wl.s)] * args.steps
+    served_run(srv, jobs[:args.slots])
+    wall, lat_sat = served_run(srv, jobs)
+    e2e_ms = max_over_ranks(wall * 1e3 / len(jobs), world)
+    # latency under a Poisson stream at 70% of the saturated rate
+    wall_p, lat = served_run(srv, jobs * max(4, 40 // len(jobs)), rate_hz=0.7 * 1e3 / e2e_ms, seed=11)
+    srv.close()
+    # plain per-call path: the reference's flow through the drop-in entry points
+    from cusnarks_b200.groth import pk_to_host
+    from cusnarks_b200.plain import PlainProver
+    plain = PlainProver(pk_to_host(wl.pk))
+    rr, ss = int.from_bytes(wl.r.tobytes(), "little"), int.from_bytes(wl.s.tobytes(), "little")
+    plain.prove(wl.circ.w, rr, ss)
+    t0 = time.perf_counter()
+    n_plain = 2
+    for _ in range(n_plain):
+        plain.prove(wl.circ.w, rr, ss)
+    plain_ms = (time.perf_counter() - t0) * 1e3 / n_plain
+    del plain
     # the 2^20 G1 MSM and its dominant kernel
     mw = MsmWorkload(ctx, 20, seed=7 + rank)
     for _ in range(3):
@@ -279,6 +416,7 @@ def run_ours(args, world, rank, local):
     units, window = mw.dominant_units()
     acc = statistics.mean(acc_ms)
     achieved = units * 11 * IMAD_PER_MONT / (acc * 1e-3)
+    e2e_val = world * 1e3 / e2e_ms
     line = {
         "metric": METRIC,
         "value": round(value, 3),
@@ -291,13 +429,24 @@ def run_ours(args, world, rank, local):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "u32x8 (256-bit Montgomery integers)",
-        "data": "synthetic: seeded R1CS (3 nonzeros per A/B row), seeded toxic waste, GPU-generated key",
-        "config": {"workload": "Groth16 prove, synthetic R1CS 2^20 constraints (domain 2^20), "
-                               "proving key resident in HBM, fixed r,s",
-                   "n_vars": wl.circ.n_vars, "domain": 1 << LOG_M, "path": "plain (one proof per call)",
-                   "l2": "flushed between timed steps (2x L2 write)"},
-        "latency_ms": {"p50": round(pct(dev_ms, 50), 3), "p99": round(pct(dev_ms, 99), 3),
-                       "basis": "device time per proof, plain per-call path"},
+        "data": "synthetic: seeded R1CS (3 nonzeros per A/B row, every wire used), seeded toxic waste, "
+                "GPU-generated key",
+        "config": {"workload": "Groth16 prove, synthetic R1CS 2^20 constraints (domain 2^20), proving key "
+                               "and fixed-base tables resident in HBM, fixed r,s",
+                   "n_vars": wl.circ.n_vars, "domain": 1 << LOG_M,
+                   "path": f"served engine: proofs overlapped over {args.slots} slots, device witness",
+                   "l2": "inputs larger than L2 (proving key + tables ~6 GB)"},
+        "latency_ms": {"p50": round(pct(lat, 50), 3), "p99": round(pct(lat, 99), 3),
+                       "basis": "served (C-ABI server, host witness), Poisson arrivals at 70% of the "
+                                "saturated rate, 2^20 circuit, submit -> proof in host memory"},
+        "single_proof": {"proofs_per_s": round(1e3 / statistics.median(single), 3),
+                         "p50_ms": round(pct(single, 50), 3), "p99_ms": round(pct(single, 99), 3),
+                         "basis": "one proof per call (cs_prove_device), device time"},
+        "plain_per_call": {"proofs_per_s": round(1e3 / plain_ms, 3), "ms": round(plain_ms, 1),
+                           "basis": "the reference's flow through the drop-in entry points: mpoly_eval, "
+                                    "ntt_interpolandmul, 6 ec_jacreduce calls with host scalars and key "
+                                    "points copied per call; wall clock"},
+        "served_vs_plain": round(e2e_val * plain_ms / 1e3, 2),
         "g1_msm_2^20_ms": round(statistics.median(msm_ms), 3),
         "roofline": {"bound": "int (IMAD pipe)", "kernel": "k_accumulate+k_combine (MSM bucket accumulation)",
                      "achieved": round(achieved / 1e12, 4), "peak": round(peak_imad / 1e12, 4),
@@ -305,11 +454,15 @@ def run_ours(args, world, rank, local):
                      "kernel_ms": round(acc, 4), "units_per_launch": units, "window": window,
                      "basis": "2^20 G1 MSM: N*W entries x 11 Montgomery products x 264 IMAD / kernel ms "
                               "(CUDA events around the kernels); peak = live IMAD microbenchmark"},
-        "e2e": {"value": round(world * 1e3 / e2e_ms, 3), "unit": UNIT, "ms": round(e2e_ms, 3),
-                "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes},
+        "e2e": {"value": round(e2e_val, 3), "unit": UNIT, "ms": round(e2e_ms, 3),
+                "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes,
+                "basis": f"C-ABI prove server ({args.slots} slots), {len(jobs)} requests submitted at once, "
+                         "host witness in, proof out; wall clock"},
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if rank == 0 and not args.no_mix:
+        line["served_mix"] = served_mix(ctx, args.slots, args.mix_requests)
     if rank == 0 and world == 1 and not args.no_cpu:
         sec, kind, threads = cpu_reference_prove_sample(ctx, CPU_SAMPLE_LOG_M, seed=55)
         scaled = sec * (1 << (LOG_M - CPU_SAMPLE_LOG_M))
@@ -355,6 +508,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--slots", type=int, default=3, help="concurrent proofs of the served engine")
+    ap.add_argument("--no-mix", action="store_true", help="skip the mixed-size served leg")
+    ap.add_argument("--mix-requests", type=int, default=96)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -18,6 +18,7 @@ CS_ERR_ARG = 2
 CS_ERR_NOMEM = 3
 CS_ERR_UNSUPPORTED = 4
 CS_ERR_NODEVICE = 5
+CS_ERR_TIMEOUT = 6
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _vp = ctypes.c_void_p
@@ -27,6 +28,17 @@ class CsError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"cusnarks_b200 error {code}: {msg}")
         self.code = code
+
+
+class ServerResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("queue_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
+                ("device_ms", ctypes.c_float)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
+                ("queued", ctypes.c_uint64), ("running", ctypes.c_uint32), ("max_concurrent", ctypes.c_uint32),
+                ("promised_bytes", ctypes.c_size_t)]
 
 
 class MpolyEval(ctypes.Structure):
@@ -124,6 +136,13 @@ _SIGNATURES = [
     ("cs_pk_fixed_window", ctypes.c_int, [_vp, ctypes.c_int]),
     ("cs_prove", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     ("cs_prove_device", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    ("cs_server_create", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(_vp)]),
+    ("cs_server_destroy", None, [_vp]),
+    ("cs_server_add_key", ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_int)]),
+    ("cs_server_submit", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_uint64)]),
+    ("cs_server_wait", ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(ServerResult)]),
+    ("cs_server_stats", ctypes.c_int, [_vp, ctypes.POINTER(ServerStats)]),
+    ("cs_server_error", ctypes.c_char_p, [_vp]),
     ("cs_setup_lagrange", ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp]),
     ("cs_setup_wire_eval", ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32, _vp]),
     ("cs_setup_c_scalars", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_uint32, _vp]),

@@ -188,6 +188,7 @@ ProvePlan plan_prove(const cs_pk* pk) {
 
 namespace csb {
 size_t prove_workspace_bytes(const cs_pk* pk) { return plan_prove(pk).total; }
+uint32_t pk_n_vars(const cs_pk* pk) { return pk->n_vars; }
 }  // namespace csb
 
 extern "C" {

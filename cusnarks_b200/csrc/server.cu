@@ -1,0 +1,287 @@
+// server.cu -- continuous-batching Groth16 prove server (host code).
+//
+// Replaces the reference's single-proof-at-a-time TCP server loop (src/python/
+// groth_prover.py:808-891 startServer, which drops requests that arrive while a proof is
+// running and re-copies the proving key to the GPU for every proof).  Here:
+//   * proving keys stay resident in HBM (cs_pk, with their fixed-base MSM tables), and the
+//     NTT twiddles stay resident in each slot's context;
+//   * requests queue FIFO; each of `slots` worker threads owns a context (its own streams
+//     and scratch arena) and takes the next request as soon as it is free AND the request
+//     is admitted by device memory: free memory (cudaMemGetInfo) minus the bytes already
+//     promised to admitted requests must cover the slot's scratch growth plus `reserve`;
+//   * admitted proofs run concurrently on the device: one proof's MSM tails, QAP and
+//     H step overlap the next one's bucket accumulation.
+// Results do not depend on the mix: every proof is computed by the same kernels on its
+// own slot scratch (a test compares proofs made alone and in a mix, byte for byte).
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/cusnarks_b200.h"
+#include "runtime.cuh"
+
+namespace csb {
+size_t prove_workspace_bytes(const cs_pk* pk);
+uint32_t pk_n_vars(const cs_pk* pk);
+}  // namespace csb
+
+namespace {
+
+double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Request {
+  uint64_t id = 0;
+  int key = 0;
+  cs_pk* pk = nullptr;
+  const uint32_t* w = nullptr;
+  uint32_t r[8], s[8];
+  uint32_t* proof = nullptr;
+  int status = CS_OK;
+  bool done = false;
+  double t_submit = 0, t_start = 0, t_end = 0;
+  float device_ms = 0.f;
+  std::string err;
+};
+
+}  // namespace
+
+struct cs_server {
+  int device = 0;
+  int nslots = 0;
+  size_t reserve = 0;
+  std::vector<cs_pk*> keys;
+  std::deque<std::shared_ptr<Request>> queue;
+  std::unordered_map<uint64_t, std::shared_ptr<Request>> live;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::vector<std::thread> workers;
+  bool stop = false;
+  uint64_t next_id = 1;
+  int busy = 0;
+  size_t promised = 0;  // scratch growth admitted but not yet allocated
+  // statistics
+  uint64_t completed = 0, failed = 0, rejected = 0;
+  int max_concurrent = 0;
+  double busy_since = 0, first_start = -1, last_end = 0;
+  std::string err;
+
+  void worker(int slot);
+};
+
+namespace {
+
+// Bytes a slot must still allocate to run a proof with key pk (its arenas only grow).
+size_t growth(const cs_ctx* ctx, const cs_pk* pk, size_t pinned_have) {
+  const size_t ws = csb::prove_workspace_bytes(pk);
+  const size_t in = (size_t)csb::pk_n_vars(pk) * 32 + 512;
+  size_t g = 0;
+  if (ws > ctx->work.bytes) g += ws + ws / 8;
+  if (in > ctx->in.bytes) g += in + in / 8;
+  (void)pinned_have;
+  return g;
+}
+
+}  // namespace
+
+void cs_server::worker(int slot) {
+  (void)slot;
+  cudaSetDevice(device);
+  cs_ctx* ctx = nullptr;
+  if (cs_ctx_create(device, &ctx) != CS_OK) {
+    std::lock_guard<std::mutex> lk(mu);
+    err = "server slot: context creation failed";
+    return;
+  }
+  csb::PinnedBuffer stage;
+  for (;;) {
+    std::shared_ptr<Request> rq;
+    size_t need = 0;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      for (;;) {
+        if (stop) {
+          lk.unlock();
+          stage.release();
+          cs_ctx_destroy(ctx);
+          return;
+        }
+        if (!queue.empty()) {
+          need = growth(ctx, queue.front()->pk, stage.bytes);
+          size_t free_b = 0, total_b = 0;
+          cudaMemGetInfo(&free_b, &total_b);
+          const size_t avail = free_b > promised ? free_b - promised : 0;
+          if (need == 0 || avail >= need + reserve) break;
+          if (busy == 0) {  // nothing will free memory: refuse the head request
+            auto bad = queue.front();
+            queue.pop_front();
+            bad->status = CS_ERR_NOMEM;
+            bad->err = "admission: proof scratch (" + std::to_string(need) + " bytes) does not fit in free device memory";
+            bad->done = true;
+            rejected++;
+            cv_done.notify_all();
+            continue;
+          }
+        }
+        cv_work.wait(lk);
+      }
+      rq = queue.front();
+      queue.pop_front();
+      promised += need;
+      busy++;
+      if (busy > max_concurrent) max_concurrent = busy;
+      rq->t_start = now_ms();
+      if (first_start < 0) first_start = rq->t_start;
+    }
+    cs_pk* pk = rq->pk;
+    const size_t wbytes = (size_t)csb::pk_n_vars(pk) * 32;
+    int st = CS_OK;
+    std::string msg;
+    if (stage.reserve(wbytes) != cudaSuccess) {
+      st = CS_ERR_NOMEM;
+      msg = "server: pinned staging buffer";
+    } else {
+      std::memcpy(stage.ptr, rq->w, wbytes);
+      st = cs_prove(ctx, pk, static_cast<const uint32_t*>(stage.ptr), rq->r, rq->s, rq->proof);
+      if (st != CS_OK) msg = cs_ctx_error(ctx);
+    }
+    const float dev_ms = cs_ctx_last_ms(ctx);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      promised = promised > need ? promised - need : 0;
+      busy--;
+      rq->status = st;
+      rq->err = msg;
+      rq->device_ms = dev_ms;
+      rq->t_end = now_ms();
+      rq->done = true;
+      last_end = rq->t_end;
+      if (st == CS_OK) completed++; else failed++;
+    }
+    cv_done.notify_all();
+    cv_work.notify_all();
+  }
+}
+
+extern "C" {
+
+int cs_server_create(int device, int slots, size_t reserve_bytes, cs_server** out) {
+  if (!out || slots < 1 || slots > 64) return CS_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return CS_ERR_NODEVICE;
+  }
+  if (device < 0 || device >= ndev) return CS_ERR_ARG;
+  std::unique_ptr<cs_server> s(new cs_server());
+  s->device = device;
+  s->nslots = slots;
+  s->reserve = reserve_bytes;
+  for (int i = 0; i < slots; i++) s->workers.emplace_back(&cs_server::worker, s.get(), i);
+  *out = s.release();
+  return CS_OK;
+}
+
+void cs_server_destroy(cs_server* s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    for (auto& rq : s->queue) {
+      rq->status = CS_ERR_ARG;
+      rq->err = "server stopped before the request ran";
+      rq->done = true;
+    }
+    s->queue.clear();
+  }
+  s->cv_work.notify_all();
+  s->cv_done.notify_all();
+  for (auto& t : s->workers) t.join();
+  delete s;
+}
+
+int cs_server_add_key(cs_server* s, cs_pk* pk, int* key_id) {
+  if (!s || !pk || !key_id) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->keys.push_back(pk);
+  *key_id = (int)s->keys.size() - 1;
+  return CS_OK;
+}
+
+int cs_server_submit(cs_server* s, int key_id, const uint32_t* w, const uint32_t* r, const uint32_t* sv,
+                     uint32_t* proof, uint64_t* ticket) {
+  if (!s || !w || !r || !sv || !proof || !ticket) return CS_ERR_ARG;
+  auto rq = std::make_shared<Request>();
+  rq->key = key_id;
+  rq->w = w;
+  std::memcpy(rq->r, r, 32);
+  std::memcpy(rq->s, sv, 32);
+  rq->proof = proof;
+  rq->t_submit = now_ms();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (key_id < 0 || key_id >= (int)s->keys.size()) return CS_ERR_ARG;
+    rq->pk = s->keys[key_id];
+    if (s->stop) return CS_ERR_ARG;
+    rq->id = s->next_id++;
+    s->live[rq->id] = rq;
+    s->queue.push_back(rq);
+    *ticket = rq->id;
+  }
+  s->cv_work.notify_one();
+  return CS_OK;
+}
+
+int cs_server_wait(cs_server* s, uint64_t ticket, double timeout_s, cs_server_result* res) {
+  if (!s) return CS_ERR_ARG;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->live.find(ticket);
+  if (it == s->live.end()) return CS_ERR_ARG;
+  auto rq = it->second;
+  const auto deadline = std::chrono::steady_clock::now() +
+                        std::chrono::microseconds((long long)(timeout_s * 1e6));
+  while (!rq->done) {
+    if (timeout_s < 0) {
+      s->cv_done.wait(lk);
+    } else if (s->cv_done.wait_until(lk, deadline) == std::cv_status::timeout && !rq->done) {
+      return CS_ERR_TIMEOUT;
+    }
+  }
+  s->live.erase(ticket);
+  if (res) {
+    res->status = rq->status;
+    res->queue_ms = rq->t_start > 0 ? rq->t_start - rq->t_submit : 0;
+    res->latency_ms = rq->t_end > 0 ? rq->t_end - rq->t_submit : 0;
+    res->device_ms = rq->device_ms;
+  }
+  if (rq->status != CS_OK) s->err = rq->err;
+  return rq->status;
+}
+
+int cs_server_stats(cs_server* s, cs_server_counters* st) {
+  if (!s || !st) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  st->completed = s->completed;
+  st->failed = s->failed;
+  st->rejected = s->rejected;
+  st->queued = s->queue.size();
+  st->running = (uint32_t)s->busy;
+  st->max_concurrent = (uint32_t)s->max_concurrent;
+  st->promised_bytes = s->promised;
+  return CS_OK;
+}
+
+const char* cs_server_error(cs_server* s) { return s ? s->err.c_str() : "null server"; }
+
+}  // extern "C"

@@ -36,6 +36,7 @@ extern "C" {
 #define CS_ERR_NOMEM 3       /* device or pinned allocation failed */
 #define CS_ERR_UNSUPPORTED 4 /* option the GPU path does not implement */
 #define CS_ERR_NODEVICE 5    /* no CUDA device */
+#define CS_ERR_TIMEOUT 6     /* a wait ran out of time (the request is still pending) */
 
 /* ------------------------------------------- reference argument structs (layouts) --- */
 /* jacadd_reduced_t, reference src/cuda/types.h:548-567 (same member order and types). */
@@ -297,6 +298,40 @@ int cs_prove(cs_ctx *ctx, cs_pk *pk, const uint32_t *w, const uint32_t *r, const
              uint32_t *proof);
 int cs_prove_device(cs_ctx *ctx, cs_pk *pk, const uint32_t *d_w, const uint32_t *r, const uint32_t *s,
                     uint32_t *d_proof);
+
+/* ----------------------------------------------- served proving (continuous batching) */
+/* Replaces the reference's one-proof-at-a-time server loop (groth_prover.py:808-891
+ * startServer, which drops requests that arrive while a proof runs and re-copies the
+ * proving key per proof).  `slots` worker threads each own a context (streams, scratch
+ * arena, twiddles); requests queue FIFO and start as soon as a slot is free and free
+ * device memory minus the bytes promised to admitted requests covers the slot's scratch
+ * growth plus reserve_bytes.  Admitted proofs run concurrently on the device.  A request
+ * whose scratch can never fit (no proof running) fails with CS_ERR_NOMEM.
+ * Keys (cs_pk, created on the same device) must outlive the server.  w and proof
+ * (host memory, as cs_prove) must stay valid until cs_server_wait returns for the ticket.
+ * cs_server_wait: timeout_s < 0 waits for good; returns the proof's status, or
+ * CS_ERR_TIMEOUT with the request still pending (wait again). */
+typedef struct cs_server cs_server;
+typedef struct {
+  int status;
+  double queue_ms;    /* submit -> start on a slot */
+  double latency_ms;  /* submit -> proof in host memory */
+  float device_ms;    /* device time of the prove kernels (CUDA events) */
+} cs_server_result;
+typedef struct {
+  uint64_t completed, failed, rejected;
+  uint64_t queued;
+  uint32_t running, max_concurrent;
+  size_t promised_bytes;
+} cs_server_counters;
+int cs_server_create(int device, int slots, size_t reserve_bytes, cs_server **out);
+void cs_server_destroy(cs_server *srv);
+int cs_server_add_key(cs_server *srv, cs_pk *pk, int *key_id);
+int cs_server_submit(cs_server *srv, int key_id, const uint32_t *w, const uint32_t *r, const uint32_t *s,
+                     uint32_t *proof, uint64_t *ticket);
+int cs_server_wait(cs_server *srv, uint64_t ticket, double timeout_s, cs_server_result *res);
+int cs_server_stats(cs_server *srv, cs_server_counters *st);
+const char *cs_server_error(cs_server *srv);
 
 /* ------------------------------------------- proving-key generation (setup) -------- */
 /* Device kernels for building proving keys (the quantities of the reference's

@@ -44,3 +44,16 @@ def test_no_device_reports_error_instead_of_exiting():
     L = lib()
     h = ctypes.c_void_p()
     assert L.cs_ctx_create(0, ctypes.byref(h)) != 0
+
+
+def test_server_refuses_without_device():
+    """The prove server needs a CUDA device: without one it fails loudly (no CPU path)."""
+    import ctypes
+    from cusnarks_b200 import lib
+    from cusnarks_b200._lib import CS_ERR_NODEVICE
+    from tests.gpu_common import gpu_available
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    h = ctypes.c_void_p()
+    assert lib().cs_server_create(0, 2, 0, ctypes.byref(h)) == CS_ERR_NODEVICE
+    assert not h.value

@@ -62,6 +62,20 @@ def test_prove_matches_cpu_and_verifies(ctx, oracle, log_m, seed):
     prover.close(); prover2.close()
 
 
+def test_plain_per_call_path_matches(ctx):
+    """The reference's flow through the drop-in entry points (one host-memory call per
+    step, key re-sent per MSM) gives the resident prover's proof byte for byte."""
+    from cusnarks_b200.groth import SyntheticCircuit, setup_pk, pk_to_host, Prover
+    from cusnarks_b200.plain import PlainProver
+    circ = SyntheticCircuit(ctx, 9, seed=41)
+    pk = setup_pk(ctx, circ, seed=42)
+    host = pk_to_host(pk)
+    r, s = 0x1111111122222222333 % R, 0x44444444555555556666 % R
+    want = Prover(ctx, pk).prove(circ.w, ints_to_limbs([r])[0], ints_to_limbs([s])[0])
+    got = PlainProver(host).prove(circ.w, r, s)
+    assert np.array_equal(got, want)
+
+
 def test_dropin_mpoly_eval_fixture(golden):
     """mpoly_eval_server_h through the C ABI reproduces the reference library's output."""
     import ctypes

@@ -1,0 +1,79 @@
+"""Served proving: proofs made in a concurrent mix of circuits equal the proofs made alone
+(byte for byte); admission by device memory refuses a request that can never fit."""
+import numpy as np
+import pytest
+
+from oracle.oracle import ints_to_limbs, R
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from cusnarks_b200 import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def keys(ctx):
+    from cusnarks_b200.groth import SyntheticCircuit, setup_pk, Prover
+    out = []
+    for log_m, seed in ((7, 21), (9, 22), (11, 23)):
+        circ = SyntheticCircuit(ctx, log_m, seed=seed)
+        pk = setup_pk(ctx, circ, seed=seed + 1)
+        out.append((circ, pk, Prover(ctx, pk)))
+    yield out
+    for _, _, p in out:
+        p.close()
+
+
+def _rs(i):
+    r = (0x1234567 * (i + 3) + 99991) % R
+    s = (0x7654321 * (i + 5) + 77773) % R
+    return ints_to_limbs([r])[0], ints_to_limbs([s])[0]
+
+
+def test_mix_equals_alone(keys):
+    from cusnarks_b200.server import ProveServer
+    jobs = [(i % 3 if i % 4 else 2, i) for i in range(14)]   # uneven mix, the largest most
+    alone = {}
+    for k, i in jobs:
+        circ, _, prover = keys[k]
+        r, s = _rs(i)
+        alone[i] = prover.prove(circ.w, r, s)
+    srv = ProveServer(0, slots=3, reserve_bytes=64 << 20)
+    try:
+        kid = [srv.add_key(p) for _, _, p in keys]
+        tickets = []
+        for k, i in jobs:
+            r, s = _rs(i)
+            tickets.append((i, srv.submit(kid[k], keys[k][0].w, r, s)))
+        for i, t in tickets:
+            proof, info = srv.wait(t, timeout=120.0)
+            assert np.array_equal(proof, alone[i]), i
+            assert info["latency_ms"] >= info["queue_ms"] >= 0.0
+        st = srv.stats()
+        assert st["completed"] == len(jobs) and st["failed"] == 0 and st["queued"] == 0
+        assert st["max_concurrent"] >= 2
+    finally:
+        srv.close()
+
+
+def test_admission_refuses_what_cannot_fit(keys):
+    """A reserve larger than the device: with nothing running, the request is refused
+    with CS_ERR_NOMEM (no allocation is attempted)."""
+    from cusnarks_b200.server import ProveServer
+    from cusnarks_b200._lib import CsError, CS_ERR_NOMEM
+    srv = ProveServer(0, slots=2, reserve_bytes=1 << 50)
+    try:
+        k = srv.add_key(keys[0][2])
+        r, s = _rs(0)
+        t = srv.submit(k, keys[0][0].w, r, s)
+        with pytest.raises(CsError) as ei:
+            srv.wait(t, timeout=60.0)
+        assert ei.value.code == CS_ERR_NOMEM
+        assert srv.stats()["rejected"] == 1
+    finally:
+        srv.close()
