@@ -51,7 +51,12 @@ import numpy as np  # noqa: E402
 
 METRIC = "Groth16 proofs/s + p50/p99 latency, 2^20 G1 MSM ms; served vs plain, 1 B200"
 UNIT = "proofs/s (2^20 constraints)"
-IMAD_PER_MONT = 264   # CIOS, 8x32-bit limbs: 8 rows x (16 a*b + 16 m*p + 1 m) multiply-adds
+# 256-bit Montgomery product, 8x32-bit limbs: 64 a*b + 64 m*p wide (32x32->64) products + 8 m
+PRODUCTS_PER_MONT = 136
+MONT_PER_MADD = 11     # mixed addition, 7M + 4S (the canonical count of the MSM cost model)
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_accumulate launch of
+# the 2^20 G1 MSM (window 16), from an ncu capture of that launch
+ACC_TRAFFIC_BYTES = 443_948_544 + 61_470_720
 L2_BYTES = 126 * 1024 * 1024
 LOG_M = 20
 CPU_SAMPLE_LOG_M = 16
@@ -353,7 +358,7 @@ def run_ours(args, world, rank, local):
     from cusnarks_b200 import Context
     from cusnarks_b200.context import kernel_launches
     ctx = Context(local)
-    peak_imad = ctx.imad_peak()
+    peak_wide = ctx.pipe_rate(3)
     wl = ProveWorkload(ctx, LOG_M, seed=100 + rank)
     sd = ServedDevice(wl, args.slots)
     # one proof per call (resident key): lone-proof device latency
@@ -415,7 +420,7 @@ def run_ours(args, world, rank, local):
         wl.l2_flush()
     units, window = mw.dominant_units()
     acc = statistics.mean(acc_ms)
-    achieved = units * 11 * IMAD_PER_MONT / (acc * 1e-3)
+    achieved = units * MONT_PER_MADD * PRODUCTS_PER_MONT / (acc * 1e-3)
     e2e_val = world * 1e3 / e2e_ms
     line = {
         "metric": METRIC,
@@ -448,12 +453,14 @@ def run_ours(args, world, rank, local):
                                     "points copied per call; wall clock"},
         "served_vs_plain": round(e2e_val * plain_ms / 1e3, 2),
         "g1_msm_2^20_ms": round(statistics.median(msm_ms), 3),
-        "roofline": {"bound": "int (IMAD pipe)", "kernel": "k_accumulate+k_combine (MSM bucket accumulation)",
-                     "achieved": round(achieved / 1e12, 4), "peak": round(peak_imad / 1e12, 4),
-                     "unit": "T IMAD/s", "frac": round(achieved / peak_imad, 4), "traffic": None,
-                     "kernel_ms": round(acc, 4), "units_per_launch": units, "window": window,
-                     "basis": "2^20 G1 MSM: N*W entries x 11 Montgomery products x 264 IMAD / kernel ms "
-                              "(CUDA events around the kernels); peak = live IMAD microbenchmark"},
+        "roofline": {"bound": "int (IMAD.WIDE pipe)", "kernel": "k_accumulate+k_combine (MSM bucket accumulation)",
+                     "achieved": round(achieved / 1e12, 4), "peak": round(peak_wide / 1e12, 4),
+                     "unit": "T wide products/s", "frac": round(achieved / peak_wide, 4),
+                     "traffic": ACC_TRAFFIC_BYTES, "kernel_ms": round(acc, 4), "units_per_launch": units,
+                     "window": window,
+                     "basis": "2^20 G1 MSM: N*W bucket entries x 11 Montgomery products x 136 32x32->64 "
+                              "products / kernel ms (CUDA events around the kernels); peak = live "
+                              "mad.wide.u32 rate (cs_bench_pipe mode 3); traffic = ncu DRAM bytes per launch"},
         "e2e": {"value": round(e2e_val, 3), "unit": UNIT, "ms": round(e2e_ms, 3),
                 "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes,
                 "basis": f"C-ABI prove server ({args.slots} slots), {len(jobs)} requests submitted at once, "

@@ -141,6 +141,13 @@ class Context:
         check(self._lib.cs_bench_imad_peak(self.handle, ctypes.byref(v)), self.handle)
         return float(v.value)
 
+    def pipe_rate(self, mode: int) -> float:
+        """Measured instruction rate per second of one pipe probe (cs_bench_pipe): 1 mad.lo,
+        2 mad.hi, 3 mad.wide.u32 (one 32x32->64 product each), 5 carry-chain mad.cc."""
+        v = ctypes.c_double()
+        check(self._lib.cs_bench_pipe(self.handle, mode, ctypes.byref(v)), self.handle)
+        return float(v.value)
+
 
 def kernel_launches() -> int:
     return int(lib().cs_kernel_launches())

@@ -110,6 +110,13 @@ CSB_DEV void row_mad_wide(uint32_t (&t)[9], const uint32_t (&a)[8], uint32_t b) 
 }
 
 template <class M>
+struct Fp;
+// Out-of-line Montgomery product (arguments and result in registers): keeps loop bodies
+// that chain many products small enough for the instruction cache.
+template <class M>
+__device__ __noinline__ Fp<M> fp_mul_call(Fp<M> a, Fp<M> b);
+
+template <class M>
 struct Fp {
   uint32_t v[8];
 
@@ -283,8 +290,10 @@ struct Fp {
   }
 
   friend CSB_DEV Fp operator*(const Fp& a, const Fp& b) {
-#ifdef CSB_MUL_LOHI
+#if defined(CSB_MUL_LOHI)
     return mul_lohi(a, b);
+#elif defined(CSB_MUL_NOINLINE)
+    return fp_mul_call<M>(a, b);
 #else
     return mul_wide(a, b);
 #endif
@@ -408,6 +417,11 @@ using Fq = Fp<ModQ>;
 using Fr = Fp<ModR>;
 
 // ------------------------------------------------------------ Fq2 = Fq[u]/(u^2+1) ----
+template <class M>
+__device__ __noinline__ Fp<M> fp_mul_call(Fp<M> a, Fp<M> b) {
+  return Fp<M>::mul_wide(a, b);
+}
+
 struct Fq2 {
   Fq c0, c1;
   static CSB_DEV Fq2 zero() { return {Fq::zero(), Fq::zero()}; }

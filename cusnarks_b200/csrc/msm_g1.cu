@@ -1,4 +1,7 @@
 // msm_g1.cu -- G1 (Fq) instantiation of the MSM pipeline.
+// Montgomery products out of line: the accumulation loop body (one XYZZ + affine
+// addition, 10 products) then fits the instruction cache; measured faster at 2^20.
+#define CSB_MUL_NOINLINE
 #include "msm_impl.cuh"
 
 namespace csb {

@@ -2,6 +2,7 @@
 
     python -m cusnarks_b200.run msm   --log-n 20 [--g2] [--fixed] [--window C] [--reps K]
     python -m cusnarks_b200.run prove --log-m 20 [--no-fixed] [--reps K]
+    python -m cusnarks_b200.run ntt   --log-n 20 [--hstep reference|coset] [--reps K]
 
 Inputs are seeded: MSM scalars uniform in Fr, bases k_i * G (k_i seeded, built on the GPU);
 prove runs the synthetic R1CS family of the benchmark (3 nonzeros per A/B row) with a key
@@ -72,6 +73,31 @@ def _prove(args, ctx):
     return call, info
 
 
+def _ntt(args, ctx):
+    import torch
+    from .synth import random_field
+    n = 1 << args.log_n
+    rng = np.random.Generator(np.random.PCG64(args.seed))
+    dev = torch.device("cuda", ctx.device)
+    a = torch.from_numpy(random_field(rng, n).view(np.int32)).to(dev)
+    b = torch.from_numpy(random_field(rng, n).view(np.int32)).to(dev)
+    c = torch.from_numpy(random_field(rng, n).view(np.int32)).to(dev)
+    out = torch.empty(2 * n * 8, dtype=torch.int32, device=dev)  # 2m coefficients (reference variant)
+    torch.cuda.synchronize()
+    if args.hstep:
+        variant = 0 if args.hstep == "reference" else 1
+
+        def call():
+            ctx.hstep_device(variant, a.data_ptr(), b.data_ptr(), c.data_ptr(), args.log_n, out.data_ptr())
+        info = {"workload": "hstep", "variant": args.hstep, "log_m": args.log_n}
+    else:
+        def call():
+            ctx.ntt_device(a.data_ptr(), out.data_ptr(), args.log_n, 1)
+        info = {"workload": "ntt", "direction": "forward", "log_n": args.log_n}
+    call.keep = (a, b, c, out)
+    return call, info
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m cusnarks_b200.run")
     sub = ap.add_subparsers(dest="what", required=True)
@@ -83,7 +109,10 @@ def main(argv=None):
     p = sub.add_parser("prove")
     p.add_argument("--log-m", type=int, default=20)
     p.add_argument("--no-fixed", action="store_true", help="generic MSMs instead of fixed-base tables")
-    for q in (m, p):
+    t = sub.add_parser("ntt")
+    t.add_argument("--log-n", type=int, default=20)
+    t.add_argument("--hstep", choices=["reference", "coset"], default=None)
+    for q in (m, p, t):
         q.add_argument("--reps", type=int, default=3)
         q.add_argument("--seed", type=int, default=100)
         q.add_argument("--device", type=int, default=0)
@@ -92,7 +121,7 @@ def main(argv=None):
     from .context import Context
     torch.cuda.set_device(args.device)
     ctx = Context(args.device)
-    call, info = (_msm if args.what == "msm" else _prove)(args, ctx)
+    call, info = {"msm": _msm, "prove": _prove, "ntt": _ntt}[args.what](args, ctx)
     call()
     ctx.sync()
     torch.cuda.profiler.start()
