@@ -24,7 +24,9 @@ that saturated rate.  ``single_proof``: one proof per call (cs_prove_device), de
 ntt_interpolandmul_server_h, ec_jacreduce_server_h per MSM with the key points copied per
 call), wall clock; ``served_vs_plain`` = e2e / plain.  ``served_mix``: 8 circuits of
 2^12..2^20 constraints (log-uniform, seeded), requests uniform over them, saturation and
-Poisson 50% / 90% with p50/p99.  Also one BN128 G1 MSM of 2^20 terms (``g1_msm_2^20_ms``),
+Poisson 50% / 90% with p50/p99.  ``batched_msm``: 64 G1 + 8 G2 MSMs of 2^floor(U(10,20))
+terms in one batch plan per group (autotuned windows, CUDA graph replay) vs one call per
+instance.  Also one BN128 G1 MSM of 2^20 terms (``g1_msm_2^20_ms``),
 whose bucket-accumulation kernel -- the dominant kernel of every proof -- carries the roofline.
 
 ``cpu_baseline`` / ``--impl reference``: the reference's own CPU library (oracle/_ref,
@@ -353,6 +355,71 @@ def served_mix(ctx, slots: int, n_requests: int, seed: int = 5):
     return out
 
 
+def batched_msm(ctx, reps: int, seed: int = 4):
+    """Config 4: 64 G1 + 8 G2 MSMs, N = 2^floor(U(10, 20)) (seeded), bases from seeded pools of
+    k_i * G, scalars uniform in Fr; one batch plan per group (windows autotuned), replayed as
+    CUDA graphs; compared with one cs_msm_device call per instance (default windows)."""
+    import torch
+    from cusnarks_b200.synth import random_field, g1_generator, g2_generator
+    rng = np.random.Generator(np.random.PCG64(seed))
+    dev = torch.device("cuda", ctx.device)
+    out = {"instances": {"g1": 64, "g2": 8}}
+    groups = []
+    for ec2, count in ((False, 64), (True, 8)):
+        pw = 32 if ec2 else 16
+        logs = [int(x) for x in rng.integers(10, 21, count)]
+        sizes = [1 << L for L in logs]
+        pool_n = max(sizes)
+        k = torch.from_numpy(random_field(rng, pool_n).view(np.int32)).to(dev)
+        g = torch.from_numpy((g2_generator() if ec2 else g1_generator()).view(np.int32)).to(dev)
+        pool = torch.empty((pool_n, pw), dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()
+        ctx.scmul_device(k.data_ptr(), g.data_ptr(), pool_n, pool.data_ptr(), ec2=ec2, point_stride_words=0)
+        ctx.sync()
+        sc = torch.from_numpy(random_field(rng, sum(sizes)).view(np.int32)).to(dev)
+        outs = torch.zeros((count, pw), dtype=torch.int32, device=dev)
+        ref = torch.zeros((count, pw), dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()
+        offs = np.concatenate([[0], np.cumsum(sizes)])
+        jobs = []
+        for q, n in enumerate(sizes):
+            p0 = int(rng.integers(0, pool_n - n + 1))
+            jobs.append((sc.data_ptr() + 32 * int(offs[q]), pool.data_ptr() + 4 * pw * p0, n,
+                         outs.data_ptr() + 4 * pw * q))
+        tuned = ctx.msm_autotune(10, 20, ec2=ec2)
+        groups.append((ec2, logs, jobs, outs, ref, tuned, (k, g, pool, sc)))
+    plans = [ctx.msm_batch(jobs, ec2=ec2) for ec2, _, jobs, _, _, _, _ in groups]
+
+    def run_batch():
+        for pl in plans:
+            pl.run(graph=True)
+        ctx.sync()
+
+    def run_single():
+        for ec2, _, jobs, _, ref, _, _ in groups:
+            pw = 32 if ec2 else 16
+            for q, (s_, p_, n, _) in enumerate(jobs):
+                ctx.msm_device(s_, p_, n, ref.data_ptr() + 4 * pw * q, ec2=ec2)
+        ctx.sync()
+
+    for _ in range(2):
+        run_batch()
+        run_single()
+    tb = min(device_span_ms(run_batch) for _ in range(reps))
+    ts = min(device_span_ms(run_single) for _ in range(reps))
+    equal = all(torch.equal(o, r) for _, _, _, o, r, _, _ in groups)
+    out.update({"log2_sizes_g1": groups[0][1], "log2_sizes_g2": groups[1][1],
+                "terms": {"g1": int(sum(1 << L for L in groups[0][1])), "g2": int(sum(1 << L for L in groups[1][1]))},
+                "windows_tuned_g1": groups[0][5], "windows_tuned_g2": groups[1][5],
+                "batch_ms": round(tb, 3), "per_call_ms": round(ts, 3), "speedup": round(ts / tb, 3),
+                "graph": True, "equal_to_single": bool(equal),
+                "basis": "device time (CUDA events) of the two graph replays (G1 batch, G2 batch) vs 72 "
+                         "cs_msm_device calls; best of the timed repetitions"})
+    for pl in plans:
+        pl.close()
+    return out
+
+
 def run_ours(args, world, rank, local):
     import torch
     from cusnarks_b200 import Context
@@ -468,6 +535,8 @@ def run_ours(args, world, rank, local):
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if rank == 0 and not args.no_batch:
+        line["batched_msm"] = batched_msm(ctx, reps=3)
     if rank == 0 and not args.no_mix:
         line["served_mix"] = served_mix(ctx, args.slots, args.mix_requests)
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -517,6 +586,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--slots", type=int, default=3, help="concurrent proofs of the served engine")
     ap.add_argument("--no-mix", action="store_true", help="skip the mixed-size served leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-MSM leg")
     ap.add_argument("--mix-requests", type=int, default=96)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -30,6 +30,10 @@ class CsError(RuntimeError):
         self.code = code
 
 
+class MsmJob(ctypes.Structure):
+    _fields_ = [("scalars", _vp), ("points", _vp), ("out", _vp), ("n", ctypes.c_uint32), ("window", ctypes.c_int)]
+
+
 class ServerResult(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("queue_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
                 ("device_ms", ctypes.c_float)]
@@ -98,6 +102,13 @@ _SIGNATURES = [
     ("cs_msm_fixed_workspace_bytes", ctypes.c_size_t, [ctypes.c_uint32, ctypes.c_int, ctypes.c_int]),
     ("cs_msm_fixed_table_device", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_uint32, ctypes.c_int, _vp]),
     ("cs_msm_fixed_device", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, ctypes.c_int, _vp]),
+    ("cs_msm_batch_create", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("cs_msm_batch_run", ctypes.c_int, [_vp, _vp, ctypes.c_int]),
+    ("cs_msm_batch_destroy", None, [_vp]),
+    ("cs_msm_batch_workspace_bytes", ctypes.c_size_t, [_vp]),
+    ("cs_msm_batch_window", ctypes.c_int, [_vp, ctypes.c_uint32]),
+    ("cs_msm_autotune", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, _vp]),
+    ("cs_msm_tuned_window", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_uint32]),
     ("cs_scmul_device", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, ctypes.c_uint32, _vp]),
     ("cs_bench_imad_peak", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     ("cs_bench_pipe", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),

@@ -106,6 +106,19 @@ class Context:
                                             ctypes.c_void_p(d_table), n, window, ctypes.c_void_p(d_out)),
               self.handle)
 
+    # ----------------------------------------------------------------- batched MSM ----
+    def msm_batch(self, jobs, ec2: bool = False, task: int = 0) -> "MsmBatch":
+        """jobs: [(d_scalars, d_points, n, d_out[, window])] device pointers -> a batch plan."""
+        return MsmBatch(self, jobs, ec2, task)
+
+    def msm_autotune(self, log_min: int, log_max: int, ec2: bool = False) -> list:
+        out = (ctypes.c_int * (log_max - log_min + 1))()
+        check(self._lib.cs_msm_autotune(self.handle, int(bool(ec2)), log_min, log_max, out), self.handle)
+        return list(out)
+
+    def msm_tuned_window(self, n: int, ec2: bool = False) -> int:
+        return int(self._lib.cs_msm_tuned_window(self.handle, int(bool(ec2)), n))
+
     # -------------------------------------------------------------- field ops -----
     FOP = {"mul": 0, "add": 1, "sub": 2, "sqr": 3, "inv": 4, "to_mont": 5, "from_mont": 6,
            "mul_lohi": 7, "fq2_mul": 8}
@@ -147,6 +160,41 @@ class Context:
         v = ctypes.c_double()
         check(self._lib.cs_bench_pipe(self.handle, mode, ctypes.byref(v)), self.handle)
         return float(v.value)
+
+
+class MsmBatch:
+    """A batch of MSM instances summed in one pass (cs_msm_batch_*)."""
+
+    def __init__(self, ctx: Context, jobs, ec2: bool = False, task: int = 0):
+        from ._lib import MsmJob
+        arr = (MsmJob * max(1, len(jobs)))()
+        for k, j in enumerate(jobs):
+            w = j[4] if len(j) > 4 else 0
+            arr[k] = MsmJob(ctypes.c_void_p(j[0]), ctypes.c_void_p(j[1]), ctypes.c_void_p(j[3]), j[2], w)
+        h = ctypes.c_void_p()
+        check(lib().cs_msm_batch_create(ctx.handle, int(bool(ec2)), ctypes.cast(arr, ctypes.c_void_p), len(jobs),
+                                        task, ctypes.byref(h)), ctx.handle)
+        self.ctx, self.handle, self.njobs = ctx, h, len(jobs)
+
+    def run(self, graph: bool = True):
+        check(lib().cs_msm_batch_run(self.ctx.handle, self.handle, int(bool(graph))), self.ctx.handle)
+
+    def windows(self) -> list:
+        return [int(lib().cs_msm_batch_window(self.handle, k)) for k in range(self.njobs)]
+
+    def workspace_bytes(self) -> int:
+        return int(lib().cs_msm_batch_workspace_bytes(self.handle))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().cs_msm_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def kernel_launches() -> int:

@@ -1,5 +1,5 @@
 // msm.cu -- MSM window choice and workspace sizing (kernels: msm_impl.cuh).
-#include "msm_impl.cuh"
+#include "msm_batch.cuh"
 
 namespace csb {
 
@@ -33,6 +33,10 @@ int msm_fixed_window(uint32_t n, bool ec2) {
   }
   (void)ec2;
   return best;
+}
+
+size_t msm_batch_workspace_bytes(const MsmBatch& b, bool ec2) {
+  return msm_detail::batch_layout(b, ec2 ? 256 : 128).total;
 }
 
 size_t msm_fixed_table_points(uint32_t n, int c) { return (size_t)msm_detail::num_windows(c) * n; }

@@ -36,6 +36,41 @@
 
 namespace csb {
 
+// Instance of a batch of MSMs: device pointers, size, window, and its first term, bucket
+// and window in the batch (instances are ordered by window so each window group occupies a
+// contiguous bucket range).
+struct BatchJob {
+  const uint32_t* scalars;
+  const uint32_t* points;
+  uint32_t* out;
+  uint32_t n, c, W, bucket0, window0, term0, pad0, pad1;
+};
+
+// A group of batch instances sharing one window c: buckets [bucket0, bucket0 + windows * B),
+// window sums [window0, window0 + windows).
+struct BatchGroup {
+  int c;
+  uint32_t bucket0, windows, window0;
+};
+
+// A batch plan: the job table (device), totals and the groups, scratch of
+// msm_batch_workspace_bytes() bytes.
+struct MsmBatch {
+  const BatchJob* d_jobs = nullptr;
+  uint32_t njobs = 0;
+  uint32_t terms = 0;      // sum of n
+  uint32_t nbuckets = 0;   // sum of W * 2^(c-1)
+  uint64_t nentries = 0;   // sum of n * W (upper bound of bucket entries)
+  uint32_t nwindows = 0;   // sum of W
+  uint64_t lv_points = 0, lv2_points = 0;  // max over groups of W*(2^(c-1)/8+1), W*(.../64+1)
+  const BatchGroup* groups = nullptr;  // host array
+  uint32_t ngroups = 0;
+  int task = 64;
+};
+size_t msm_batch_workspace_bytes(const MsmBatch& b, bool ec2);
+cudaError_t msm_batch_g1(const MsmBatch& b, void* d_work, size_t work_bytes, cudaStream_t stream);
+cudaError_t msm_batch_g2(const MsmBatch& b, void* d_work, size_t work_bytes, cudaStream_t stream);
+
 struct MsmConfig {
   int c = 0;          // window bits; 0 = pick from N
   int task = 64;      // max points per accumulation task

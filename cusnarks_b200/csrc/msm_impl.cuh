@@ -113,10 +113,21 @@ __global__ void k_scatter(const uint32_t* __restrict__ scalars, const uint32_t* 
 }
 
 // Task record: entries [start, start+len) summed into dst.  dst < nb: bucket index;
-// dst >= nb: partial slot (dst - nb).
+// dst >= nb: partial slot (dst - nb).  job: the instance whose bases the entries index (a
+// batch of MSMs shares one task list; 0 for a single MSM).
 struct Task {
-  uint32_t start, len, dst, pad;
+  uint32_t start, len, dst, job;
 };
+
+// Index of the job whose bucket range holds bucket b (bucket0 ascending, bucket0[0] = 0).
+CSB_DEV uint32_t job_of_bucket(const BatchJob* jobs, uint32_t njobs, uint32_t b) {
+  uint32_t lo = 0, hi = njobs;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (jobs[mid].bucket0 <= b) lo = mid; else hi = mid;
+  }
+  return lo;
+}
 struct Multi {
   uint32_t bucket, pbase, count, pad;
 };
@@ -166,7 +177,8 @@ static __global__ void k_task_bins(const uint32_t* __restrict__ hist, uint32_t t
 template <class F>
 __global__ void k_task_emit(const uint32_t* __restrict__ offsets, uint32_t nb, uint32_t task_len,
                             uint32_t* __restrict__ cursor, Task* __restrict__ tasks,
-                            uint32_t* __restrict__ counters, Multi* __restrict__ multi) {
+                            uint32_t* __restrict__ counters, Multi* __restrict__ multi,
+                            const BatchJob* __restrict__ jobs = nullptr, uint32_t njobs = 0) {
   __shared__ uint32_t cnt_s[kMaxTask + 1], base_s[kMaxTask + 1];
   for (int i = threadIdx.x; i <= kMaxTask; i += blockDim.x) cnt_s[i] = 0;
   __syncthreads();
@@ -190,6 +202,7 @@ __global__ void k_task_emit(const uint32_t* __restrict__ offsets, uint32_t nb, u
   __syncthreads();
   if (cnt == 0) return;
   const uint32_t nt = nfull + 1;
+  const uint32_t job = jobs ? job_of_bucket(jobs, njobs, b) : 0u;
   uint32_t pbase = 0;
   if (nt > 1) {
     pbase = atomicAdd(&counters[1], nt);
@@ -200,7 +213,7 @@ __global__ void k_task_emit(const uint32_t* __restrict__ offsets, uint32_t nb, u
   for (uint32_t t = 0; t < nt; t++) {
     const uint32_t len = t < nfull ? task_len : last;
     const uint32_t slot = base_s[len] + atomicAdd(&cnt_s[len], 1u);
-    tasks[slot] = {start + t * task_len, len, nt == 1 ? b : nb + pbase + t, 0u};
+    tasks[slot] = {start + t * task_len, len, nt == 1 ? b : nb + pbase + t, job};
   }
 }
 
@@ -218,17 +231,19 @@ __global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate(cons
                                                     const uint32_t* __restrict__ entries,
                                                     const uint32_t* __restrict__ points, uint32_t nb,
                                                     uint32_t* __restrict__ buckets,
-                                                    uint32_t* __restrict__ partials) {
+                                                    uint32_t* __restrict__ partials,
+                                                    const BatchJob* __restrict__ jobs = nullptr) {
   constexpr int PW = 2 * FieldWords<F>::value;
   constexpr int XW = 4 * FieldWords<F>::value;
   const uint32_t ntasks = counters[0];
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < ntasks; t += gridDim.x * blockDim.x) {
     const Task tk = tasks[t];
+    const uint32_t* base = jobs ? jobs[tk.job].points : points;
     XYZZ<F> acc = XYZZ<F>::inf();
 #pragma unroll 1
     for (uint32_t e = 0; e < tk.len; e++) {
       const uint32_t ent = entries[tk.start + e];
-      Affine<F> p = ld_affine<F>(points + (size_t)(ent & ~NEG_BIT) * PW);
+      Affine<F> p = ld_affine<F>(base + (size_t)(ent & ~NEG_BIT) * PW);
       if (ent & NEG_BIT) p.y = p.y.neg();
       acc = xyzz_madd(acc, p);
     }

@@ -200,6 +200,34 @@ int cs_msm_fixed_table_device(cs_ctx *ctx, int ec2, const uint32_t *d_points, ui
 int cs_msm_fixed_device(cs_ctx *ctx, int ec2, const uint32_t *d_scalars, const uint32_t *d_table,
                         uint32_t n, int window, uint32_t *d_out_affine);
 
+/* Batched multi-exponentiation: many instances of uneven size (device pointers) summed in one
+ * pass -- one digit sort and ONE bucket-accumulation launch over the union of their buckets,
+ * split by bucket size, then one reduction per distinct window.  Replaces one GPU multi-exp
+ * call per instance (cuda_wrapper.py:216 ec_mad_cuda2 driven by groth_prover.py:1563).
+ * window 0 = the autotuned window for the instance's size (cs_msm_autotune) or, untuned, the
+ * cost-model default.  cs_msm_batch_run is asynchronous on the context stream; use_graph != 0
+ * captures the sequence into a CUDA graph on the first run and replays it afterwards (the
+ * plan's pointers are baked in: change inputs in place).  task = bucket tile (max entries
+ * per accumulation task, 32..64; 0 = 64).  Each result equals cs_msm_device's. */
+typedef struct {
+  const uint32_t *scalars, *points;
+  uint32_t *out;
+  uint32_t n;
+  int window;
+} cs_msm_job;
+typedef struct cs_msm_batch cs_msm_batch;
+int cs_msm_batch_create(cs_ctx *ctx, int ec2, const cs_msm_job *jobs, uint32_t njobs, int task,
+                        cs_msm_batch **out);
+int cs_msm_batch_run(cs_ctx *ctx, cs_msm_batch *batch, int use_graph);
+void cs_msm_batch_destroy(cs_msm_batch *batch);
+size_t cs_msm_batch_workspace_bytes(const cs_msm_batch *batch);
+int cs_msm_batch_window(const cs_msm_batch *batch, uint32_t job);
+/* Window autotuner: times the MSM at each size 2^log_min..2^log_max for windows around the
+ * cost-model choice and keeps the fastest per size (per device, process-wide); windows_out
+ * (optional) receives them.  Synchronous. */
+int cs_msm_autotune(cs_ctx *ctx, int ec2, uint32_t log_min, uint32_t log_max, int *windows_out);
+int cs_msm_tuned_window(cs_ctx *ctx, int ec2, uint32_t n);
+
 /* Elementwise field operation on n elements of device arrays (8 words each; 16 for
  * CS_FOP_FQ2_MUL, which multiplies in Fq2 = Fq[u]/(u^2+1) regardless of pidx).
  * d_b is ignored by the unary operations.  Asynchronous on the context stream. */
