@@ -15,11 +15,24 @@ void domain_release(cs_ctx* ctx);  // hstep.cu
 static std::atomic<unsigned long long> g_launches{0};
 void note_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+#ifndef CSB_PRIO_MODE
+#define CSB_PRIO_MODE 2  // G2 MSM and the QAP/H chain first (measured 32.0 -> 31.6 ms per 2^20 proof)
+#endif
+
+// Auxiliary streams of the prove pipeline: aux[0..3] carry the A, B1, B2 (G2) and C MSMs,
+// aux_h the QAP -> H step -> H MSM chain.  Priorities (lower number = higher priority)
+// decide which MSM's blocks the SMs take first when several are ready.
 cudaError_t ctx_aux_init(cs_ctx* ctx) {
   if (ctx->aux_ready) return cudaSuccess;
-  cudaError_t e = cudaSuccess;
+  int least = 0, greatest = 0;
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  int prio[4] = {least, least, least, least}, prio_h = least;
+  if (CSB_PRIO_MODE == 1) { prio[2] = greatest; }
+  if (CSB_PRIO_MODE == 2) { prio[2] = greatest; prio_h = greatest; }
+  if (CSB_PRIO_MODE == 3) { prio[2] = greatest < least ? greatest + 1 : greatest; prio_h = greatest; }
   for (int i = 0; i < 4 && e == cudaSuccess; i++)
-    if (!ctx->aux[i]) e = cudaStreamCreateWithFlags(&ctx->aux[i], cudaStreamNonBlocking);
+    if (!ctx->aux[i]) e = cudaStreamCreateWithPriority(&ctx->aux[i], cudaStreamNonBlocking, prio[i]);
+  if (e == cudaSuccess && !ctx->aux_h) e = cudaStreamCreateWithPriority(&ctx->aux_h, cudaStreamNonBlocking, prio_h);
   for (int i = 0; i < 8 && e == cudaSuccess; i++)
     if (!ctx->aux_ev[i]) e = cudaEventCreateWithFlags(&ctx->aux_ev[i], cudaEventDisableTiming);
   if (e == cudaSuccess) ctx->aux_ready = true;
@@ -151,6 +164,7 @@ void cs_ctx_destroy(cs_ctx* ctx) {
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   for (int i = 0; i < 4; i++)
     if (ctx->aux[i]) { cudaStreamSynchronize(ctx->aux[i]); cudaStreamDestroy(ctx->aux[i]); }
+  if (ctx->aux_h) { cudaStreamSynchronize(ctx->aux_h); cudaStreamDestroy(ctx->aux_h); }
   for (int i = 0; i < 8; i++)
     if (ctx->aux_ev[i]) cudaEventDestroy(ctx->aux_ev[i]);
   delete ctx;

@@ -222,7 +222,10 @@ __global__ void k_task_emit(const uint32_t* __restrict__ offsets, uint32_t nb, u
 #ifndef CSB_ACC_G2_MINB
 #define CSB_ACC_G2_MINB 3  // 168 registers: 12 warps per SM instead of 8 (measured faster)
 #endif
-template <class F> struct AccMinBlocks { static constexpr int value = 0; };
+#ifndef CSB_ACC_G1_MINB
+#define CSB_ACC_G1_MINB 0
+#endif
+template <class F> struct AccMinBlocks { static constexpr int value = CSB_ACC_G1_MINB; };
 template <> struct AccMinBlocks<Fq2> { static constexpr int value = CSB_ACC_G2_MINB; };
 
 template <class F>

@@ -384,19 +384,23 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
   k_scale_point<Fq><<<1, 32, 0, sa>>>(outA, rs + 8, sA);   // s * pi_A
   k_scale_point<Fq><<<1, 32, 0, sb1>>>(outB1, rs, rB1);    // r * pi_B1
   note_launch(2);
-  // QAP evaluation and H step on the main stream
-  ok = (e = qap_eval(pk->rows_a, d_w, pA, 0, s0)) == cudaSuccess &&
-       (e = qap_eval(pk->rows_b, d_w, pB, 0, s0)) == cudaSuccess &&
+  // QAP evaluation, H step and H MSM on their own stream
+  cudaStream_t sh = ctx->aux_h;
+  cudaStreamWaitEvent(sh, ev_w, 0);
+  ok = (e = qap_eval(pk->rows_a, d_w, pA, 0, sh)) == cudaSuccess &&
+       (e = qap_eval(pk->rows_b, d_w, pB, 0, sh)) == cudaSuccess &&
        (e = hstep_reference_core(pA, pB, pk->log_m, domain_wf(dom2), domain_wi(dom2), domain_wf(dom2),
-                                 domain_consts(dom1) + 16, domain_consts(dom2) + 24, M, hscr, s0)) == cudaSuccess &&
+                                 domain_consts(dom1) + 16, domain_consts(dom2) + 24, M, hscr, sh)) == cudaSuccess &&
        // polH = M[m .. 2m-2]; M[2m-1] (always zero) becomes the -rs term for delta_1
-       (e = cudaMemcpyAsync(M + (size_t)(2 * m - 1) * 8, rs + 16, 32, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess &&
-       (e = run_msm(false, M + (size_t)m * 8, pk->h_ext, pk->fh, m, outH, P.ms_h, P.bytes_h, s0)) == cudaSuccess;
+       (e = cudaMemcpyAsync(M + (size_t)(2 * m - 1) * 8, rs + 16, 32, cudaMemcpyDeviceToDevice, sh)) == cudaSuccess &&
+       (e = run_msm(false, M + (size_t)m * 8, pk->h_ext, pk->fh, m, outH, P.ms_h, P.bytes_h, sh)) == cudaSuccess;
   if (!ok) return fail(ctx, e, "prove QAP/H");
   for (int i = 0; i < 4; i++) {
     cudaEventRecord(ctx->aux_ev[1 + i], ctx->aux[i]);
     cudaStreamWaitEvent(s0, ctx->aux_ev[1 + i], 0);
   }
+  cudaEventRecord(ctx->aux_ev[5], sh);
+  cudaStreamWaitEvent(s0, ctx->aux_ev[5], 0);
   k_final_c<<<1, 32, 0, s0>>>(outH, outC, sA, rB1, piC);
   note_launch();
   // proof = pi_A (16) | pi_B (32) | pi_C (16), affine Montgomery

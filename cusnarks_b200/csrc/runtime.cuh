@@ -76,6 +76,7 @@ struct cs_ctx {
   std::mutex mu;               // one call at a time per context
   // auxiliary streams / events for fork-join pipelines (prove), created on first use
   cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaStream_t aux_h = nullptr;  // QAP -> H step -> H MSM chain of a proof
   cudaEvent_t aux_ev[8] = {nullptr};
   bool aux_ready = false;
 };
