@@ -54,6 +54,10 @@ class Context:
     def sync(self):
         check(self._lib.cs_ctx_sync(self.handle), self.handle)
 
+    def set_msm_affine_rounds(self, rounds: int):
+        """Batch-affine halving rounds before the XYZZ bucket accumulation (-1 auto, 0 off)."""
+        check(self._lib.cs_ctx_set_msm_affine_rounds(self.handle, rounds), self.handle)
+
     @property
     def last_ms(self) -> float:
         return float(self._lib.cs_ctx_last_ms(self.handle))

@@ -101,11 +101,12 @@ struct EventScope {
 
 int msm_device_locked(cs_ctx* ctx, int ec2, const uint32_t* s, const uint32_t* p, uint32_t n,
                       uint32_t* out, int window) {
-  const size_t need = csb::msm_workspace_bytes(n, window, ec2 != 0);
+  const size_t need = csb::msm_workspace_bytes(n, window, ec2 != 0, ctx->msm_affine != 0);
   cudaError_t e = ctx->work.reserve(need, ctx->stream);
   if (e != cudaSuccess) return fail(ctx, e, "msm workspace");
   csb::MsmConfig cfg;
   cfg.c = window;
+  cfg.affine = ctx->msm_affine;
   cfg.acc_start = ctx->ev_phase0;
   cfg.acc_stop = ctx->ev_phase1;
   ctx->phase_valid = true;
@@ -197,6 +198,13 @@ int cs_ctx_sync(cs_ctx* ctx) {
   return CS_OK;
 }
 
+int cs_ctx_set_msm_affine_rounds(cs_ctx* ctx, int rounds) {
+  if (!ctx || rounds < -1 || rounds > 6) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->msm_affine = rounds;
+  return CS_OK;
+}
+
 const char* cs_ctx_error(cs_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 float cs_ctx_last_ms(cs_ctx* ctx) { return ctx ? ctx->last_ms : 0.f; }
 float cs_ctx_last_phase_ms(cs_ctx* ctx) { return ctx ? ctx->last_phase_ms : 0.f; }
@@ -283,6 +291,7 @@ int cs_msm_fixed_device(cs_ctx* ctx, int ec2, const uint32_t* d_scalars, const u
   if (e != cudaSuccess) return fail(ctx, e, "fixed-base msm workspace");
   csb::MsmConfig cfg;
   cfg.c = window;
+  cfg.affine = ctx->msm_affine;
   cfg.acc_start = ctx->ev_phase0;
   cfg.acc_stop = ctx->ev_phase1;
   ctx->phase_valid = true;

@@ -16,10 +16,10 @@ int msm_default_window(uint32_t n, bool ec2) {
   return best;
 }
 
-size_t msm_workspace_bytes(uint32_t n, int c, bool ec2) {
+size_t msm_workspace_bytes(uint32_t n, int c, bool ec2, bool affine) {
   if (c <= 0) c = msm_default_window(n, ec2);
   const int xb = ec2 ? 256 : 128;
-  return msm_detail::make_layout(n, c, xb, msm_detail::kMinTask).total;
+  return msm_detail::make_layout(n, c, xb, msm_detail::kMinTask, false, affine).total;
 }
 
 int msm_fixed_window(uint32_t n, bool ec2) {

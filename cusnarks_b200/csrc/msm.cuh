@@ -74,12 +74,13 @@ cudaError_t msm_batch_g2(const MsmBatch& b, void* d_work, size_t work_bytes, cud
 struct MsmConfig {
   int c = 0;          // window bits; 0 = pick from N
   int task = 64;      // max points per accumulation task
+  int affine = -1;    // batch-affine halving rounds before the XYZZ accumulation: -1 auto, 0 off
   // optional events recorded around the bucket-accumulation kernels (phase timing)
   cudaEvent_t acc_start = nullptr, acc_stop = nullptr;
 };
 
 // Bytes of device scratch one MSM of n terms needs (G2 when ec2).
-size_t msm_workspace_bytes(uint32_t n, int c, bool ec2);
+size_t msm_workspace_bytes(uint32_t n, int c, bool ec2, bool affine = true);
 int msm_default_window(uint32_t n, bool ec2);
 
 // d_scalars: n x 8 words (normal form), d_points: n affine points (16 or 32 words),

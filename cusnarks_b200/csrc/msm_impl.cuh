@@ -1,6 +1,7 @@
 // msm_impl.cuh -- kernels and launch sequence of the Pippenger MSM (pipeline in msm.cuh),
 // instantiated for G1 in msm_g1.cu and for G2 in msm_g2.cu.
 #pragma once
+#include <algorithm>
 #include "msm.cuh"
 #include "curve.cuh"
 #include "scan.cuh"
@@ -243,12 +244,20 @@ __global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate(cons
     const Task tk = tasks[t];
     const uint32_t* base = jobs ? jobs[tk.job].points : points;
     XYZZ<F> acc = XYZZ<F>::inf();
+    if (entries) {
 #pragma unroll 1
-    for (uint32_t e = 0; e < tk.len; e++) {
-      const uint32_t ent = entries[tk.start + e];
-      Affine<F> p = ld_affine<F>(base + (size_t)(ent & ~NEG_BIT) * PW);
-      if (ent & NEG_BIT) p.y = p.y.neg();
-      acc = xyzz_madd(acc, p);
+      for (uint32_t e = 0; e < tk.len; e++) {
+        const uint32_t ent = entries[tk.start + e];
+        Affine<F> p = ld_affine<F>(base + (size_t)(ent & ~NEG_BIT) * PW);
+        if (ent & NEG_BIT) p.y = p.y.neg();
+        acc = xyzz_madd(acc, p);
+      }
+    } else {  // after batch-affine rounds: points in bucket order, (0, 0) = infinity
+#pragma unroll 1
+      for (uint32_t e = 0; e < tk.len; e++) {
+        const Affine<F> p = ld_affine<F>(base + (size_t)(tk.start + e) * PW);
+        if (!(p.x.is_zero() && p.y.is_zero())) acc = xyzz_madd(acc, p);
+      }
     }
     uint32_t* dst = tk.dst < nb ? buckets + (size_t)tk.dst * XW : partials + (size_t)(tk.dst - nb) * XW;
     st_xyzz<F>(dst, acc);
@@ -540,6 +549,144 @@ __global__ void k_store_inf(uint32_t* out) {
   if (threadIdx.x == 0) st_affine<F>(out, Affine<F>{F::zero(), F::one()});
 }
 
+// ---------------------------------------------------------- batch-affine rounds ----
+// Before the XYZZ accumulation, buckets are halved R times by adding their points in pairs
+// in affine coordinates: lambda = (y2 - y1) / (x2 - x1) (or 3 x^2 / 2y for equal points),
+// x3 = lambda^2 - x1 - x2, y3 = lambda (x1 - x3) - y1.  The divisions of kAffK consecutive
+// pairs share one inversion (Montgomery's simultaneous inversion: prefix products, one
+// inverse, back substitution), so an addition costs about 6 products instead of the
+// 10 of an XYZZ + affine addition.  Round r maps bucket b's c_b points at in_off[b] to
+// ceil(c_b / 2) points at out_off[b]; an odd last point is copied.  Points at infinity
+// inside the rounds are (0, 0), which is on neither curve.
+constexpr uint32_t kAffK = 64;
+
+template <class F>
+CSB_DEV bool aff_zero(const Affine<F>& a) { return a.x.is_zero() && a.y.is_zero(); }
+
+// Pair of round-r inputs for output slot s of bucket b.  FIRST: round 0 reads the bases
+// through the sorted entries (sign bit -> negated y); later rounds read the previous round.
+template <class F, bool FIRST>
+CSB_DEV void aff_pair(const uint32_t* in_off, const uint32_t* out_off, uint32_t b, uint32_t s,
+                      const uint32_t* entries, const uint32_t* src, Affine<F>& p, Affine<F>& q, bool& has_q) {
+  constexpr int PW = 2 * FieldWords<F>::value;
+  const uint32_t j = s - out_off[b];
+  const uint32_t i0 = in_off[b] + 2 * j;
+  has_q = i0 + 1 < in_off[b + 1];
+  if (FIRST) {
+    const uint32_t e0 = entries[i0];
+    p = ld_affine<F>(src + (size_t)(e0 & ~NEG_BIT) * PW);
+    if (e0 & NEG_BIT) p.y = p.y.neg();
+    if (has_q) {
+      const uint32_t e1 = entries[i0 + 1];
+      q = ld_affine<F>(src + (size_t)(e1 & ~NEG_BIT) * PW);
+      if (e1 & NEG_BIT) q.y = q.y.neg();
+    }
+  } else {
+    p = ld_affine<F>(src + (size_t)i0 * PW);
+    if (has_q) q = ld_affine<F>(src + (size_t)(i0 + 1) * PW);
+  }
+}
+
+// Denominator of a pair and its kind: 0 add, 1 double, 2 result p, 3 result q, 4 infinity.
+template <class F>
+CSB_DEV int aff_kind(const Affine<F>& p, const Affine<F>& q, bool has_q, F& d) {
+  d = F::one();
+  if (!has_q || aff_zero(q)) return 2;
+  if (aff_zero(p)) return 3;
+  if (!(p.x == q.x)) {
+    d = q.x - p.x;
+    return 0;
+  }
+  if (p.y == q.y) {
+    d = p.y.dbl();
+    return 1;
+  }
+  return 4;
+}
+
+template <class F>
+CSB_DEV uint32_t bucket_of_slot(const uint32_t* off, uint32_t nb, uint32_t s) {
+  uint32_t lo = 0, hi = nb;  // largest b with off[b] <= s (empty buckets share offsets)
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (off[mid] <= s) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+template <class F, bool FIRST>
+__global__ void __launch_bounds__(128) k_affine_round(const uint32_t* __restrict__ in_off,
+                                                      const uint32_t* __restrict__ out_off, uint32_t nb,
+                                                      const uint32_t* __restrict__ entries,
+                                                      const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
+                                                      uint32_t* __restrict__ pref) {
+  constexpr int FW = FieldWords<F>::value;
+  constexpr int PW = 2 * FW;
+  const uint32_t total = out_off[nb];
+  const uint32_t s0 = (blockIdx.x * blockDim.x + threadIdx.x) * kAffK;
+  if (s0 >= total) return;
+  const uint32_t s1 = min(total, s0 + kAffK);
+  const uint32_t b0 = bucket_of_slot<F>(out_off, nb, s0);
+  // phase 1: prefix products of the denominators
+  F acc = F::one();
+  uint32_t b = b0;
+  for (uint32_t s = s0; s < s1; s++) {
+    while (out_off[b + 1] <= s) b++;
+    Affine<F> p, q;
+    bool has_q;
+    aff_pair<F, FIRST>(in_off, out_off, b, s, entries, src, p, q, has_q);
+    F d;
+    aff_kind(p, q, has_q, d);
+    acc = acc * d;
+    st_field(pref + (size_t)s * FW, acc);
+  }
+  F inv = acc.inv();
+  // phase 2: back substitution and the additions, last slot first
+  for (uint32_t s = s1; s-- > s0;) {
+    while (out_off[b] > s) b--;
+    Affine<F> p, q;
+    bool has_q;
+    aff_pair<F, FIRST>(in_off, out_off, b, s, entries, src, p, q, has_q);
+    F d;
+    const int kind = aff_kind(p, q, has_q, d);
+    F before = F::one();
+    if (s > s0) {  // written above by this thread: a plain (coherent) load, not __ldg
+      uint32_t* bw = reinterpret_cast<uint32_t*>(&before);
+      const uint4* pv = reinterpret_cast<const uint4*>(pref + (size_t)(s - 1) * FW);
+#pragma unroll
+      for (int k = 0; k < FW / 4; k++) {
+        const uint4 v = pv[k];
+        bw[4 * k] = v.x; bw[4 * k + 1] = v.y; bw[4 * k + 2] = v.z; bw[4 * k + 3] = v.w;
+      }
+    }
+    const F id = inv * before;  // 1 / d
+    inv = inv * d;
+    Affine<F> r;
+    if (kind == 0 || kind == 1) {
+      const F lam = kind == 0 ? (q.y - p.y) * id : (p.x.sqr() * (F::one() + F::one() + F::one())) * id;
+      const F x3 = lam.sqr() - p.x - q.x;
+      r.x = x3;
+      r.y = lam * (p.x - x3) - p.y;
+    } else if (kind == 2) {
+      r = p;
+    } else if (kind == 3) {
+      r = q;
+    } else {
+      r.x = F::zero();
+      r.y = F::zero();
+    }
+    st_affine<F>(dst + (size_t)s * PW, r);
+  }
+}
+
+// out[b] = ceil(in[b] / 2) for the next round's counts (written into a count array that the
+// scan turns into offsets; out[nb] = 0 so the scan's last element is the total).
+static __global__ void k_half_counts(const uint32_t* __restrict__ off, uint32_t nb, uint32_t* __restrict__ out) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nb) out[b] = (off[b + 1] - off[b] + 1) >> 1;
+  if (b == nb) out[b] = 0;
+}
+
 // --------------------------------------------------------------- workspace layout ----
 // counters block: [0] tasks, [1] partial slots, [2] split buckets; hist at +16 and
 // bin cursors at +96 (kMaxTask + 1 words each).
@@ -549,12 +696,14 @@ constexpr uint32_t kTopSegments = 256;
 
 struct Layout {
   size_t counts, offsets, entries, tasks, multi, partials, buckets, lv_y, lv_z, lv_y2, lv_z2, wsum,
-      counters, total;
+      counters, off2, pa, pb, pref, total;
+  bool affine;
 };
 
 static inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
-inline Layout make_layout(uint32_t n, int c, int xyzz_bytes, uint32_t task_len, bool fixed = false) {
+inline Layout make_layout(uint32_t n, int c, int xyzz_bytes, uint32_t task_len, bool fixed = false,
+                          bool affine = true) {
   const int W = num_windows(c);
   const size_t nb = fixed ? ((size_t)1 << (c - 1)) : (size_t)W << (c - 1);
   const int WR = fixed ? 1 : W;  // bucket sets reduced
@@ -578,8 +727,30 @@ inline Layout make_layout(uint32_t n, int c, int xyzz_bytes, uint32_t task_len, 
   L.lv_y2 = o;    o = align256(o + n2 * xyzz_bytes);
   L.lv_z2 = o;    o = align256(o + n2 * xyzz_bytes);
   L.wsum = o;     o = align256(o + (size_t)WR * xyzz_bytes);
+  L.affine = affine;
+  if (affine) {  // batch-affine rounds: offsets ping-pong, two point arrays, prefix products
+    const size_t pb = (size_t)xyzz_bytes / 2, fb = (size_t)xyzz_bytes / 4;
+    L.off2 = o;   o = align256(o + (nb + 1) * sizeof(uint32_t));
+    L.pa = o;     o = align256(o + (ne / 2 + 2 * nb + 1) * pb);
+    L.pb = o;     o = align256(o + (ne / 4 + 2 * nb + 1) * pb);
+    L.pref = o;   o = align256(o + (ne / 2 + 2 * nb + 1) * fb);
+  }
   L.total = o + scan_workspace_bytes(nb + 1);
   return L;
+}
+
+// Batch-affine rounds before the XYZZ accumulation (the expected bucket size is N W /
+// buckets; a round needs about 8 points per bucket to pay).  Measured at 2^20: G1 is
+// fastest without rounds (its XYZZ addition costs 10 products of 136 wide multiplies and
+// already outruns the gather-bound affine round), G2 with two (Fq2 products are 3 Fq
+// products, so the 6-vs-10 product saving outweighs the extra traffic).
+template <class F>
+inline int auto_affine_rounds(uint32_t n, int W, size_t nb) {
+  const int cap = FieldWords<F>::value == 16 ? 2 : 0;
+  const double avg = (double)n * W / (double)nb;
+  int r = 0;
+  while (r < cap && avg >= (double)(8u << r)) r++;
+  return r;
 }
 
 template <class F>
@@ -616,7 +787,8 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   const int W = num_windows(c);
   if (FIXED && (uint64_t)W * n >= (uint64_t)NEG_BIT) return cudaErrorInvalidValue;
   const uint32_t nb = FIXED ? (1u << (c - 1)) : (uint32_t)W << (c - 1);
-  const Layout L = make_layout(n, c, XB, kMinTask, FIXED);
+  const int rounds_req = cfg.affine < 0 ? auto_affine_rounds<F>(n, W, nb) : cfg.affine;
+  const Layout L = make_layout(n, c, XB, kMinTask, FIXED, cfg.affine != 0);
   if (work_bytes < L.total || d_work == nullptr) return cudaErrorInvalidValue;
   char* base = static_cast<char*>(d_work);
   uint32_t* counters = reinterpret_cast<uint32_t*>(base + L.counters);
@@ -646,18 +818,51 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
     return e;
   k_scatter<F, FIXED><<<(n + T - 1) / T, T, 0, st>>>(d_scalars, d_points, n, c, W, counts, entries);
   note_launch();
-  k_task_hist<F><<<(nb + T - 1) / T, T, 0, st>>>(offsets, nb, task_len, counters + kCtrHist, buckets);
+  // batch-affine halving rounds (counts is free again and holds the halved counts)
+  const uint32_t* acc_entries = entries;
+  const uint32_t* acc_points = d_points;
+  uint32_t* acc_off = offsets;
+  const int rounds = L.affine ? std::min(rounds_req, 6) : 0;
+  if (rounds > 0) {
+    uint32_t* off_in = offsets;
+    uint32_t* off_out = reinterpret_cast<uint32_t*>(base + L.off2);
+    uint32_t* pa = reinterpret_cast<uint32_t*>(base + L.pa);
+    uint32_t* pb = reinterpret_cast<uint32_t*>(base + L.pb);
+    uint32_t* pref = reinterpret_cast<uint32_t*>(base + L.pref);
+    const uint32_t* src = d_points;
+    uint32_t* dst = pa;
+    size_t max_slots = (size_t)n * W / 2 + 2 * (size_t)nb + 1;
+    for (int r = 0; r < rounds; r++) {
+      k_half_counts<<<(nb + 1 + T - 1) / T, T, 0, st>>>(off_in, nb, counts);
+      if ((e = scan_exclusive_u32(counts, off_out, nb + 1, scan_tmp, st)) != cudaSuccess) return e;
+      const size_t threads = (max_slots + kAffK - 1) / kAffK;
+      const unsigned blocks = (unsigned)((threads + 127) / 128);
+      if (r == 0)
+        k_affine_round<F, true><<<blocks, 128, 0, st>>>(off_in, off_out, nb, entries, d_points, dst, pref);
+      else
+        k_affine_round<F, false><<<blocks, 128, 0, st>>>(off_in, off_out, nb, nullptr, src, dst, pref);
+      note_launch(2);
+      src = dst;
+      dst = dst == pa ? pb : pa;
+      uint32_t* t = off_in; off_in = off_out; off_out = t;
+      max_slots = max_slots / 2 + 2 * (size_t)nb + 1;
+    }
+    acc_entries = nullptr;
+    acc_points = src;
+    acc_off = off_in;
+  }
+  k_task_hist<F><<<(nb + T - 1) / T, T, 0, st>>>(acc_off, nb, task_len, counters + kCtrHist, buckets);
   note_launch();
   k_task_bins<<<1, 32, 0, st>>>(counters + kCtrHist, task_len, counters + kCtrCursor, counters);
   note_launch();
-  k_task_emit<F><<<(nb + T - 1) / T, T, 0, st>>>(offsets, nb, task_len, counters + kCtrCursor, tasks,
+  k_task_emit<F><<<(nb + T - 1) / T, T, 0, st>>>(acc_off, nb, task_len, counters + kCtrCursor, tasks,
                                                   counters, multi);
   note_launch();
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (cfg.acc_start) cudaEventRecord(cfg.acc_start, st);
-  k_accumulate<F><<<accumulate_grid<F>(sms), 128, 0, st>>>(tasks, counters, entries, d_points, nb,
+  k_accumulate<F><<<accumulate_grid<F>(sms), 128, 0, st>>>(tasks, counters, acc_entries, acc_points, nb,
                                                            buckets, partials);
   note_launch();
   k_combine_small<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);

@@ -72,6 +72,7 @@ struct cs_ctx {
   float last_ms = 0.f;
   float last_phase_ms = 0.f;
   bool phase_valid = false;
+  int msm_affine = -1;         // batch-affine rounds of MSMs on this context: -1 auto, 0 off
   std::string err;
   std::mutex mu;               // one call at a time per context
   // auxiliary streams / events for fork-join pipelines (prove), created on first use

@@ -170,6 +170,10 @@ const char *cs_ctx_error(cs_ctx *ctx);
 float cs_ctx_last_ms(cs_ctx *ctx);
 /* Device time in milliseconds of the bucket-accumulation kernels of the last MSM. */
 float cs_ctx_last_phase_ms(cs_ctx *ctx);
+/* Batch-affine halving rounds run before the XYZZ bucket accumulation by this context's
+ * cs_msm / cs_msm_device / cs_msm_fixed_device calls: -1 automatic (default), 0 none, 1..6.
+ * Results do not depend on it. */
+int cs_ctx_set_msm_affine_rounds(cs_ctx *ctx, int rounds);
 
 /* Multi-exponentiation with host pointers: copies in, computes, copies the affine result
  * out, synchronises.  ec2 selects G2.  window = Pippenger window bits (0 = automatic). */

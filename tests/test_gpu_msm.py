@@ -154,3 +154,32 @@ def test_scmul_matches_oracle(ctx, oracle, golden, ec2):
                      point_stride_words=0)
     ctx.sync()
     assert np.array_equal(dout.cpu().numpy().view(np.uint32), oracle.scmul(s, p[3:4], ec2))
+
+
+@pytest.mark.parametrize("rounds", [0, 1, 3, 6])
+def test_msm_affine_rounds(ctx, oracle, pts_g1, pts_g2, rounds):
+    """Batch-affine halving rounds before the XYZZ accumulation: same results for any number
+    of rounds, including equal points (doubling), P + (-P) (infinity inside a round), zero
+    scalars, one giant bucket (all scalars equal) and G2."""
+    one = oracle.const(0)[0]
+    inf = np.concatenate([np.zeros(8, np.uint32), one])
+    q = 21888242871839275222246405745257275088696311157297823662689037894645226208583
+    ctx.set_msm_affine_rounds(rounds)
+    try:
+        rng = np.random.Generator(np.random.PCG64(700 + rounds))
+        s = random_field(rng, pts_g1.shape[0], 1)
+        assert np.array_equal(ctx.msm(s, pts_g1, window=8), oracle.msm(s, pts_g1))
+        P = pts_g1[7].copy()
+        negP = P.copy()
+        negP[8:] = ints_to_limbs([q - limbs_to_int(P[8:])])[0]
+        pts = np.stack([P] * 64 + [negP] * 63 + [inf] * 5 + list(pts_g1[100:164]))
+        sc = np.concatenate([np.tile(ints_to_limbs([424242]), (127, 1)), random_field(rng, 5, 1),
+                             random_field(rng, 64, 1)])
+        sc[130] = 0
+        assert np.array_equal(ctx.msm(sc, pts, window=6), oracle.msm(sc, pts))
+        s1 = np.tile(ints_to_limbs([0xdeadbeef12345]), (4096, 1))
+        assert np.array_equal(ctx.msm(s1, pts_g1, window=10), oracle.msm(s1, pts_g1))
+        s2 = random_field(rng, pts_g2.shape[0], 1)
+        assert np.array_equal(ctx.msm(s2, pts_g2, ec2=True, window=6), oracle.msm(s2, pts_g2, ec2=1))
+    finally:
+        ctx.set_msm_affine_rounds(-1)
