@@ -161,6 +161,29 @@ _SIGNATURES = [
     ("cs_setup_pow_scalars", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint32, _vp]),
     ("cs_r1cs_layer_eval", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_uint32, _vp, _vp]),
     ("ec_jacreduce_server_h", None, [ctypes.POINTER(JacaddReduced)]),
+    ("ec_jac2aff_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ec2_jac2aff_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ec_jacaddreduce_h", None, [_vp, _vp] + [ctypes.c_uint32] * 5),
+    ("ec2_jacaddreduce_h", None, [_vp, _vp] + [ctypes.c_uint32] * 5),
+    ("ec_jacscmul_h", None, [_vp, _vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ec2_jacscmul_h", None, [_vp, _vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ec_jacsc1mul_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ec2_jacsc1mul_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ec_isoncurve_h", ctypes.c_uint32, [_vp, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ec2_isoncurve_h", ctypes.c_uint32, [_vp, ctypes.c_uint32, ctypes.c_uint32]),
+    ("sortu256_idx_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ntt_build_h", None, [_vp, ctypes.c_uint32]),
+    ("init_h", None, []),
+    ("release_h", None, []),
+    ("get_nprocs_h", ctypes.c_uint32, []),
+    ("readU256CircuitFile_h", None, [_vp, ctypes.c_char_p, ctypes.c_ulonglong]),
+    ("readU256PKFile_h", None, [_vp, ctypes.c_char_p, ctypes.c_ulonglong]),
+    ("readU256DataFile_h", None, [_vp, ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32]),
+    ("readU256DataFileFromOffset_h", None, [_vp, ctypes.c_char_p, ctypes.c_ulonglong, ctypes.c_ulonglong]),
+    ("writeU256DataFile_h", None, [_vp, ctypes.c_char_p, ctypes.c_ulonglong]),
+    ("appendU256DataFile_h", None, [_vp, ctypes.c_char_p, ctypes.c_ulonglong]),
+    ("readWitnessFile_h", None, [_vp, ctypes.c_char_p, ctypes.c_uint32, ctypes.c_ulonglong]),
+    ("writeWitnessFile_h", None, [_vp, ctypes.c_char_p, ctypes.c_ulonglong]),
     ("ec2_jacreduce_server_h", None, [ctypes.POINTER(JacaddReduced)]),
 ]
 

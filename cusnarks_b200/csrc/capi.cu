@@ -120,6 +120,16 @@ int msm_device_locked(cs_ctx* ctx, int ec2, const uint32_t* s, const uint32_t* p
 
 }  // namespace
 
+namespace csb {
+// Default context of the current device for the drop-in entry points (created on first use);
+// *status and the thread's cs_last_error describe a failure.
+cs_ctx* dropin_ctx(int* status) { return default_ctx(status); }
+void dropin_status(int st, const char* msg) {
+  t_status = st;
+  if (msg) t_error = msg;
+}
+}  // namespace csb
+
 extern "C" {
 
 int cs_ctx_create(int device, cs_ctx** out) {

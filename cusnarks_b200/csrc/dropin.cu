@@ -1,0 +1,316 @@
+// dropin.cu -- the rest of the reference's host functions the Cython layer binds
+// (src/cython/_utils_host.pxd): point utilities of src/cuda/ec.cpp on the GPU, and the
+// bookkeeping / file routines of bigint.cpp, ntt.cpp, init.cpp, utils_host.cpp and
+// file_utils.cpp on the host.  Same names, arguments and layouts; like the other drop-ins,
+// failures are reported by cs_last_status() / cs_last_error() instead of exit().
+//
+// Point rows: G1 Jacobian 3 x 8 words (X, Y, Z), affine 2 x 8; G2 Jacobian 3 x 16, affine
+// 2 x 16; Montgomery form; infinity (0, 1, 0) / (0, 1).  Jacobian results are returned
+// normalised (Z = 1), which is the same point as the reference's (x = X/Z^2, y = Y/Z^3).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/cusnarks_b200.h"
+#include "ecops.cuh"
+#include "runtime.cuh"
+
+namespace csb {
+cs_ctx* dropin_ctx(int* status);
+void dropin_status(int st, const char* msg);
+}  // namespace csb
+
+namespace {
+
+using namespace csb;
+
+// Stages host rows into the context's input arena, runs fn(d_in, d_out) on its stream and
+// copies out_words back.  Returns a cs status.
+// d_scr: scratch_words of device scratch that overlaps neither input nor output.
+template <class Fn>
+int run_on_device(const char* what, const uint32_t* in, size_t in_words, uint32_t* out, size_t out_words,
+                  size_t scratch_words, Fn fn) {
+  int st = CS_OK;
+  cs_ctx* ctx = dropin_ctx(&st);
+  if (!ctx) return st;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  auto al = [](size_t w) { return (w * 4 + 255) & ~size_t(255); };
+  const size_t in_b = al(in_words), out_b = al(out_words);
+  cudaError_t e = ctx->in.reserve(in_b + out_b + al(scratch_words), ctx->stream);
+  if (e != cudaSuccess) { dropin_status(CS_ERR_NOMEM, what); return CS_ERR_NOMEM; }
+  char* base = static_cast<char*>(ctx->in.ptr);
+  uint32_t* d_in = reinterpret_cast<uint32_t*>(base);
+  uint32_t* d_out = reinterpret_cast<uint32_t*>(base + in_b);
+  uint32_t* d_scr = reinterpret_cast<uint32_t*>(base + in_b + out_b);
+  if (in_words) e = cudaMemcpyAsync(d_in, in, in_words * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = fn(d_in, d_out, d_scr, ctx->stream);
+  if (e == cudaSuccess && out_words) e = cudaMemcpyAsync(out, d_out, out_words * 4, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    const std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    cudaGetLastError();
+    dropin_status(CS_ERR_CUDA, m.c_str());
+    return CS_ERR_CUDA;
+  }
+  dropin_status(CS_OK, "");
+  return CS_OK;
+}
+
+bool bad_pidx(uint32_t pidx, const char* what) {
+  if (pidx == 0) return false;
+  dropin_status(CS_ERR_ARG, (std::string(what) + ": points live in MOD_GROUP (pidx 0)").c_str());
+  return true;
+}
+
+// y (rows of 2 or 3 coordinates) from affine rows in d_aff.
+cudaError_t emit_rows(bool ec2, const uint32_t* d_aff, uint32_t n, uint32_t* d_out, bool strip, cudaStream_t st) {
+  const size_t fw = ec2 ? 16 : 8;
+  if (strip)
+    return cudaMemcpyAsync(d_out, d_aff, (size_t)n * 2 * fw * 4, cudaMemcpyDeviceToDevice, st);
+  return ec2 ? affine_to_jac_g2(d_aff, n, d_out, st) : affine_to_jac_g1(d_aff, n, d_out, st);
+}
+
+void jac2aff(bool ec2, uint32_t* y, const uint32_t* x, uint32_t n, uint32_t pidx, uint32_t strip) {
+  if (bad_pidx(pidx, "ec_jac2aff_h")) return;
+  const size_t fw = ec2 ? 16 : 8;
+  run_on_device("ec_jac2aff_h", x, (size_t)n * 3 * fw, y, (size_t)n * (strip ? 2 : 3) * fw, (size_t)n * 2 * fw,
+                [&](uint32_t* d_in, uint32_t* d_out, uint32_t* d_scr, cudaStream_t st) {
+                  uint32_t* d_aff = strip ? d_out : d_scr;
+                  cudaError_t e = ec2 ? jac_to_affine_g2(d_in, n, d_aff, st) : jac_to_affine_g1(d_in, n, d_aff, st);
+                  if (e != cudaSuccess || strip) return e;
+                  return emit_rows(ec2, d_aff, n, d_out, false, st);
+                });
+}
+
+void jacaddreduce(bool ec2, uint32_t* z, const uint32_t* x, uint32_t n, uint32_t pidx, uint32_t to_aff,
+                  uint32_t add_in, uint32_t strip) {
+  if (bad_pidx(pidx, "ec_jacaddreduce_h")) return;
+  (void)to_aff;  // affine and Z = 1 Jacobian rows coincide
+  const size_t fw = ec2 ? 16 : 8;
+  const int dims = add_in ? 2 : 3;
+  run_on_device("ec_jacaddreduce_h", x, (size_t)n * dims * fw, z, (strip ? 2 : 3) * fw, 2 * fw,
+                [&](uint32_t* d_in, uint32_t* d_out, uint32_t* d_aff, cudaStream_t st) {
+                  cudaError_t e = ec2 ? point_sum_g2(d_in, n, dims, d_aff, st) : point_sum_g1(d_in, n, dims, d_aff, st);
+                  if (e != cudaSuccess) return e;
+                  return emit_rows(ec2, d_aff, 1, d_out, strip != 0, st);
+                });
+}
+
+// z[i] = scl[i] * P_i: P_i rows of 3 (Jacobian) or 2 (add_last: affine) coordinates,
+// stride 0 = one shared point (the sc1mul form).
+void jacscmul(bool ec2, uint32_t* z, const uint32_t* scl, const uint32_t* x, uint32_t n, uint32_t add_last,
+              bool shared_point) {
+  const size_t fw = ec2 ? 16 : 8;
+  const uint32_t dims = add_last ? 2 : 3;
+  const uint32_t npts = shared_point ? 1u : n;
+  // input: scalars (n x 8) then points (npts x dims x fw)
+  std::vector<uint32_t> in((size_t)n * 8 + (size_t)npts * dims * fw);
+  std::memcpy(in.data(), scl, (size_t)n * 32);
+  std::memcpy(in.data() + (size_t)n * 8, x, (size_t)npts * dims * fw * 4);
+  // scratch: npts affine bases, then n affine products
+  run_on_device("ec_jacscmul_h", in.data(), in.size(), z, (size_t)n * 3 * fw, ((size_t)npts + n) * 2 * fw,
+                [&](uint32_t* d_in, uint32_t* d_out, uint32_t* d_scr, cudaStream_t st) {
+                  const uint32_t* d_s = d_in;
+                  uint32_t* d_p = d_in + (size_t)n * 8;
+                  uint32_t* d_base = d_p;
+                  cudaError_t e = cudaSuccess;
+                  if (!add_last) {  // Jacobian bases -> affine
+                    d_base = d_scr;
+                    e = ec2 ? jac_to_affine_g2(d_p, npts, d_base, st) : jac_to_affine_g1(d_p, npts, d_base, st);
+                  }
+                  if (e != cudaSuccess) return e;
+                  uint32_t* d_aff = d_scr + (size_t)npts * 2 * fw;
+                  const uint32_t stride = shared_point ? 0u : (uint32_t)(2 * fw);
+                  e = ec2 ? scmul_g2(d_s, d_base, stride, n, d_aff, st) : scmul_g1(d_s, d_base, stride, n, d_aff, st);
+                  if (e != cudaSuccess) return e;
+                  return ec2 ? affine_to_jac_g2(d_aff, n, d_out, st) : affine_to_jac_g1(d_aff, n, d_out, st);
+                });
+}
+
+uint32_t isoncurve(bool ec2, const uint32_t* x, uint32_t is_affine, uint32_t pidx) {
+  if (bad_pidx(pidx, "ec_isoncurve_h")) return 0;
+  const size_t fw = ec2 ? 16 : 8;
+  uint32_t flag = 0;
+  run_on_device("ec_isoncurve_h", x, (is_affine ? 2 : 3) * fw, &flag, 1, 0,
+                [&](uint32_t* d_in, uint32_t* d_out, uint32_t*, cudaStream_t st) {
+                  return ec2 ? on_curve_g2(d_in, is_affine ? 0 : 1, d_out, st)
+                             : on_curve_g1(d_in, is_affine ? 0 : 1, d_out, st);
+                });
+  return flag;
+}
+
+}  // namespace
+
+extern "C" {
+
+void ec_jac2aff_h(uint32_t* y, uint32_t* x, uint32_t n, uint32_t pidx, uint32_t strip_last) {
+  jac2aff(false, y, x, n, pidx, strip_last);
+}
+void ec2_jac2aff_h(uint32_t* y, uint32_t* x, uint32_t n, uint32_t pidx, uint32_t strip_last) {
+  jac2aff(true, y, x, n, pidx, strip_last);
+}
+void ec_jacaddreduce_h(uint32_t* z, uint32_t* x, uint32_t n, uint32_t pidx, uint32_t to_aff, uint32_t add_in,
+                       uint32_t strip_last) {
+  jacaddreduce(false, z, x, n, pidx, to_aff, add_in, strip_last);
+}
+void ec2_jacaddreduce_h(uint32_t* z, uint32_t* x, uint32_t n, uint32_t pidx, uint32_t to_aff, uint32_t add_in,
+                        uint32_t strip_last) {
+  jacaddreduce(true, z, x, n, pidx, to_aff, add_in, strip_last);
+}
+void ec_jacscmul_h(uint32_t* z, uint32_t* scl, uint32_t* x, uint32_t n, uint32_t pidx, uint32_t add_last) {
+  if (bad_pidx(pidx, "ec_jacscmul_h")) return;
+  jacscmul(false, z, scl, x, n, add_last, false);
+}
+void ec2_jacscmul_h(uint32_t* z, uint32_t* scl, uint32_t* x, uint32_t n, uint32_t pidx, uint32_t add_last) {
+  if (bad_pidx(pidx, "ec2_jacscmul_h")) return;
+  jacscmul(true, z, scl, x, n, add_last, false);
+}
+// x = n scalars followed by one base point (ec.cpp:819)
+void ec_jacsc1mul_h(uint32_t* z, uint32_t* x, uint32_t n, uint32_t pidx, uint32_t add_last) {
+  if (bad_pidx(pidx, "ec_jacsc1mul_h")) return;
+  jacscmul(false, z, x, x + (size_t)n * 8, n, add_last, true);
+}
+void ec2_jacsc1mul_h(uint32_t* z, uint32_t* x, uint32_t n, uint32_t pidx, uint32_t add_last) {
+  if (bad_pidx(pidx, "ec2_jacsc1mul_h")) return;
+  jacscmul(true, z, x, x + (size_t)n * 8, n, add_last, true);
+}
+uint32_t ec_isoncurve_h(uint32_t* x, uint32_t is_affine, uint32_t pidx) { return isoncurve(false, x, is_affine, pidx); }
+uint32_t ec2_isoncurve_h(uint32_t* x, uint32_t is_affine, uint32_t pidx) { return isoncurve(true, x, is_affine, pidx); }
+
+// ------------------------------------------------------------------ host routines ----
+// bigint.cpp:72: idx = 0..len-1, sorted (std::sort, unstable) by the most significant word
+// of v[idx] when sort_en.
+void sortu256_idx_h(uint32_t* idx, const uint32_t* v, uint32_t len, uint32_t sort_en) {
+  for (uint32_t i = 0; i < len; i++) idx[i] = i;
+  if (sort_en)
+    std::sort(idx, idx + len, [v](uint32_t a, uint32_t b) { return v[(size_t)a * 8 + 7] < v[(size_t)b * 8 + 7]; });
+}
+
+// ntt.cpp:1116: transform decomposition parameters for nsamples (the prover reads levels
+// and fft_N to size its roots tables).
+void ntt_build_h(fft_params_t* p, uint32_t nsamples) {
+  const uint32_t min_samples = 1u << 6;
+  const uint32_t ns = std::max(nsamples, min_samples);
+  uint32_t levels = (uint32_t)std::ceil(std::log2((double)ns));
+  std::memset(p, 0, sizeof(fft_params_t));
+  p->padding = (1u << levels) - nsamples;
+  p->levels = levels;
+  if (ns <= 32) {
+    p->fft_type = FFT_T_1D;
+    p->fft_N[0] = levels;
+  } else if (ns <= (1u << 20)) {
+    p->fft_type = FFT_T_3D;
+    p->fft_N[3] = levels / 2;
+    p->fft_N[2] = levels - levels / 2;
+    p->fft_N[1] = levels / 4;
+    p->fft_N[0] = (levels - levels / 2) / 2;
+  } else {
+    p->fft_type = FFT_T_4D;
+    p->fft_N[7] = levels / 2;
+    p->fft_N[6] = levels - levels / 2;
+    p->fft_N[5] = levels / 4;
+    p->fft_N[4] = (levels - levels / 2) / 2;
+    levels = p->fft_N[7];
+    p->fft_N[3] = levels / 2;
+    p->fft_N[2] = levels - levels / 2;
+    p->fft_N[1] = levels / 4;
+    p->fft_N[0] = (levels - levels / 2) / 2;
+  }
+}
+
+uint32_t get_nprocs_h(void) {
+  const unsigned n = std::thread::hardware_concurrency();
+  return n ? n : 1;
+}
+
+// init.cpp:44 / :54.  Nothing to load here (no roots files: twiddles are computed on the
+// device when first needed); init_h creates the current device's default context early,
+// release_h synchronises it.
+void init_h(void) {
+  int st = CS_OK;
+  dropin_ctx(&st);
+}
+void release_h(void) {
+  int st = CS_OK;
+  cs_ctx* ctx = dropin_ctx(&st);
+  if (ctx) cs_ctx_sync(ctx);
+}
+
+// file_utils.cpp routines (raw little-endian uint32 words).
+void readU256CircuitFile_h(uint32_t* samples, const char* filename, unsigned long long nwords) {
+  FILE* f = std::fopen(filename, "rb");
+  if (!f) { dropin_status(CS_ERR_ARG, "readU256CircuitFile_h: cannot open file"); return; }
+  if (nwords) {
+    if (std::fread(samples, 4, nwords, f) != nwords) dropin_status(CS_ERR_ARG, "readU256CircuitFile_h: short file");
+  } else {
+    size_t i = 0;
+    while (std::fread(&samples[i], 4, 1, f) == 1) i++;
+  }
+  std::fclose(f);
+}
+void readU256PKFile_h(uint32_t* samples, const char* filename, unsigned long long nwords) {
+  readU256CircuitFile_h(samples, filename, nwords);
+}
+// insize 256-bit elements in the file; every (insize/outsize)-th is kept
+void readU256DataFile_h(uint32_t* samples, const char* filename, uint32_t insize, uint32_t outsize) {
+  FILE* f = std::fopen(filename, "rb");
+  if (!f) { dropin_status(CS_ERR_ARG, "readU256DataFile_h: cannot open file"); return; }
+  const uint32_t count = outsize ? insize / outsize : 1;
+  if (count != 1) {
+    uint32_t r[8];
+    uint32_t k = 0;
+    for (uint32_t i = 0; i < insize; i++) {
+      if (std::fread(r, 4, 8, f) != 8) break;
+      if (i % count == 0) std::memcpy(&samples[(size_t)k++ * 8], r, 32);
+    }
+  } else if (std::fread(samples, 32, outsize, f) != outsize) {
+    dropin_status(CS_ERR_ARG, "readU256DataFile_h: short file");
+  }
+  std::fclose(f);
+}
+void readU256DataFileFromOffset_h(uint32_t* samples, const char* filename, unsigned long long woffset,
+                                  unsigned long long nwords) {
+  FILE* f = std::fopen(filename, "rb");
+  if (!f) { dropin_status(CS_ERR_ARG, "readU256DataFileFromOffset_h: cannot open file"); return; }
+  if (std::fseek(f, (long)(woffset * 4), SEEK_SET) != 0 || std::fread(samples, 4, nwords, f) != nwords)
+    dropin_status(CS_ERR_ARG, "readU256DataFileFromOffset_h: short file");
+  std::fclose(f);
+}
+void writeU256DataFile_h(uint32_t* samples, const char* filename, unsigned long long nwords) {
+  FILE* f = std::fopen(filename, "wb");
+  if (!f) { dropin_status(CS_ERR_ARG, "writeU256DataFile_h: cannot open file"); return; }
+  std::fwrite(samples, 4, nwords, f);
+  std::fclose(f);
+}
+void appendU256DataFile_h(uint32_t* samples, const char* filename, unsigned long long nwords) {
+  FILE* f = std::fopen(filename, "ab");
+  if (!f) { dropin_status(CS_ERR_ARG, "appendU256DataFile_h: cannot open file"); return; }
+  std::fwrite(samples, 4, nwords, f);
+  std::fclose(f);
+}
+// witness .bin (fmt 1: values after the 4-word header) / .dat (fmt 0: values from byte 32)
+void readWitnessFile_h(uint32_t* samples, const char* filename, uint32_t fmt, unsigned long long inlen) {
+  FILE* f = std::fopen(filename, "rb");
+  if (!f) { dropin_status(CS_ERR_ARG, "readWitnessFile_h: cannot open file"); return; }
+  if (std::fseek(f, fmt ? 16 : 32, SEEK_SET) != 0 || std::fread(samples, 32, inlen, f) != inlen)
+    dropin_status(CS_ERR_ARG, "readWitnessFile_h: short file");
+  std::fclose(f);
+}
+void writeWitnessFile_h(uint32_t* samples, const char* filename, unsigned long long nwords) {
+  FILE* f = std::fopen(filename, "wb");
+  if (!f) { dropin_status(CS_ERR_ARG, "writeWitnessFile_h: cannot open file"); return; }
+  const uint64_t n = nwords;
+  const uint32_t wsize = 8, wmore = 0;
+  std::fwrite(&n, 8, 1, f);
+  std::fwrite(&wsize, 4, 1, f);
+  std::fwrite(&wmore, 4, 1, f);
+  std::fwrite(samples, 32, nwords, f);
+  std::fclose(f);
+}
+
+}  // extern "C"

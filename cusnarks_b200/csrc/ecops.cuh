@@ -14,4 +14,17 @@ cudaError_t scmul_g1(const uint32_t* d_scalars, const uint32_t* d_points,
 cudaError_t scmul_g2(const uint32_t* d_scalars, const uint32_t* d_points,
                      uint32_t point_stride_words, uint32_t n, uint32_t* d_out, cudaStream_t st);
 
+// Point utilities behind the reference's ec_jac2aff_h / ec_jacaddreduce_h / ec_isoncurve_h
+// (src/cuda/ec.cpp:963, :1266, :1064): Jacobian rows (3 coordinates) <-> affine rows (2),
+// the sum of n rows (dims 2 or 3) as one affine point, and a curve check (2 infinity,
+// 1 on the curve, 0 not).
+cudaError_t jac_to_affine_g1(const uint32_t* jac, uint32_t n, uint32_t* aff, cudaStream_t st);
+cudaError_t jac_to_affine_g2(const uint32_t* jac, uint32_t n, uint32_t* aff, cudaStream_t st);
+cudaError_t affine_to_jac_g1(const uint32_t* aff, uint32_t n, uint32_t* jac, cudaStream_t st);
+cudaError_t affine_to_jac_g2(const uint32_t* aff, uint32_t n, uint32_t* jac, cudaStream_t st);
+cudaError_t point_sum_g1(const uint32_t* pts, uint32_t n, int dims, uint32_t* out, cudaStream_t st);
+cudaError_t point_sum_g2(const uint32_t* pts, uint32_t n, int dims, uint32_t* out, cudaStream_t st);
+cudaError_t on_curve_g1(const uint32_t* p, int jac, uint32_t* flag, cudaStream_t st);
+cudaError_t on_curve_g2(const uint32_t* p, int jac, uint32_t* flag, cudaStream_t st);
+
 }  // namespace csb

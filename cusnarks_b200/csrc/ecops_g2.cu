@@ -6,4 +6,16 @@ cudaError_t scmul_g2(const uint32_t* s, const uint32_t* p, uint32_t stride, uint
                      cudaStream_t st) {
   return ecops_detail::scmul<Fq2>(s, p, stride, n, out, st);
 }
+cudaError_t jac_to_affine_g2(const uint32_t* jac, uint32_t n, uint32_t* aff, cudaStream_t st) {
+  return ecops_detail::jac_to_affine<Fq2>(jac, n, aff, st);
+}
+cudaError_t affine_to_jac_g2(const uint32_t* aff, uint32_t n, uint32_t* jac, cudaStream_t st) {
+  return ecops_detail::affine_to_jac<Fq2>(aff, n, jac, st);
+}
+cudaError_t point_sum_g2(const uint32_t* pts, uint32_t n, int dims, uint32_t* out, cudaStream_t st) {
+  return ecops_detail::point_sum<Fq2>(pts, n, dims, out, st);
+}
+cudaError_t on_curve_g2(const uint32_t* p, int jac, uint32_t* flag, cudaStream_t st) {
+  return ecops_detail::on_curve<Fq2>(p, jac, flag, st);
+}
 }  // namespace csb

@@ -273,6 +273,57 @@ int cs_ntt_device(cs_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uint32_t l
 int cs_hstep_device(cs_ctx *ctx, int variant, const uint32_t *d_A, const uint32_t *d_B,
                     const uint32_t *d_C, uint32_t log_m, uint32_t *d_out);
 
+/* ----------------------------------------- remaining host functions of the binding --- */
+/* The rest of the reference's host functions that src/cython/_utils_host.pxd binds and
+ * the prover calls.  Point rows: Montgomery, G1 Jacobian 3 x 8 words / affine 2 x 8, G2
+ * 3 x 16 / 2 x 16, infinity (0, 1, 0) / (0, 1); pidx must be 0 (MOD_GROUP).  The point
+ * routines run on the GPU (default context of the current device); Jacobian results come
+ * back normalised (Z = 1): the same points as the reference's.  Status: cs_last_status(). */
+/* ec.cpp:963 -- Jacobian -> affine rows (strip_last: 2 coordinates, else x, y, 1). */
+void ec_jac2aff_h(uint32_t *y, uint32_t *x, uint32_t n, uint32_t pidx, uint32_t strip_last);
+void ec2_jac2aff_h(uint32_t *y, uint32_t *x, uint32_t n, uint32_t pidx, uint32_t strip_last);
+/* ec.cpp:1266 -- sum of n rows (add_in: affine rows of 2, else Jacobian rows of 3). */
+void ec_jacaddreduce_h(uint32_t *z, uint32_t *x, uint32_t n, uint32_t pidx, uint32_t to_aff, uint32_t add_in,
+                       uint32_t strip_last);
+void ec2_jacaddreduce_h(uint32_t *z, uint32_t *x, uint32_t n, uint32_t pidx, uint32_t to_aff, uint32_t add_in,
+                        uint32_t strip_last);
+/* ec.cpp:833 / :819 -- z[i] = scl[i] * P_i (bases Jacobian, or affine with add_last);
+ * sc1mul: x = n scalars followed by one base.  Jacobian rows out. */
+void ec_jacscmul_h(uint32_t *z, uint32_t *scl, uint32_t *x, uint32_t n, uint32_t pidx, uint32_t add_last);
+void ec2_jacscmul_h(uint32_t *z, uint32_t *scl, uint32_t *x, uint32_t n, uint32_t pidx, uint32_t add_last);
+void ec_jacsc1mul_h(uint32_t *z, uint32_t *x, uint32_t n, uint32_t pidx, uint32_t add_last);
+void ec2_jacsc1mul_h(uint32_t *z, uint32_t *x, uint32_t n, uint32_t pidx, uint32_t add_last);
+/* ec.cpp:1064 -- 2: the infinity encoding (X = 0, Y = 1), 1: on the curve, 0: not. */
+uint32_t ec_isoncurve_h(uint32_t *x, uint32_t is_affine, uint32_t pidx);
+uint32_t ec2_isoncurve_h(uint32_t *x, uint32_t is_affine, uint32_t pidx);
+/* bigint.cpp:72 -- indices 0..len-1, sorted (std::sort) by the top word of v[i] if sort_en. */
+void sortu256_idx_h(uint32_t *idx, const uint32_t *v, uint32_t len, uint32_t sort_en);
+/* ntt.cpp:1116 -- transform decomposition of nsamples (types.h fft_params_t layout). */
+typedef enum { FFT_T_1D = 0, FFT_T_2D, FFT_T_3D, FFT_T_4D, FFT_T_N } fft_t;
+typedef struct {
+  fft_t fft_type;
+  uint32_t fft_N[1 << (FFT_T_N - 1)];
+  uint32_t padding;
+  uint32_t levels;
+} fft_params_t;
+void ntt_build_h(fft_params_t *ntt_params, uint32_t nsamples);
+/* init.cpp:44 / :54 (no roots files are read: twiddles are made on the device), and
+ * utils_host get_nprocs_h. */
+void init_h(void);
+void release_h(void);
+uint32_t get_nprocs_h(void);
+/* file_utils.cpp: raw little-endian words; witness .bin values after a 4-word header
+ * (fmt 1), .dat values from byte 32 (fmt 0). */
+void readU256CircuitFile_h(uint32_t *samples, const char *filename, unsigned long long nwords);
+void readU256PKFile_h(uint32_t *samples, const char *filename, unsigned long long nwords);
+void readU256DataFile_h(uint32_t *samples, const char *filename, uint32_t insize, uint32_t outsize);
+void readU256DataFileFromOffset_h(uint32_t *samples, const char *filename, unsigned long long woffset,
+                                  unsigned long long nwords);
+void writeU256DataFile_h(uint32_t *samples, const char *filename, unsigned long long nwords);
+void appendU256DataFile_h(uint32_t *samples, const char *filename, unsigned long long nwords);
+void readWitnessFile_h(uint32_t *samples, const char *filename, uint32_t fmt, unsigned long long inlen);
+void writeWitnessFile_h(uint32_t *samples, const char *filename, unsigned long long nwords);
+
 /* G1 multi-exponentiation that allocates nothing (no counterpart in the reference).
  * For callers whose device memory is owned by a host framework's pool and who may not
  * call cudaMalloc themselves, or cannot afford its implicit synchronisation on a

@@ -1,0 +1,54 @@
+"""Host routines of the binding (no GPU): sortu256_idx_h and ntt_build_h against the
+reference library's outputs, and the file routines on their documented layouts."""
+import ctypes
+
+import numpy as np
+
+from cusnarks_b200 import lib, pkfile
+
+
+def test_sortu256_idx_matches_reference(golden):
+    g = golden("dropin.npz")
+    v = np.ascontiguousarray(g["sort_v"])
+    idx = np.zeros(v.shape[0], np.uint32)
+    lib().sortu256_idx_h(idx.ctypes.data, v.ctypes.data, v.shape[0], 1)
+    assert np.array_equal(idx, g["sort_idx"])
+    lib().sortu256_idx_h(idx.ctypes.data, v.ctypes.data, v.shape[0], 0)
+    assert np.array_equal(idx, np.arange(v.shape[0]))
+
+
+def test_ntt_build_matches_reference(golden):
+    g = golden("dropin.npz")
+    for ns, want in zip(g["build_sizes"], g["build_params"]):
+        buf = np.zeros(11, np.uint32)
+        lib().ntt_build_h(buf.ctypes.data, int(ns))
+        assert np.array_equal(buf, want), int(ns)
+
+
+def test_file_routines(tmp_path):
+    L = lib()
+    rng = np.random.default_rng(5)
+    data = rng.integers(0, 1 << 32, 64 * 8, dtype=np.uint64).astype(np.uint32)
+    p = str(tmp_path / "d.bin").encode()
+    L.writeU256DataFile_h(data.ctypes.data, p, data.size)
+    L.appendU256DataFile_h(data.ctypes.data, p, 16)
+    got = np.zeros(data.size + 16, np.uint32)
+    L.readU256CircuitFile_h(got.ctypes.data, p, got.size)
+    assert np.array_equal(got, np.concatenate([data, data[:16]]))
+    part = np.zeros(40, np.uint32)
+    L.readU256DataFileFromOffset_h(part.ctypes.data, p, 24, 40)
+    assert np.array_equal(part, data[24:64])
+    every = np.zeros(16 * 8, np.uint32)
+    L.readU256DataFile_h(every.ctypes.data, p, 64, 16)          # every 4th element
+    assert np.array_equal(every.reshape(16, 8), data.reshape(64, 8)[::4])
+    same = np.zeros(64 * 8, np.uint32)
+    L.readU256DataFile_h(same.ctypes.data, p, 64, 64)
+    assert np.array_equal(same, data)
+    w = data.reshape(64, 8)[:10]
+    wp = str(tmp_path / "w.bin").encode()
+    L.writeWitnessFile_h(np.ascontiguousarray(w).ctypes.data, wp, 10)
+    assert np.array_equal(np.fromfile(wp.decode(), dtype="<u4"), pkfile.write_witness_bin(w))
+    back = np.zeros((10, 8), np.uint32)
+    L.readWitnessFile_h(back.ctypes.data, wp, 1, 10)
+    assert np.array_equal(back, w)
+    assert L.get_nprocs_h() >= 1
