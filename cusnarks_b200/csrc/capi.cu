@@ -101,7 +101,7 @@ struct EventScope {
 
 int msm_device_locked(cs_ctx* ctx, int ec2, const uint32_t* s, const uint32_t* p, uint32_t n,
                       uint32_t* out, int window) {
-  const size_t need = csb::msm_workspace_bytes(n, window, ec2 != 0, ctx->msm_affine != 0);
+  const size_t need = csb::msm_workspace_bytes(n, window, ec2 != 0, ctx->msm_affine);
   cudaError_t e = ctx->work.reserve(need, ctx->stream);
   if (e != cudaSuccess) return fail(ctx, e, "msm workspace");
   csb::MsmConfig cfg;
@@ -297,7 +297,7 @@ int cs_msm_fixed_device(cs_ctx* ctx, int ec2, const uint32_t* d_scalars, const u
   if (!ctx || !d_out || window < 4 || window > 24 || (n && (!d_scalars || !d_table))) return CS_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
-  cudaError_t e = ctx->work.reserve(csb::msm_fixed_workspace_bytes(n, window, ec2 != 0), ctx->stream);
+  cudaError_t e = ctx->work.reserve(csb::msm_fixed_workspace_bytes(n, window, ec2 != 0, ctx->msm_affine), ctx->stream);
   if (e != cudaSuccess) return fail(ctx, e, "fixed-base msm workspace");
   csb::MsmConfig cfg;
   cfg.c = window;

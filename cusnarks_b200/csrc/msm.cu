@@ -16,10 +16,11 @@ int msm_default_window(uint32_t n, bool ec2) {
   return best;
 }
 
-size_t msm_workspace_bytes(uint32_t n, int c, bool ec2, bool affine) {
+size_t msm_workspace_bytes(uint32_t n, int c, bool ec2, int affine_mode) {
   if (c <= 0) c = msm_default_window(n, ec2);
   const int xb = ec2 ? 256 : 128;
-  return msm_detail::make_layout(n, c, xb, msm_detail::kMinTask, false, affine).total;
+  return msm_detail::make_layout(n, c, xb, msm_detail::kMinTask, false,
+                                 msm_detail::layout_affine(ec2, affine_mode, n, c, false)).total;
 }
 
 int msm_fixed_window(uint32_t n, bool ec2) {
@@ -45,9 +46,10 @@ size_t msm_fixed_table_work_bytes(uint32_t n, bool ec2) {
   return msm_detail::fixed_table_work_bytes(n, ec2 ? 256 : 128, ec2 ? 64 : 32);
 }
 
-size_t msm_fixed_workspace_bytes(uint32_t n, int c, bool ec2) {
+size_t msm_fixed_workspace_bytes(uint32_t n, int c, bool ec2, int affine_mode) {
   if (c <= 0) c = msm_fixed_window(n, ec2);
-  return msm_detail::make_layout(n, c, ec2 ? 256 : 128, msm_detail::kMinTask, true).total;
+  return msm_detail::make_layout(n, c, ec2 ? 256 : 128, msm_detail::kMinTask, true,
+                                 msm_detail::layout_affine(ec2, affine_mode, n, c, true)).total;
 }
 
 }  // namespace csb

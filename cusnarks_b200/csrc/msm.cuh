@@ -80,7 +80,8 @@ struct MsmConfig {
 };
 
 // Bytes of device scratch one MSM of n terms needs (G2 when ec2).
-size_t msm_workspace_bytes(uint32_t n, int c, bool ec2, bool affine = true);
+// affine_mode: batch-affine rounds the MSM will run (-1 automatic, 0 none, > 0 that many).
+size_t msm_workspace_bytes(uint32_t n, int c, bool ec2, int affine_mode = -1);
 int msm_default_window(uint32_t n, bool ec2);
 
 // d_scalars: n x 8 words (normal form), d_points: n affine points (16 or 32 words),
@@ -99,7 +100,7 @@ cudaError_t msm_g2(const uint32_t* d_scalars, const uint32_t* d_points, uint32_t
 int msm_fixed_window(uint32_t n, bool ec2);
 size_t msm_fixed_table_points(uint32_t n, int c);
 size_t msm_fixed_table_work_bytes(uint32_t n, bool ec2);
-size_t msm_fixed_workspace_bytes(uint32_t n, int c, bool ec2);
+size_t msm_fixed_workspace_bytes(uint32_t n, int c, bool ec2, int affine_mode = -1);
 cudaError_t msm_fixed_table_g1(const uint32_t* d_points, uint32_t n, int c, uint32_t* d_table, void* d_work,
                                size_t work_bytes, cudaStream_t stream);
 cudaError_t msm_fixed_table_g2(const uint32_t* d_points, uint32_t n, int c, uint32_t* d_table, void* d_work,

@@ -744,13 +744,27 @@ inline Layout make_layout(uint32_t n, int c, int xyzz_bytes, uint32_t task_len, 
 // fastest without rounds (its XYZZ addition costs 10 products of 136 wide multiplies and
 // already outruns the gather-bound affine round), G2 with two (Fq2 products are 3 Fq
 // products, so the 6-vs-10 product saving outweighs the extra traffic).
-template <class F>
-inline int auto_affine_rounds(uint32_t n, int W, size_t nb) {
-  const int cap = FieldWords<F>::value == 16 ? 2 : 0;
+inline int auto_affine_rounds_rt(bool ec2, uint32_t n, int W, size_t nb) {
+  // a round runs kAffK pairs per thread in sequence around one inversion: it needs enough
+  // pairs (>= 2^22, i.e. N W >= 2^23 entries) to fill the GPU, or its chain sets the latency
+  // (2 rounds cost 2.5 ms in a 2^12-term G2 MSM)
+  if ((uint64_t)n * W < (1ull << 23)) return 0;
+  const int cap = ec2 ? 2 : 0;
   const double avg = (double)n * W / (double)nb;
   int r = 0;
   while (r < cap && avg >= (double)(8u << r)) r++;
   return r;
+}
+template <class F>
+inline int auto_affine_rounds(uint32_t n, int W, size_t nb) {
+  return auto_affine_rounds_rt(FieldWords<F>::value == 16, n, W, nb);
+}
+// Whether an MSM reserves the round buffers: affine_mode -1 auto, 0 never, > 0 that many rounds.
+inline bool layout_affine(bool ec2, int affine_mode, uint32_t n, int c, bool fixed) {
+  if (affine_mode >= 0) return affine_mode > 0;
+  const int W = num_windows(c);
+  const size_t nb = fixed ? ((size_t)1 << (c - 1)) : (size_t)W << (c - 1);
+  return auto_affine_rounds_rt(ec2, n, W, nb) > 0;
 }
 
 template <class F>
@@ -785,10 +799,11 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   if (task_len < kMinTask) task_len = kMinTask;
   if (task_len > (uint32_t)kMaxTask) task_len = kMaxTask;
   const int W = num_windows(c);
-  if (FIXED && (uint64_t)W * n >= (uint64_t)NEG_BIT) return cudaErrorInvalidValue;
+  // entry positions are uint32 and fixed-base entries carry a table index below the sign bit
+  if ((uint64_t)W * n >= (uint64_t)NEG_BIT) return cudaErrorInvalidValue;
   const uint32_t nb = FIXED ? (1u << (c - 1)) : (uint32_t)W << (c - 1);
   const int rounds_req = cfg.affine < 0 ? auto_affine_rounds<F>(n, W, nb) : cfg.affine;
-  const Layout L = make_layout(n, c, XB, kMinTask, FIXED, cfg.affine != 0);
+  const Layout L = make_layout(n, c, XB, kMinTask, FIXED, layout_affine(EC2, cfg.affine, n, c, FIXED));
   if (work_bytes < L.total || d_work == nullptr) return cudaErrorInvalidValue;
   char* base = static_cast<char*>(d_work);
   uint32_t* counters = reinterpret_cast<uint32_t*>(base + L.counters);
