@@ -62,6 +62,26 @@ def test_prove_matches_cpu_and_verifies(ctx, oracle, log_m, seed):
     prover.close(); prover2.close()
 
 
+@pytest.mark.parametrize("log_m,n_public,seed", [(3, 1, 71), (4, 2, 72), (7, 3, 73), (8, 5, 74)])
+def test_prove_public_inputs_and_tiny_domains(ctx, oracle, log_m, n_public, seed):
+    """Several public inputs (the extra rows polsA gets) and domains down to 8 points: byte
+    equal to the CPU sequence, verifies, and a changed public input fails."""
+    from cusnarks_b200.groth import SyntheticCircuit, setup_pk, pk_to_host, Prover
+    circ = SyntheticCircuit(ctx, log_m, seed=seed, n_public=n_public)
+    pk = setup_pk(ctx, circ, seed=seed + 1)
+    host = pk_to_host(pk)
+    r, s = (seed * 1000003) % R, (seed * 999983 + 7) % R
+    for fixed in (0, -1):
+        prover = Prover(ctx, pk, fixed_base=fixed)
+        proof = prover.prove(circ.w, ints_to_limbs([r])[0], ints_to_limbs([s])[0])
+        prover.close()
+        assert np.array_equal(proof, cpu_prove(oracle, host, circ.w, r, s)), fixed
+    assert verify(host["vk"], proof, circ.public_inputs)
+    bad = circ.public_inputs.copy()
+    bad[-1, 0] ^= 1
+    assert not verify(host["vk"], proof, bad)
+
+
 def test_plain_per_call_path_matches(ctx):
     """The reference's flow through the drop-in entry points (one host-memory call per
     step, key re-sent per MSM) gives the resident prover's proof byte for byte."""
