@@ -419,7 +419,11 @@ using Fr = Fp<ModR>;
 // ------------------------------------------------------------ Fq2 = Fq[u]/(u^2+1) ----
 template <class M>
 __device__ __noinline__ Fp<M> fp_mul_call(Fp<M> a, Fp<M> b) {
+#ifdef CSB_MUL_CALL_LOHI
+  return Fp<M>::mul_lohi(a, b);
+#else
   return Fp<M>::mul_wide(a, b);
+#endif
 }
 
 struct Fq2 {

@@ -100,22 +100,131 @@ __global__ void k_neg_rs(const uint32_t* __restrict__ r, const uint32_t* __restr
   st_fp<ModR>(dst, Fr::zero() - rm * ld_fp<ModR>(s));
 }
 
-// out (XYZZ) = k * P (affine), left-to-right double-and-add over 256 bits
-template <class F>
-__global__ void k_scale_point(const uint32_t* __restrict__ P, const uint32_t* __restrict__ k,
-                              uint32_t* __restrict__ out) {
-  if (threadIdx.x != 0) return;
-  uint32_t kk[8];
-  for (int i = 0; i < 8; i++) kk[i] = k[i];
-  const Affine<F> p = ld_affine<F>(P);
-  XYZZ<F> acc = XYZZ<F>::inf();
-  if (!affine_is_inf(p)) {
-    for (int b = 255; b >= 0; b--) {
-      acc = xyzz_dbl_cold(acc);
-      if ((kk[b >> 5] >> (b & 31)) & 1u) acc = xyzz_add_cold(acc, XYZZ<F>::from_affine(p));
+// ---- k * P through the GLV endomorphism of BN254 G1: phi(x, y) = (beta x, y) = lambda P
+// with beta^3 = 1 in Fq and lambda^2 + lambda + 1 = 0 in Fr.  k = k1 + k2 lambda (mod r) with
+// |k1|, |k2| < 2^127 from the short lattice basis (a1, b1), (a2, b2) of
+// {(x, y) : x + y lambda = 0 mod r} (extended Euclid on (r, lambda); b2 = a1, b1 < 0):
+//   c1 = round(b2 k / r), c2 = round(-b1 k / r) (as (k g1) >> 256, (k g2) >> 256),
+//   k1 = k - c1 a1 - c2 a2,  k2 = c1 |b1| - c2 b2.
+// Then k P = k1 P + k2 phi(P): 127 joint doublings instead of 254.
+struct GlvSplit {
+  uint32_t k1[4], k2[4];  // magnitudes, little-endian
+  uint32_t neg1, neg2, pad[6];
+};
+
+namespace glv {
+constexpr uint64_t G1C[2] = {0xd91d232ec7e0b3d7ull, 0x2ull};
+constexpr uint64_t G2C[3] = {0x7a7bd9d4391eb18eull, 0x4ccef014a773d2cfull, 0x2ull};
+constexpr uint64_t A1 = 0x89d3256894d213e3ull;                                  // = b2
+constexpr uint64_t A2[2] = {0x0be4e1541221250bull, 0x6f4d8248eeb859fdull};
+constexpr uint64_t B1ABS[2] = {0x8211bbeb7d4f1128ull, 0x6f4d8248eeb859fcull};
+
+typedef unsigned __int128 u128;
+
+// r = a * b for little-endian 64-bit limb vectors, into an na + nb limb result
+inline void mul(const uint64_t* a, int na, const uint64_t* b, int nb, uint64_t* r) {
+  for (int i = 0; i < na + nb; i++) r[i] = 0;
+  for (int i = 0; i < na; i++) {
+    u128 c = 0;
+    for (int j = 0; j < nb; j++) {
+      c += (u128)a[i] * b[j] + r[i + j];
+      r[i + j] = (uint64_t)c;
+      c >>= 64;
+    }
+    r[i + nb] = (uint64_t)c;
+  }
+}
+// acc (4 limbs, mod 2^256) += sign * v (up to 4 limbs)
+inline void addsub(uint64_t* acc, const uint64_t* v, int nv, bool sub) {
+  u128 c = sub ? 1 : 0;  // two's complement: acc + ~v + 1
+  for (int i = 0; i < 4; i++) {
+    const uint64_t w = i < nv ? v[i] : 0;
+    c += (u128)acc[i] + (sub ? ~w : w);
+    acc[i] = (uint64_t)c;
+    c >>= 64;
+  }
+}
+inline void to_mag(const uint64_t* v, uint32_t* mag, uint32_t* neg) {
+  uint64_t t[4] = {v[0], v[1], v[2], v[3]};
+  *neg = (t[3] >> 63) ? 1u : 0u;
+  if (*neg) {  // negate
+    u128 c = 1;
+    for (int i = 0; i < 4; i++) {
+      c += (u128)(~t[i]);
+      t[i] = (uint64_t)c;
+      c >>= 64;
     }
   }
-  st_xyzz<F>(out, acc);
+  for (int i = 0; i < 2; i++) {  // |k1|, |k2| < 2^127
+    mag[2 * i] = (uint32_t)t[i];
+    mag[2 * i + 1] = (uint32_t)(t[i] >> 32);
+  }
+}
+
+// k mod r for any 256-bit k (at most 5 subtractions)
+inline void reduce_r(uint64_t* k) {
+  static constexpr uint64_t R[4] = {0x43e1f593f0000001ull, 0x2833e84879b97091ull, 0xb85045b68181585dull,
+                                    0x30644e72e131a029ull};
+  for (int it = 0; it < 6; it++) {
+    bool ge = true;
+    for (int i = 3; i >= 0; i--) {
+      if (k[i] != R[i]) { ge = k[i] > R[i]; break; }
+    }
+    if (!ge) return;
+    addsub(k, R, 4, true);
+  }
+}
+
+inline GlvSplit split(const uint32_t* k32) {
+  uint64_t k[4];
+  for (int i = 0; i < 4; i++) k[i] = (uint64_t)k32[2 * i] | ((uint64_t)k32[2 * i + 1] << 32);
+  reduce_r(k);
+  uint64_t p1[6], p2[7];
+  mul(k, 4, G1C, 2, p1);
+  mul(k, 4, G2C, 3, p2);
+  const uint64_t c1[1] = {p1[4]};            // < 2^64
+  const uint64_t c2[2] = {p2[4], p2[5]};     // < 2^128
+  uint64_t t[4];
+  uint64_t k1[4] = {k[0], k[1], k[2], k[3]}, k2[4] = {0, 0, 0, 0};
+  mul(c1, 1, &A1, 1, t);                     // c1 a1 (2 limbs)
+  addsub(k1, t, 2, true);
+  uint64_t t4[4];
+  mul(c2, 2, A2, 2, t4);                     // c2 a2
+  addsub(k1, t4, 4, true);
+  mul(c1, 1, B1ABS, 2, t);                   // c1 |b1| (3 limbs)
+  addsub(k2, t, 3, false);
+  mul(c2, 2, &A1, 1, t);                     // c2 b2, b2 = a1 (3 limbs)
+  addsub(k2, t, 3, true);
+  GlvSplit g{};
+  to_mag(k1, g.k1, &g.neg1);
+  to_mag(k2, g.k2, &g.neg2);
+  return g;
+}
+}  // namespace glv
+
+// out (XYZZ) = k * P for P affine (G1), k given as its GLV split.
+__global__ void k_scale_point_glv(const uint32_t* __restrict__ P, const GlvSplit* __restrict__ gs,
+                                  uint32_t* __restrict__ out) {
+  if (threadIdx.x != 0) return;
+  const Fq beta{{0xd782e155u, 0x71930c11u, 0xffbe3323u, 0xa6bb947cu, 0xd4741444u, 0xaa303344u, 0x26594943u,
+                 0x2c3b3f0du}};
+  const GlvSplit g = *gs;
+  Affine<Fq> p = ld_affine<Fq>(P);
+  XYZZ<Fq> acc = XYZZ<Fq>::inf();
+  if (!affine_is_inf(p)) {
+    Affine<Fq> q{p.x * beta, p.y};  // phi(P) = lambda P
+    if (g.neg1) p.y = p.y.neg();
+    if (g.neg2) q.y = q.y.neg();
+    const XYZZ<Fq> pq = xyzz_madd(XYZZ<Fq>::from_affine(p), q);  // P + phi(P) (never infinity)
+    for (int b = 127; b >= 0; b--) {
+      acc = xyzz_dbl_cold(acc);
+      const uint32_t e1 = (g.k1[b >> 5] >> (b & 31)) & 1u, e2 = (g.k2[b >> 5] >> (b & 31)) & 1u;
+      if (e1 && e2) acc = xyzz_add_cold(acc, pq);
+      else if (e1) acc = xyzz_add_cold(acc, XYZZ<Fq>::from_affine(p));
+      else if (e2) acc = xyzz_add_cold(acc, XYZZ<Fq>::from_affine(q));
+    }
+  }
+  st_xyzz<Fq>(out, acc);
 }
 
 // pi_C = C2 + C + sA + rB1 (C2, C affine; sA, rB1 XYZZ) -> affine
@@ -179,7 +288,7 @@ ProvePlan plan_prove(const cs_pk* pk) {
   P.ms_c = o; o += al256(P.bytes_c);
   P.ms_h = o; o += al256(P.bytes_h);
   P.pts = o; o += 2048;   // outA 64, outB1 64, outB2 128, outC 64, outH 64, sA 128, rB1 128, piC 64
-  P.rs = o; o += 256;     // r, s, -rs
+  P.rs = o; o += 256;     // r, s, -rs, then the GLV splits of s and r (2 x 64 B)
   P.total = o;
   return P;
 }
@@ -349,10 +458,12 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
   if ((e = domain_get(ctx, pk->log_m + 1, &dom2)) != cudaSuccess || (e = domain_get(ctx, pk->log_m, &dom1)) != cudaSuccess)
     return fail(ctx, e, "prove tables");
   MsmConfig cfg;
+  const GlvSplit glv_rs[2] = {glv::split(s), glv::split(r)};  // s * pi_A, r * pi_B1
   cudaEventRecord(ctx->ev_start, s0);
   // scalars: w ++ [1, r] and w ++ [1, s]; r, s, -rs
   bool ok = (e = cudaMemcpyAsync(rs, r, 32, cudaMemcpyHostToDevice, s0)) == cudaSuccess &&
             (e = cudaMemcpyAsync(rs + 8, s, 32, cudaMemcpyHostToDevice, s0)) == cudaSuccess &&
+            (e = cudaMemcpyAsync(rs + 32, glv_rs, sizeof(glv_rs), cudaMemcpyHostToDevice, s0)) == cudaSuccess &&
             (e = cudaMemcpyAsync(wA, d_w, (size_t)nv * 32, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess &&
             (e = cudaMemcpyAsync(wB, d_w, (size_t)nv * 32, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess;
   if (!ok) return fail(ctx, e, "prove inputs");
@@ -381,8 +492,11 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
        (e = run_msm(false, wA + (size_t)np1 * 8, pk->c + (size_t)np1 * 16, pk->fc, nv - np1, outC, P.ms_c, P.bytes_c,
                     sc)) == cudaSuccess;
   if (!ok) return fail(ctx, e, "prove witness MSMs");
-  k_scale_point<Fq><<<1, 32, 0, sa>>>(outA, rs + 8, sA);   // s * pi_A
-  k_scale_point<Fq><<<1, 32, 0, sb1>>>(outB1, rs, rB1);    // r * pi_B1
+  {
+    const GlvSplit* gsp = reinterpret_cast<const GlvSplit*>(rs + 32);
+    k_scale_point_glv<<<1, 32, 0, sa>>>(outA, gsp, sA);        // s * pi_A
+    k_scale_point_glv<<<1, 32, 0, sb1>>>(outB1, gsp + 1, rB1);  // r * pi_B1
+  }
   note_launch(2);
   // QAP evaluation, H step and H MSM on their own stream
   cudaStream_t sh = ctx->aux_h;
