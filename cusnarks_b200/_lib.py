@@ -19,6 +19,7 @@ CS_ERR_NOMEM = 3
 CS_ERR_UNSUPPORTED = 4
 CS_ERR_NODEVICE = 5
 CS_ERR_TIMEOUT = 6
+CS_ERR_CANCELLED = 7
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _vp = ctypes.c_void_p
@@ -41,8 +42,10 @@ class ServerResult(ctypes.Structure):
 
 class ServerStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
-                ("queued", ctypes.c_uint64), ("running", ctypes.c_uint32), ("max_concurrent", ctypes.c_uint32),
-                ("promised_bytes", ctypes.c_size_t)]
+                ("cancelled", ctypes.c_uint64), ("queued", ctypes.c_uint64), ("running", ctypes.c_uint32),
+                ("max_concurrent", ctypes.c_uint32), ("promised_bytes", ctypes.c_size_t),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("hbm_free_bytes", ctypes.c_size_t), ("hbm_total_bytes", ctypes.c_size_t)]
 
 
 class MpolyEval(ctypes.Structure):
@@ -155,6 +158,8 @@ _SIGNATURES = [
     ("cs_server_wait", ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(ServerResult)]),
     ("cs_server_stats", ctypes.c_int, [_vp, ctypes.POINTER(ServerStats)]),
     ("cs_server_error", ctypes.c_char_p, [_vp]),
+    ("cs_server_cancel", ctypes.c_int, [_vp, ctypes.c_uint64]),
+    ("cs_debug_fail_allocs", None, [ctypes.c_int]),
     ("cs_setup_lagrange", ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp]),
     ("cs_setup_wire_eval", ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32, _vp]),
     ("cs_setup_c_scalars", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_uint32, _vp]),

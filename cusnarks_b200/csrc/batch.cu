@@ -170,6 +170,7 @@ int cs_msm_batch_window(const cs_msm_batch* b, uint32_t i) {
 
 int cs_msm_batch_run(cs_ctx* ctx, cs_msm_batch* b, int use_graph) {
   if (!ctx || !b) return CS_ERR_ARG;
+  csb::NvtxRange nvtx(use_graph ? "msm_batch_graph" : "msm_batch");
   if (b->device != ctx->device) return CS_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);

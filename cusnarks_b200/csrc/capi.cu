@@ -101,6 +101,7 @@ struct EventScope {
 
 int msm_device_locked(cs_ctx* ctx, int ec2, const uint32_t* s, const uint32_t* p, uint32_t n,
                       uint32_t* out, int window) {
+  csb::NvtxRange nvtx(ec2 ? "msm_g2" : "msm_g1");
   const size_t need = csb::msm_workspace_bytes(n, window, ec2 != 0, ctx->msm_affine);
   cudaError_t e = ctx->work.reserve(need, ctx->stream);
   if (e != cudaSuccess) return fail(ctx, e, "msm workspace");
@@ -121,6 +122,14 @@ int msm_device_locked(cs_ctx* ctx, int ec2, const uint32_t* s, const uint32_t* p
 }  // namespace
 
 namespace csb {
+std::atomic<int> g_fail_allocs{0};
+bool debug_take_alloc_failure() {
+  int v = g_fail_allocs.load();
+  while (v > 0) {
+    if (g_fail_allocs.compare_exchange_weak(v, v - 1)) return true;
+  }
+  return false;
+}
 // Default context of the current device for the drop-in entry points (created on first use);
 // *status and the thread's cs_last_error describe a failure.
 cs_ctx* dropin_ctx(int* status) { return default_ctx(status); }
@@ -207,6 +216,8 @@ int cs_ctx_sync(cs_ctx* ctx) {
   cudaGetLastError();
   return CS_OK;
 }
+
+void cs_debug_fail_allocs(int count) { csb::g_fail_allocs.store(count > 0 ? count : 0); }
 
 int cs_ctx_set_msm_affine_rounds(cs_ctx* ctx, int rounds) {
   if (!ctx || rounds < -1 || rounds > 6) return CS_ERR_ARG;

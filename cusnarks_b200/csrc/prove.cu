@@ -438,6 +438,7 @@ size_t cs_prove_workspace_bytes(const cs_pk* pk) { return pk ? plan_prove(pk).to
 int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t* r, const uint32_t* s,
                     uint32_t* d_proof) {
   if (!ctx || !pk || !d_w || !r || !s || !d_proof) return CS_ERR_ARG;
+  NvtxRange nvtx("cs_prove");
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
   cudaError_t e = ctx_aux_init(ctx);

@@ -8,7 +8,21 @@
 #include <mutex>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>  // header-only; ranges cost nothing unless a profiler is attached
+
 namespace csb {
+
+// Named host range around the enqueueing of a library call (nsys / ncu --nvtx).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
+// Test hook (cs_debug_fail_allocs): while positive, arena growth fails as if the device
+// were out of memory, one failure per call.
+bool debug_take_alloc_failure();
 
 // Grow-only device buffer (256-byte aligned).  Growing synchronises the owning stream
 // first so no in-flight kernel still uses the old block.
@@ -25,6 +39,7 @@ struct DeviceBuffer {
       bytes = 0;
     }
     size_t sz = need + need / 8;  // headroom for slightly larger calls
+    if (debug_take_alloc_failure()) return cudaErrorMemoryAllocation;
     cudaError_t e = cudaMalloc(&ptr, sz);
     if (e != cudaSuccess) { ptr = nullptr; return e; }
     bytes = sz;

@@ -13,6 +13,7 @@
 //     H step overlap the next one's bucket accumulation.
 // Results do not depend on the mix: every proof is computed by the same kernels on its
 // own slot scratch (a test compares proofs made alone and in a mix, byte for byte).
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -34,6 +35,8 @@ uint32_t pk_n_vars(const cs_pk* pk);
 }  // namespace csb
 
 namespace {
+
+constexpr size_t kLatRing = 1024;
 
 double now_ms() {
   using namespace std::chrono;
@@ -71,7 +74,9 @@ struct cs_server {
   int busy = 0;
   size_t promised = 0;  // scratch growth admitted but not yet allocated
   // statistics
-  uint64_t completed = 0, failed = 0, rejected = 0;
+  uint64_t completed = 0, failed = 0, rejected = 0, cancelled = 0;
+  std::vector<double> lat_ring;  // latencies (ms) of the last kLatRing completed proofs
+  size_t lat_next = 0;
   int max_concurrent = 0;
   double busy_since = 0, first_start = -1, last_end = 0;
   std::string err;
@@ -166,7 +171,15 @@ void cs_server::worker(int slot) {
       rq->t_end = now_ms();
       rq->done = true;
       last_end = rq->t_end;
-      if (st == CS_OK) completed++; else failed++;
+      if (st == CS_OK) {
+        completed++;
+        const double lat = rq->t_end - rq->t_submit;
+        if (lat_ring.size() < kLatRing) lat_ring.push_back(lat);
+        else lat_ring[lat_next] = lat;
+        lat_next = (lat_next + 1) % kLatRing;
+      } else {
+        failed++;
+      }
     }
     cv_done.notify_all();
     cv_work.notify_all();
@@ -271,15 +284,51 @@ int cs_server_wait(cs_server* s, uint64_t ticket, double timeout_s, cs_server_re
 
 int cs_server_stats(cs_server* s, cs_server_counters* st) {
   if (!s || !st) return CS_ERR_ARG;
-  std::lock_guard<std::mutex> lk(s->mu);
-  st->completed = s->completed;
-  st->failed = s->failed;
-  st->rejected = s->rejected;
-  st->queued = s->queue.size();
-  st->running = (uint32_t)s->busy;
-  st->max_concurrent = (uint32_t)s->max_concurrent;
-  st->promised_bytes = s->promised;
+  std::vector<double> lat;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    st->completed = s->completed;
+    st->failed = s->failed;
+    st->rejected = s->rejected;
+    st->cancelled = s->cancelled;
+    st->queued = s->queue.size();
+    st->running = (uint32_t)s->busy;
+    st->max_concurrent = (uint32_t)s->max_concurrent;
+    st->promised_bytes = s->promised;
+    lat = s->lat_ring;
+  }
+  st->p50_ms = st->p99_ms = 0.0;
+  if (!lat.empty()) {
+    std::sort(lat.begin(), lat.end());
+    st->p50_ms = lat[(size_t)(0.50 * (lat.size() - 1) + 0.5)];
+    st->p99_ms = lat[(size_t)(0.99 * (lat.size() - 1) + 0.5)];
+  }
+  size_t free_b = 0, total_b = 0;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(s->device);
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) cudaGetLastError();
+  cudaSetDevice(prev);
+  st->hbm_free_bytes = free_b;
+  st->hbm_total_bytes = total_b;
   return CS_OK;
+}
+
+int cs_server_cancel(cs_server* s, uint64_t ticket) {
+  if (!s) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (auto it = s->queue.begin(); it != s->queue.end(); ++it) {
+    if ((*it)->id == ticket) {
+      (*it)->status = CS_ERR_CANCELLED;
+      (*it)->err = "cancelled before it ran";
+      (*it)->done = true;
+      s->queue.erase(it);
+      s->cancelled++;
+      s->cv_done.notify_all();
+      return CS_OK;
+    }
+  }
+  return CS_ERR_ARG;  // unknown, running or finished: not cancellable
 }
 
 const char* cs_server_error(cs_server* s) { return s ? s->err.c_str() : "null server"; }

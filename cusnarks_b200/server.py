@@ -59,6 +59,10 @@ class ProveServer:
             raise CsError(st, msg.decode() if msg else "prove failed")
         return proof, {"queue_ms": res.queue_ms, "latency_ms": res.latency_ms, "device_ms": res.device_ms}
 
+    def cancel(self, ticket: int) -> bool:
+        """Removes a still-queued request; its wait() then raises CsError(CS_ERR_CANCELLED)."""
+        return lib().cs_server_cancel(self.handle, ticket) == CS_OK
+
     def stats(self) -> dict:
         s = ServerStats()
         lib().cs_server_stats(self.handle, ctypes.byref(s))

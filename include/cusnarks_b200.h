@@ -37,6 +37,7 @@ extern "C" {
 #define CS_ERR_UNSUPPORTED 4 /* option the GPU path does not implement */
 #define CS_ERR_NODEVICE 5    /* no CUDA device */
 #define CS_ERR_TIMEOUT 6     /* a wait ran out of time (the request is still pending) */
+#define CS_ERR_CANCELLED 7   /* the request was cancelled before it ran */
 
 /* ------------------------------------------- reference argument structs (layouts) --- */
 /* jacadd_reduced_t, reference src/cuda/types.h:548-567 (same member order and types). */
@@ -174,6 +175,9 @@ float cs_ctx_last_phase_ms(cs_ctx *ctx);
  * cs_msm / cs_msm_device / cs_msm_fixed_device calls: -1 automatic (default), 0 none, 1..6.
  * Results do not depend on it. */
 int cs_ctx_set_msm_affine_rounds(cs_ctx *ctx, int rounds);
+/* Test hook: the next `count` growths of any context's device arenas fail as if the device
+ * were out of memory (the call reports CS_ERR_NOMEM and the context stays usable). */
+void cs_debug_fail_allocs(int count);
 
 /* Multi-exponentiation with host pointers: copies in, computes, copies the affine result
  * out, synchronises.  ec2 selects G2.  window = Pippenger window bits (0 = automatic). */
@@ -402,10 +406,12 @@ typedef struct {
   float device_ms;    /* device time of the prove kernels (CUDA events) */
 } cs_server_result;
 typedef struct {
-  uint64_t completed, failed, rejected;
+  uint64_t completed, failed, rejected, cancelled;
   uint64_t queued;
   uint32_t running, max_concurrent;
   size_t promised_bytes;
+  double p50_ms, p99_ms;            /* latency (submit -> done) over the last 1024 proofs */
+  size_t hbm_free_bytes, hbm_total_bytes;
 } cs_server_counters;
 int cs_server_create(int device, int slots, size_t reserve_bytes, cs_server **out);
 void cs_server_destroy(cs_server *srv);
@@ -414,6 +420,9 @@ int cs_server_submit(cs_server *srv, int key_id, const uint32_t *w, const uint32
                      uint32_t *proof, uint64_t *ticket);
 int cs_server_wait(cs_server *srv, uint64_t ticket, double timeout_s, cs_server_result *res);
 int cs_server_stats(cs_server *srv, cs_server_counters *st);
+/* Removes a request that is still queued (its wait returns CS_ERR_CANCELLED); CS_ERR_ARG when
+ * the request is unknown, already running or finished. */
+int cs_server_cancel(cs_server *srv, uint64_t ticket);
 const char *cs_server_error(cs_server *srv);
 
 /* ------------------------------------------- proving-key generation (setup) -------- */

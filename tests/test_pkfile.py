@@ -80,3 +80,16 @@ def test_proof_json_normal_form():
     assert j["pi_a"] == [str(G1_GEN[0]), str(G1_GEN[1]), "1"] == j["pi_c"]
     assert j["pi_b"] == [[str(G2_GEN[0][0]), str(G2_GEN[0][1])], [str(G2_GEN[1][0]), str(G2_GEN[1][1])], ["1", "0"]]
     assert j["protocol"] == "groth"
+
+
+def test_truncated_files_are_rejected(golden, tmp_path):
+    g = _inputs(golden)
+    import pytest
+    with pytest.raises(ValueError):
+        pkfile.read_pk_bin(g["pk_bin"][:200])           # header only
+    with pytest.raises(ValueError):
+        pkfile.read_pk_bin(g["pk_bin"][:-500])          # points cut off
+    p = tmp_path / "w.bin"
+    g["witness_bin"][:40].astype("<u4").tofile(p)
+    with pytest.raises(ValueError):
+        pkfile.read_witness(p, int(g["n_vars"]))
