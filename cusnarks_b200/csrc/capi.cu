@@ -34,7 +34,7 @@ cudaError_t ctx_aux_init(cs_ctx* ctx) {
     if (!ctx->aux[i]) e = cudaStreamCreateWithPriority(&ctx->aux[i], cudaStreamNonBlocking, prio[i]);
   if (e == cudaSuccess && !ctx->aux_h) e = cudaStreamCreateWithPriority(&ctx->aux_h, cudaStreamNonBlocking, prio_h);
   for (int i = 0; i < 8 && e == cudaSuccess; i++)
-    if (!ctx->aux_ev[i]) e = cudaEventCreateWithFlags(&ctx->aux_ev[i], cudaEventDisableTiming);
+    if (!ctx->aux_ev[i]) e = cudaEventCreate(&ctx->aux_ev[i]);  // timed: prove stage times
   if (e == cudaSuccess) ctx->aux_ready = true;
   return e;
 }
@@ -223,6 +223,24 @@ int cs_ctx_set_msm_affine_rounds(cs_ctx* ctx, int rounds) {
   if (!ctx || rounds < -1 || rounds > 6) return CS_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->msm_affine = rounds;
+  return CS_OK;
+}
+
+int cs_ctx_prove_stages(cs_ctx* ctx, float* ms, int n) {
+  if (!ctx || !ms || n < 1) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!ctx->aux_ready) return CS_ERR_ARG;
+  // completion of: A, B1, B2, C MSM chains, the H step, the H MSM, the whole proof
+  cudaEvent_t evs[7] = {ctx->aux_ev[1], ctx->aux_ev[2], ctx->aux_ev[3], ctx->aux_ev[4], ctx->aux_ev[6],
+                        ctx->aux_ev[5], ctx->ev_stop};
+  for (int i = 0; i < n && i < 7; i++) {
+    float t = -1.f;
+    if (cudaEventElapsedTime(&t, ctx->ev_start, evs[i]) != cudaSuccess) {
+      cudaGetLastError();
+      t = -1.f;
+    }
+    ms[i] = t;
+  }
   return CS_OK;
 }
 

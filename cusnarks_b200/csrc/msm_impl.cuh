@@ -558,7 +558,10 @@ __global__ void k_store_inf(uint32_t* out) {
 // 10 of an XYZZ + affine addition.  Round r maps bucket b's c_b points at in_off[b] to
 // ceil(c_b / 2) points at out_off[b]; an odd last point is copied.  Points at infinity
 // inside the rounds are (0, 0), which is on neither curve.
-constexpr uint32_t kAffK = 64;
+#ifndef CSB_AFF_K
+#define CSB_AFF_K 64
+#endif
+constexpr uint32_t kAffK = CSB_AFF_K;
 
 template <class F>
 CSB_DEV bool aff_zero(const Affine<F>& a) { return a.x.is_zero() && a.y.is_zero(); }

@@ -506,6 +506,7 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
        (e = qap_eval(pk->rows_b, d_w, pB, 0, sh)) == cudaSuccess &&
        (e = hstep_reference_core(pA, pB, pk->log_m, domain_wf(dom2), domain_wi(dom2), domain_wf(dom2),
                                  domain_consts(dom1) + 16, domain_consts(dom2) + 24, M, hscr, sh)) == cudaSuccess &&
+       (e = cudaEventRecord(ctx->aux_ev[6], sh)) == cudaSuccess &&  // H step done (stage times)
        // polH = M[m .. 2m-2]; M[2m-1] (always zero) becomes the -rs term for delta_1
        (e = cudaMemcpyAsync(M + (size_t)(2 * m - 1) * 8, rs + 16, 32, cudaMemcpyDeviceToDevice, sh)) == cudaSuccess &&
        (e = run_msm(false, M + (size_t)m * 8, pk->h_ext, pk->fh, m, outH, P.ms_h, P.bytes_h, sh)) == cudaSuccess;

@@ -295,6 +295,13 @@ class Prover:
         """Windows of the A, B1, B2, C, H tables (0 = no table)."""
         return [int(lib().cs_pk_fixed_window(self.handle, k)) for k in range(5)]
 
+    def stages(self) -> dict:
+        """Stage completion times (ms) of the last finished proof on this prover's context."""
+        out = (ctypes.c_float * 7)()
+        check(lib().cs_ctx_prove_stages(self.ctx.handle, out, 7), self.ctx.handle)
+        keys = ("A", "B1", "B2", "C", "hstep", "H", "total")
+        return {k: round(float(v), 3) for k, v in zip(keys, out)}
+
     def device_bytes(self) -> int:
         return int(lib().cs_pk_device_bytes(self.handle))
 

@@ -131,6 +131,8 @@ def main(argv=None):
         rec = dict(info, rep=i, ms=round(ctx.last_ms, 4))
         if args.what == "msm":
             rec["accumulate_ms"] = round(ctx.last_phase_ms, 4)
+        if args.what == "prove":
+            rec["stages_ms"] = call.keep[2].stages()
         print(json.dumps(rec), flush=True)
     torch.cuda.profiler.stop()
 

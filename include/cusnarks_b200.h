@@ -385,6 +385,10 @@ int cs_prove(cs_ctx *ctx, cs_pk *pk, const uint32_t *w, const uint32_t *r, const
              uint32_t *proof);
 int cs_prove_device(cs_ctx *ctx, cs_pk *pk, const uint32_t *d_w, const uint32_t *r, const uint32_t *s,
                     uint32_t *d_proof);
+/* Stage completion times (ms after the start) of the context's last finished proof: A, B1,
+ * B2 (G2), C MSM chains, H step, H MSM, whole proof (up to n of them; the reference prover's
+ * t_GP phase dict).  Call after the proof has completed (cs_prove, or cs_ctx_sync). */
+int cs_ctx_prove_stages(cs_ctx *ctx, float *ms, int n);
 
 /* ----------------------------------------------- served proving (continuous batching) */
 /* Replaces the reference's one-proof-at-a-time server loop (groth_prover.py:808-891
