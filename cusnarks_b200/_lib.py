@@ -134,6 +134,11 @@ _SIGNATURES = [
     ("find_roots_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32]),
     ("ntt_interpolandmul_server_h", ctypes.POINTER(ctypes.c_uint32), [_vp]),
     ("get_Mtranspose_h", ctypes.POINTER(ctypes.c_uint32), []),
+    ("get_Mmul_h", ctypes.POINTER(ctypes.c_uint32), []),
+    ("ntt_parallel_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_ulonglong, ctypes.c_int32,
+                              ctypes.c_int, ctypes.c_uint32]),
+    ("ntt_parallel2D_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                ctypes.c_ulonglong, ctypes.c_int32, ctypes.c_uint32]),
     ("cs_ntt_last_status", ctypes.c_int, []),
     ("cs_ntt_device", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint32, ctypes.c_int, ctypes.c_int]),
     ("cs_hstep_device", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, ctypes.c_uint32, _vp]),

@@ -37,6 +37,20 @@ CSB_DEV bool affine_is_inf(const Affine<F>& a) {
 template <class F>
 CSB_DEV XYZZ<F> xyzz_dbl(const XYZZ<F>& p) {
   if (p.is_inf()) return p;
+#if CSB_PAIRED
+  const F U = p.Y.dbl();
+  F V, X2, W, S, MM, T1, T2;
+  F::sqr2(U, p.X, V, X2);
+  F::mul2(U, V, p.X, V, W, S);
+  const F M = X2.dbl() + X2;
+  XYZZ<F> r;
+  F::mul2(M, M, W, p.ZZZ, MM, r.ZZZ);
+  r.X = MM - S.dbl();
+  F::mul2(M, S - r.X, W, p.Y, T1, T2);
+  r.Y = T1 - T2;
+  r.ZZ = V * p.ZZ;
+  return r;
+#else
   const F U = p.Y.dbl();
   const F V = U.sqr();
   const F W = U * V;
@@ -49,6 +63,7 @@ CSB_DEV XYZZ<F> xyzz_dbl(const XYZZ<F>& p) {
   r.ZZ = V * p.ZZ;
   r.ZZZ = W * p.ZZZ;
   return r;
+#endif
 }
 
 // mdbl-2008-s-1: double an affine point
@@ -72,6 +87,26 @@ CSB_DEV XYZZ<F> xyzz_mdbl(const Affine<F>& p) {
 template <class F>
 CSB_DEV XYZZ<F> xyzz_madd(const XYZZ<F>& p, const Affine<F>& q) {
   if (p.is_inf()) return XYZZ<F>::from_affine(q);
+#if CSB_PAIRED
+  // the ten products go in five independent pairs (F::mul2 interleaves each pair)
+  F U2, S2;
+  F::mul2(q.x, p.ZZ, q.y, p.ZZZ, U2, S2);
+  const F P = U2 - p.X;
+  const F R = S2 - p.Y;
+  if (P.is_zero()) {
+    if (R.is_zero()) return xyzz_mdbl(q);
+    return XYZZ<F>::inf();
+  }
+  F PP, RR, PPP, Q, T1, T2;
+  F::sqr2(P, R, PP, RR);
+  F::mul2(P, PP, p.X, PP, PPP, Q);
+  XYZZ<F> r;
+  r.X = RR - PPP - Q.dbl();
+  F::mul2(R, Q - r.X, p.Y, PPP, T1, T2);
+  r.Y = T1 - T2;
+  F::mul2(p.ZZ, PP, p.ZZZ, PPP, r.ZZ, r.ZZZ);
+  return r;
+#else
   const F U2 = q.x * p.ZZ;
   const F S2 = q.y * p.ZZZ;
   const F P = U2 - p.X;
@@ -89,6 +124,7 @@ CSB_DEV XYZZ<F> xyzz_madd(const XYZZ<F>& p, const Affine<F>& q) {
   r.ZZ = p.ZZ * PP;
   r.ZZZ = p.ZZZ * PPP;
   return r;
+#endif
 }
 
 // add-2008-s: p + q, both XYZZ
@@ -96,6 +132,27 @@ template <class F>
 CSB_DEV XYZZ<F> xyzz_add(const XYZZ<F>& p, const XYZZ<F>& q) {
   if (p.is_inf()) return q;
   if (q.is_inf()) return p;
+#if CSB_PAIRED
+  F U1, U2, S1, S2;
+  F::mul2(p.X, q.ZZ, q.X, p.ZZ, U1, U2);
+  F::mul2(p.Y, q.ZZZ, q.Y, p.ZZZ, S1, S2);
+  const F P = U2 - U1;
+  const F R = S2 - S1;
+  if (P.is_zero()) {
+    if (R.is_zero()) return xyzz_dbl(p);
+    return XYZZ<F>::inf();
+  }
+  F PP, RR, PPP, Q, T1, T2, Z2, Z3;
+  F::sqr2(P, R, PP, RR);
+  F::mul2(P, PP, U1, PP, PPP, Q);
+  XYZZ<F> r;
+  r.X = RR - PPP - Q.dbl();
+  F::mul2(R, Q - r.X, S1, PPP, T1, T2);
+  r.Y = T1 - T2;
+  F::mul2(p.ZZ, q.ZZ, p.ZZZ, q.ZZZ, Z2, Z3);
+  F::mul2(Z2, PP, Z3, PPP, r.ZZ, r.ZZZ);
+  return r;
+#else
   const F U1 = p.X * q.ZZ;
   const F U2 = q.X * p.ZZ;
   const F S1 = p.Y * q.ZZZ;
@@ -115,6 +172,7 @@ CSB_DEV XYZZ<F> xyzz_add(const XYZZ<F>& p, const XYZZ<F>& q) {
   r.ZZ = p.ZZ * q.ZZ * PP;
   r.ZZZ = p.ZZZ * q.ZZZ * PPP;
   return r;
+#endif
 }
 
 // Out-of-line copies for kernels whose cost is latency, not throughput (bucket-sum

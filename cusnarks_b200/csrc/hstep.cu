@@ -298,6 +298,12 @@ std::vector<uint32_t>& interp_result() {
   static std::vector<uint32_t> buf;
   return buf;
 }
+// the last H step's (Nrows, Ncols) and its result in the reference's pre-transpose layout
+uint32_t g_interp_rows = 0, g_interp_cols = 0;
+std::vector<uint32_t>& interp_mmul() {
+  static std::vector<uint32_t> buf;
+  return buf;
+}
 
 }  // namespace
 
@@ -393,11 +399,60 @@ uint32_t* ntt_interpolandmul_server_h(ntt_interpolandmul_t* args) {
          (e = cudaStreamSynchronize(ctx->stream)) == cudaSuccess;
   }
   if (!ok) { set_status(fail(ctx, e, "interpolandmul"), ctx); return nullptr; }
+  g_interp_rows = args->Nrows;
+  g_interp_cols = args->Ncols;
+  interp_mmul().clear();
   set_status(CS_OK, ctx);
   return res.data();
 }
 
 uint32_t* get_Mtranspose_h(void) { return interp_result().empty() ? nullptr : interp_result().data(); }
+
+// The reference keeps the H step's coefficients in M_mul as a 2^mr x 2^mc matrix before its
+// last transpose into M_transpose (ntt.cpp:1066, split from ntt.cpp:767).
+uint32_t* get_Mmul_h(void) {
+  std::vector<uint32_t>& res = interp_result();
+  if (res.empty()) return nullptr;
+  std::vector<uint32_t>& mm = interp_mmul();
+  if (mm.empty()) {
+    const uint32_t mr = g_interp_rows < g_interp_cols ? g_interp_rows + 1 : g_interp_rows;
+    const uint32_t mc = g_interp_rows < g_interp_cols ? g_interp_cols : g_interp_cols + 1;
+    const size_t R = (size_t)1 << mr, C = (size_t)1 << mc;
+    if (R * C * 8 != res.size()) return nullptr;
+    mm.resize(res.size());
+    for (size_t r = 0; r < R; r++)
+      for (size_t c = 0; c < C; c++) std::memcpy(&mm[(r * C + c) * 8], &res[(c * R + r) * 8], 32);
+  }
+  return mm.data();
+}
+
+// Four-step transforms of the reference (ntt.cpp:274, :199): their result is the
+// natural-order transform of 2^(Nrows+Ncols) points, computed here in one pass.
+void ntt_parallel_h(uint32_t* A, const uint32_t* roots, uint32_t Nrows, uint32_t Ncols,
+                    unsigned long long rstride, int32_t direction, fft_mode_t fft_mode, uint32_t pidx) {
+  cs_ctx* ctx = ntt_default_ctx();
+  if (!ctx) { t_ntt_status = CS_ERR_NODEVICE; return; }
+  if (pidx != 1 || !A || !roots || rstride == 0 || (int)fft_mode < 0 || fft_mode >= FFT_T_MODE_N) {
+    t_ntt_status = CS_ERR_ARG;
+    return;
+  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  set_status(host_ntt(ctx, A, roots, Nrows + Ncols, 1, rstride, direction >= 0 ? 1 : -1, -1), ctx);
+}
+
+void ntt_parallel2D_h(uint32_t* A, const uint32_t* roots, uint32_t Nrows, uint32_t fft_Nyx, uint32_t Ncols,
+                      uint32_t fft_Nxx, unsigned long long rstride, int32_t direction, uint32_t pidx) {
+  cs_ctx* ctx = ntt_default_ctx();
+  if (!ctx) { t_ntt_status = CS_ERR_NODEVICE; return; }
+  if (pidx != 1 || !A || !roots || rstride == 0 || direction != 1 || fft_Nyx > Nrows || fft_Nxx > Ncols) {
+    t_ntt_status = CS_ERR_ARG;
+    return;
+  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  set_status(host_ntt(ctx, A, roots, Nrows + Ncols, 1, rstride, 1, -1), ctx);
+}
 
 // ------------------------------------------------------------ context API ------------
 int cs_ntt_device(cs_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, int direction,

@@ -224,7 +224,11 @@ __global__ void k_task_emit(const uint32_t* __restrict__ offsets, uint32_t nb, u
 #define CSB_ACC_G2_MINB 3  // 168 registers: 12 warps per SM instead of 8 (measured faster)
 #endif
 #ifndef CSB_ACC_G1_MINB
+#if CSB_PAIRED
+#define CSB_ACC_G1_MINB 4  // paired products fit 128 registers without spills
+#else
 #define CSB_ACC_G1_MINB 0
+#endif
 #endif
 template <class F> struct AccMinBlocks { static constexpr int value = CSB_ACC_G1_MINB; };
 template <> struct AccMinBlocks<Fq2> { static constexpr int value = CSB_ACC_G2_MINB; };

@@ -141,6 +141,27 @@ void find_roots_h(uint32_t *roots, uint32_t *primitive_root, uint32_t nroots, ui
 uint32_t *ntt_interpolandmul_server_h(ntt_interpolandmul_t *args);
 /* Replaces get_Mtranspose_h, reference src/cuda/ntt.cpp:659: the last H-step result. */
 uint32_t *get_Mtranspose_h(void);
+/* Replaces get_Mmul_h, reference src/cuda/ntt.cpp:650 (_utils_host.pxd:91): the last H-step
+ * result before the reference's final transpose, i.e. the 2m coefficients as a
+ * 2^mNrows x 2^mNcols matrix M with M[r][c] = coefficient c*2^mNrows + r, where
+ * (mNrows, mNcols) = (Nrows+1, Ncols) if Nrows < Ncols else (Nrows, Ncols+1)
+ * (ntt.cpp:767).  Valid until the next H-step call; NULL before the first. */
+uint32_t *get_Mmul_h(void);
+/* fft_mode_t, reference src/cuda/types.h:235 */
+typedef enum { FFT_T_DIT = 0, FFT_T_DIF, FFT_T_MODE_N } fft_mode_t;
+/* Replaces ntt_parallel_h, reference src/cuda/ntt.cpp:274 (_utils_host.pxd:78): the reference
+ * computes the 2^(Nrows+Ncols)-point transform by four steps (column transforms, twiddles,
+ * row transforms, transpose); its result is the natural-order transform of ntt_h with
+ * levels = Nrows + Ncols, astride 1, for both fft_mode values, which is what this returns. */
+void ntt_parallel_h(uint32_t *A, const uint32_t *roots, uint32_t Nrows, uint32_t Ncols,
+                    unsigned long long rstride, int32_t direction, fft_mode_t fft_mode, uint32_t pidx);
+/* Replaces ntt_parallel2D_h, reference src/cuda/ntt.cpp:199 (_utils_host.pxd:82): with
+ * direction 1 (the reference's only use: intt_parallel2D_h and its tests pass inverse roots
+ * with direction 1) the same natural-order 2^(Nrows+Ncols)-point transform.  The reference's
+ * twiddle step ignores direction, so direction -1 is not a transform there; it is refused
+ * here (status CS_ERR_ARG).  fft_Nyx / fft_Nxx only choose the reference's inner split. */
+void ntt_parallel2D_h(uint32_t *A, const uint32_t *roots, uint32_t Nrows, uint32_t fft_Nyx, uint32_t Ncols,
+                      uint32_t fft_Nxx, unsigned long long rstride, int32_t direction, uint32_t pidx);
 int cs_ntt_last_status(void);
 
 /* QAP evaluation.  Replaces mpoly_eval_server_h, reference src/cuda/mpoly.cpp:67

@@ -293,6 +293,14 @@ class RefLib:
                                ctypes.c_uint32]
         self._interp = L._Z27ntt_interpolandmul_server_hP20ntt_interpolandmul_t
         self._interp.restype = ctypes.POINTER(ctypes.c_uint32)
+        self._mmul = L._Z10get_Mmul_hv
+        self._mmul.restype = ctypes.POINTER(ctypes.c_uint32)
+        self._nttp = L._Z14ntt_parallel_hPjPKjjjyi10fft_mode_tj
+        self._nttp.argtypes = [_u32p, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64,
+                               ctypes.c_int32, ctypes.c_int, ctypes.c_uint32]
+        self._ntt2d = L._Z16ntt_parallel2D_hPjPKjjjjjyij
+        self._ntt2d.argtypes = [_u32p, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint32]
         self._mpoly = L._Z12mpoly_eval_hPv
         self._montmult = L._Z10montmult_hPjPKjS1_j
 
@@ -317,6 +325,25 @@ class RefLib:
         roots = np.ascontiguousarray(roots, dtype=np.uint32)
         self._intt(_p(A), _p(roots), fmat, levels, rstride, pidx)
         return A
+
+    def ntt_parallel(self, A, roots, nrows, ncols, rstride=1, direction=1, fft_mode=0, pidx=1):
+        """ntt_parallel_h (src/cuda/ntt.cpp:274): four-step transform of 2^(nrows+ncols)."""
+        A = np.array(A, dtype=np.uint32, copy=True).reshape(-1, 8)
+        roots = np.ascontiguousarray(roots, dtype=np.uint32)
+        self._nttp(_p(A), _p(roots), nrows, ncols, rstride, direction, fft_mode, pidx)
+        return A
+
+    def ntt_parallel2D(self, A, roots, nrows, fft_ny, ncols, fft_nx, rstride=1, direction=1, pidx=1):
+        """ntt_parallel2D_h (src/cuda/ntt.cpp:199)."""
+        A = np.array(A, dtype=np.uint32, copy=True).reshape(-1, 8)
+        roots = np.ascontiguousarray(roots, dtype=np.uint32)
+        self._ntt2d(_p(A), _p(roots), nrows, fft_ny, ncols, fft_nx, rstride, direction, pidx)
+        return A
+
+    def mmul(self, levels):
+        """get_Mmul_h (src/cuda/ntt.cpp:650) after an interpolandmul of 2^levels points."""
+        ptr = self._mmul()
+        return np.ctypeslib.as_array(ptr, shape=((2 << levels) * 8,)).copy().reshape(-1, 8)
 
     def interpolandmul(self, A, B, roots_full, levels, rstride=2, max_threads=8):
         """roots_full: the caller's concatenated table [2m | 2^(n/2) | 2^(...)] roots."""

@@ -13,7 +13,8 @@ Sources:
     (Montgomery products mod r, :94-164), p_root128 and roots_128_test (:90, :165),
     ext_X_test / ext_X0X1_test (Fp2 products, :6395, :6700).
   * outputs of the reference CPU library itself (oracle/_ref) on small seeded inputs for
-    ntt_h, intt_h, ntt_interpolandmul_server_h and mpoly_eval_h.
+    ntt_h, intt_h, ntt_parallel_h, ntt_parallel2D_h, ntt_interpolandmul_server_h (with
+    get_Mmul_h after it) and mpoly_eval_h.
 
 The fixtures are what the GPU tests compare against on a machine without the reference.
 """
@@ -107,6 +108,7 @@ def main():
         out[f"hstep_A_{L}"] = A
         out[f"hstep_B_{L}"] = B
         out[f"hstep_M_{L}"] = ref.interpolandmul(A, B, table, L, 2)
+        out[f"hstep_Mmul_{L}"] = ref.mmul(L)
     for (nv, nc, k) in ((16, 16, 3), (300, 256, 4)):
         pin = make_mpoly(rng, nv, nc, k, oracle)
         w = random_field(rng, nv, 1)
@@ -114,6 +116,19 @@ def main():
         out[f"mpoly_w_{nv}"] = w
         out[f"mpoly_out_{nv}"] = ref.mpoly_eval(w, pin, nc, 0, nv, 1)
         out[f"mpoly_ncons_{nv}"] = np.array([nc], np.uint32)
+    # four-step transforms (ntt_parallel_h, ntt_parallel2D_h): (rows, cols, inner splits)
+    for (nr, nc, fy, fx) in ((3, 4, 1, 2), (5, 5, 2, 3), (6, 4, 3, 2)):
+        L = nr + nc
+        A = oracle.to_mont(random_field(rng, 1 << L, 1), 1)
+        roots = oracle.find_roots(L + 1)
+        iroots = np.concatenate([roots[:1], roots[1:][::-1]])   # w^-j
+        out[f"par_in_{nr}_{nc}"] = A
+        for d in (1, -1):
+            for mode in (0, 1):
+                out[f"par_{nr}_{nc}_{d}_{mode}"] = ref.ntt_parallel(A, roots, nr, nc, 2, d, mode, 1)
+        out[f"par2d_{nr}_{nc}_fwd"] = ref.ntt_parallel2D(A, roots, nr, fy, nc, fx, 2, 1, 1)
+        out[f"par2d_{nr}_{nc}_inv"] = ref.ntt_parallel2D(A, iroots, nr, fy, nc, fx, 2, 1, 1)
+        out[f"par2d_{nr}_{nc}_shape"] = np.array([nr, fy, nc, fx], np.uint32)
     np.savez_compressed(os.path.join(HERE, "ref_transforms.npz"), **out)
     print("fixtures written to", HERE)
 

@@ -78,6 +78,49 @@ def test_dropin_interpolandmul_reference_fixture(oracle, golden, L):
     assert np.array_equal(A, f[f"hstep_A_{L}"])  # inputs untouched
 
 
+@pytest.mark.parametrize("nr,nc", [(3, 4), (5, 5), (6, 4)])
+def test_dropin_ntt_parallel_reference_fixture(oracle, golden, nr, nc):
+    """ntt_parallel_h (both fft modes and directions) and ntt_parallel2D_h (forward table and
+    inverse table, direction 1) reproduce the reference library's four-step outputs."""
+    f = golden("ref_transforms.npz")
+    L_ = _lib()
+    L = nr + nc
+    roots = np.ascontiguousarray(oracle.find_roots(L + 1))
+    iroots = np.ascontiguousarray(np.concatenate([roots[:1], roots[1:][::-1]]))
+    A = np.ascontiguousarray(f[f"par_in_{nr}_{nc}"])
+    for d in (1, -1):
+        for mode in (0, 1):
+            a = A.copy()
+            L_.ntt_parallel_h(a.ctypes.data, roots.ctypes.data, nr, nc, 2, d, mode, 1)
+            assert L_.cs_ntt_last_status() == 0
+            assert np.array_equal(a, f[f"par_{nr}_{nc}_{d}_{mode}"]), (d, mode)
+    _, fy, _, fx = (int(x) for x in f[f"par2d_{nr}_{nc}_shape"])
+    for tab, key in ((roots, "fwd"), (iroots, "inv")):
+        a = A.copy()
+        L_.ntt_parallel2D_h(a.ctypes.data, tab.ctypes.data, nr, fy, nc, fx, 2, 1, 1)
+        assert L_.cs_ntt_last_status() == 0
+        assert np.array_equal(a, f[f"par2d_{nr}_{nc}_{key}"]), key
+    a = A.copy()
+    L_.ntt_parallel2D_h(a.ctypes.data, roots.ctypes.data, nr, fy, nc, fx, 2, -1, 1)
+    assert L_.cs_ntt_last_status() != 0 and np.array_equal(a, A)  # not a transform in the reference
+
+
+@pytest.mark.parametrize("L", [4, 7, 10])
+def test_dropin_get_mmul_reference_fixture(oracle, golden, L):
+    """get_Mmul_h after an H step: the reference's pre-transpose matrix of the result."""
+    from cusnarks_b200._lib import InterpolAndMul
+    f = golden("ref_transforms.npz")
+    L_ = _lib()
+    table = np.ascontiguousarray(hstep_roots_table(oracle, L))
+    A = np.ascontiguousarray(f[f"hstep_A_{L}"]); B = np.ascontiguousarray(f[f"hstep_B_{L}"])
+    args = InterpolAndMul(A.ctypes.data, B.ctypes.data, table.ctypes.data, L - L // 2, L // 2, 0, 0, L, 2, 1, 8, 0, 0, 0)
+    assert L_.ntt_interpolandmul_server_h(ctypes.byref(args))
+    ptr = L_.get_Mmul_h()
+    assert ptr
+    M = np.ctypeslib.as_array(ptr, shape=((2 << L) * 8,)).copy().reshape(-1, 8)
+    assert np.array_equal(M, f[f"hstep_Mmul_{L}"])
+
+
 def _dev(a):
     import torch
     return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
