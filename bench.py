@@ -6,7 +6,9 @@
 Prints ONE JSON line (rank 0).  Under torchrun (N > 1) every rank runs its own replica of
 the workload (proofs are independent: no data-path collective); the timed region is
 bracketed by barriers, device time is the max over ranks, and ``value`` is the total over
-all ranks (weak scaling).
+all ranks (weak scaling).  With N > 1 the line also carries ``sharded_g1_msm_2^20``: one
+2^20-term G1 MSM split over the N GPUs (one-point NCCL all-gather of the partial sums), the
+strong-scaling case of a single MSM.
 
 Workload (the configuration the headline metric is quoted on): full Groth16 prove for a
 synthetic R1CS of 2^20 constraints (nConstraints = 2^20 - 2, one public input, A and B rows
@@ -251,6 +253,36 @@ class MsmWorkload:
         from cusnarks_b200._lib import lib
         c = lib().cs_msm_default_window(self.n, 0)
         return self.n * lib().cs_msm_num_windows(c), c
+
+
+def sharded_msm_leg(ctx, world, rank, reps: int, log_n: int = 20, seed: int = 7):
+    """One 2^log_n G1 MSM split over all ranks (cusnarks_b200.sharded): each rank makes its own
+    shard's bases and scalars on its GPU; per call, local MSM + one-point all-gather (NCCL) +
+    point sum.  Device span per rank (events around the synchronising call), max over ranks."""
+    import torch
+    from cusnarks_b200.sharded import sharded_msm, shard_range
+    from cusnarks_b200.synth import random_field, g1_generator
+    n = 1 << log_n
+    lo, hi = shard_range(n, rank, world)
+    rng = np.random.Generator(np.random.PCG64(seed + 31 * rank))
+    dev = torch.device("cuda", ctx.device)
+    k = torch.from_numpy(random_field(rng, hi - lo).view(np.int32)).to(dev)
+    sc = torch.from_numpy(random_field(rng, hi - lo).view(np.int32)).to(dev)
+    g = torch.from_numpy(g1_generator().view(np.int32)).to(dev)
+    pts = torch.empty((hi - lo, 16), dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    ctx.scmul_device(k.data_ptr(), g.data_ptr(), hi - lo, pts.data_ptr(), point_stride_words=0)
+    ctx.sync()
+    for _ in range(2):
+        sharded_msm(ctx, sc, pts)
+    spans = []
+    for _ in range(reps):
+        barrier(world)
+        spans.append(device_span_ms(lambda: sharded_msm(ctx, sc, pts)))
+    ms = max_over_ranks(statistics.median(spans), world)
+    return {"ms": round(ms, 3), "terms": n, "terms_per_rank": hi - lo, "ranks": world,
+            "basis": "one 2^20 G1 MSM split over the ranks (contiguous shards, one-point NCCL all-gather, "
+                     "point sum); device span per call, median of reps, max over ranks (strong scaling)"}
 
 
 class ServedDevice:
@@ -537,6 +569,8 @@ def run_ours(args, world, rank, local):
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if world > 1:  # every rank takes part (collective)
+        line["sharded_g1_msm_2^20"] = sharded_msm_leg(ctx, world, rank, reps=max(3, args.steps))
     if rank == 0 and not args.no_batch:
         line["batched_msm"] = batched_msm(ctx, reps=3)
     if rank == 0 and not args.no_mix:

@@ -153,6 +153,11 @@ class Context:
                                         ctypes.c_void_p(d_points), point_stride_words, n,
                                         ctypes.c_void_p(d_out)), self.handle)
 
+    def point_sum_device(self, d_points: int, n: int, d_out: int, ec2: bool = False, dims: int = 2):
+        """d_out = the affine sum of n points (rows of dims = 2 affine / 3 Jacobian coordinates)."""
+        check(self._lib.cs_point_sum_device(self.handle, int(bool(ec2)), ctypes.c_void_p(d_points), n, dims,
+                                            ctypes.c_void_p(d_out)), self.handle)
+
     def imad_peak(self) -> float:
         v = ctypes.c_double()
         check(self._lib.cs_bench_imad_peak(self.handle, ctypes.byref(v)), self.handle)

@@ -355,6 +355,19 @@ int cs_scmul_device(cs_ctx* ctx, int ec2, const uint32_t* d_scalars, const uint3
   return CS_OK;
 }
 
+int cs_point_sum_device(cs_ctx* ctx, int ec2, const uint32_t* d_points, uint32_t n, int dims,
+                        uint32_t* d_out) {
+  if (!ctx || !d_out || (n && !d_points) || (dims != 2 && dims != 3)) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  EventScope ev(ctx);
+  cudaError_t e = ec2 ? csb::point_sum_g2(d_points, n, dims, d_out, ctx->stream)
+                      : csb::point_sum_g1(d_points, n, dims, d_out, ctx->stream);
+  ev.stop();
+  if (e != cudaSuccess) return fail(ctx, e, "point sum launch");
+  return CS_OK;
+}
+
 // ------------------------------------------------------------ drop-in entry points ---
 int cs_last_status(void) { return t_status; }
 unsigned long long cs_kernel_launches(void) { return csb::g_launches.load(); }

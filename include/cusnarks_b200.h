@@ -280,6 +280,13 @@ int cs_field_op_device(cs_ctx *ctx, int op, int pidx, const uint32_t *d_a, const
 int cs_scmul_device(cs_ctx *ctx, int ec2, const uint32_t *d_scalars, const uint32_t *d_points,
                     uint32_t point_stride_words, uint32_t n, uint32_t *d_out_affine);
 
+/* Sum of n points as one affine point (Montgomery, the reference's infinity encoding):
+ * rows of dims = 2 (affine) or 3 (Jacobian) coordinates, as the reference's
+ * ec_jacaddreduce_h (src/cuda/ec.cpp:1266) on device data.  It combines the per-shard
+ * results of an MSM split across GPUs.  Device pointers, asynchronous on the context stream. */
+int cs_point_sum_device(cs_ctx *ctx, int ec2, const uint32_t *d_points, uint32_t n, int dims,
+                        uint32_t *d_out_affine);
+
 /* Transform of 2^log_n Fr elements (Montgomery) with the context's resident twiddles
  * (primitive roots 5^((r-1)/2^k), the reference's proots_field chain).  direction >= 0:
  * forward; < 0: inverse scaled by 2^-log_n, Montgomery (fmat 1) or normal (fmat 0) out.
