@@ -2,6 +2,7 @@
 // instantiated for G1 in msm_g1.cu and for G2 in msm_g2.cu.
 #pragma once
 #include <algorithm>
+#include <type_traits>
 #include "msm.cuh"
 #include "curve.cuh"
 #include "scan.cuh"
@@ -900,11 +901,18 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   note_launch();
   int levels = 1;
   uint32_t *y = lv_y, *z = lv_z, *y2 = lv_y2, *z2 = lv_z2;
-  // more (warp-cooperative) levels keep the top block's chain short
+  // more levels until the top block's chain is short.  Measured at 2^20 (B200): a proof
+  // (five MSMs sharing the GPU) 30.5 -> 29.2 ms with one thread per 8 segments, which does a
+  // quarter of the cooperative levels' work; a lone G2 fixed-base MSM is 0.47 ms faster with
+  // the cooperative levels' shorter chains; a lone G1 MSM is equal or faster serial.
+  const bool serial_levels = cfg.reduce_serial >= 0 ? cfg.reduce_serial != 0 : !std::is_same<F, Fq2>::value;
   while (nseg > kTopSegments) {
     const uint32_t nnext = (nseg + 7) / 8;
     const uint32_t threads = (uint32_t)WR * nnext * 8;
-    k_reduce_level_coop<F><<<(threads + 127) / 128, 128, 0, st>>>(y, z, nseg, nnext, WR, levels, y2, z2);
+    if (serial_levels)
+      k_reduce_level<F><<<((uint32_t)WR * nnext + 127) / 128, 128, 0, st>>>(y, z, nseg, nnext, WR, levels, y2, z2);
+    else
+      k_reduce_level_coop<F><<<(threads + 127) / 128, 128, 0, st>>>(y, z, nseg, nnext, WR, levels, y2, z2);
     note_launch();
     uint32_t* ty = y; y = y2; y2 = ty;
     uint32_t* tz = z; z = z2; z2 = tz;

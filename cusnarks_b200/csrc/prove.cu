@@ -459,6 +459,7 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
   if ((e = domain_get(ctx, pk->log_m + 1, &dom2)) != cudaSuccess || (e = domain_get(ctx, pk->log_m, &dom1)) != cudaSuccess)
     return fail(ctx, e, "prove tables");
   MsmConfig cfg;
+  cfg.reduce_serial = 1;
   const GlvSplit glv_rs[2] = {glv::split(s), glv::split(r)};  // s * pi_A, r * pi_B1
   cudaEventRecord(ctx->ev_start, s0);
   // scalars: w ++ [1, r] and w ++ [1, s]; r, s, -rs
@@ -482,6 +483,7 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
     if (pk->has_fixed()) {
       MsmConfig fcfg;
       fcfg.c = f.c;
+      fcfg.reduce_serial = 1;  // the proof's MSMs share the GPU: least reduction work
       return ec2 ? msm_fixed_g2(sc, f.table, n, out, at(off), bytes, fcfg, st)
                  : msm_fixed_g1(sc, f.table, n, out, at(off), bytes, fcfg, st);
     }
