@@ -612,6 +612,29 @@ CSB_DEV int aff_kind(const Affine<F>& p, const Affine<F>& q, bool has_q, F& d) {
   return 4;
 }
 
+// The denominator of slot s from the two x coordinates alone (half the bytes of the pair);
+// the y coordinates are read only where the kind depends on them (a zero x: a point at
+// infinity or x = 0; equal x: doubling or opposite points).
+template <class F, bool FIRST>
+CSB_DEV F aff_denominator(const uint32_t* in_off, const uint32_t* out_off, uint32_t b, uint32_t s,
+                          const uint32_t* entries, const uint32_t* src) {
+  constexpr int PW = 2 * FieldWords<F>::value;
+  const uint32_t i0 = in_off[b] + 2 * (s - out_off[b]);
+  if (i0 + 1 >= in_off[b + 1]) return F::one();  // odd last point: copied
+  const uint32_t a0 = FIRST ? (entries[i0] & ~NEG_BIT) : i0;
+  const uint32_t a1 = FIRST ? (entries[i0 + 1] & ~NEG_BIT) : i0 + 1;
+  F px, qx;
+  ld_field(px, src + (size_t)a0 * PW);
+  ld_field(qx, src + (size_t)a1 * PW);
+  if (!px.is_zero() && !qx.is_zero() && !(px == qx)) return qx - px;
+  Affine<F> p, q;
+  bool has_q;
+  aff_pair<F, FIRST>(in_off, out_off, b, s, entries, src, p, q, has_q);
+  F d;
+  aff_kind(p, q, has_q, d);
+  return d;
+}
+
 template <class F>
 CSB_DEV uint32_t bucket_of_slot(const uint32_t* off, uint32_t nb, uint32_t s) {
   uint32_t lo = 0, hi = nb;  // largest b with off[b] <= s (empty buckets share offsets)
@@ -640,12 +663,7 @@ __global__ void __launch_bounds__(128) k_affine_round(const uint32_t* __restrict
   uint32_t b = b0;
   for (uint32_t s = s0; s < s1; s++) {
     while (out_off[b + 1] <= s) b++;
-    Affine<F> p, q;
-    bool has_q;
-    aff_pair<F, FIRST>(in_off, out_off, b, s, entries, src, p, q, has_q);
-    F d;
-    aff_kind(p, q, has_q, d);
-    acc = acc * d;
+    acc = acc * aff_denominator<F, FIRST>(in_off, out_off, b, s, entries, src);
     st_field(pref + (size_t)s * FW, acc);
   }
   F inv = acc.inv();
@@ -757,7 +775,10 @@ inline int auto_affine_rounds_rt(bool ec2, uint32_t n, int W, size_t nb) {
   // pairs (>= 2^22, i.e. N W >= 2^23 entries) to fill the GPU, or its chain sets the latency
   // (2 rounds cost 2.5 ms in a 2^12-term G2 MSM)
   if ((uint64_t)n * W < (1ull << 23)) return 0;
-  const int cap = ec2 ? 2 : 0;
+#ifndef CSB_AFF_G1_CAP
+#define CSB_AFF_G1_CAP 0
+#endif
+  const int cap = ec2 ? 2 : CSB_AFF_G1_CAP;
   const double avg = (double)n * W / (double)nb;
   int r = 0;
   while (r < cap && avg >= (double)(8u << r)) r++;
