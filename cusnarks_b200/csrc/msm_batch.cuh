@@ -172,9 +172,12 @@ cudaError_t batch_impl(const MsmBatch& b, void* d_work, size_t work_bytes, cudaS
     while (nseg > kTopSegments) {
       const uint32_t nnext = (nseg + 7) / 8;
       const uint32_t threads = WR * nnext * 8;
-      // one thread per 8 segments: the batch's groups fill the GPU, so least work wins
-      k_reduce_level<F><<<(WR * nnext + 127) / 128, 128, 0, st>>>(y, z, nseg, nnext, (int)WR, levels, y2, z2);
-      (void)threads;
+      // large levels one thread per 8 segments (least work: the batch's groups fill the GPU),
+      // small top levels cooperative (short chains)
+      if ((uint64_t)WR * nseg > kSerialMinSegments)
+        k_reduce_level<F><<<(WR * nnext + 127) / 128, 128, 0, st>>>(y, z, nseg, nnext, (int)WR, levels, y2, z2);
+      else
+        k_reduce_level_coop<F><<<(threads + 127) / 128, 128, 0, st>>>(y, z, nseg, nnext, (int)WR, levels, y2, z2);
       note_launch();
       uint32_t* ty = y; y = y2; y2 = ty;
       uint32_t* tz = z; z = z2; z2 = tz;
