@@ -33,37 +33,51 @@ CSB_DEV bool affine_is_inf(const Affine<F>& a) {
   return a.x.is_zero() && a.y == F::one();
 }
 
+// Paired-product helpers of the formulas below: PAIR = true computes each independent pair
+// of products in one out-of-line call with interleaved rows (F::mul2_ool), which shortens a
+// single thread's dependent chain; false uses F::mul2 (two products unless CSB_PAIR).
+template <class F, bool PAIR>
+struct PairOps {
+  static CSB_DEV void mul2(const F& a, const F& b, const F& c, const F& d, F& x, F& y) {
+    if constexpr (PAIR) F::mul2_ool(a, b, c, d, x, y); else F::mul2(a, b, c, d, x, y);
+  }
+  static CSB_DEV void sqr2(const F& a, const F& c, F& x, F& y) {
+    if constexpr (PAIR) F::sqr2_ool(a, c, x, y); else F::sqr2(a, c, x, y);
+  }
+};
+
 // dbl-2008-s-1 (a = 0)
-template <class F>
+template <class F, bool PAIR = (CSB_PAIRED != 0)>
 CSB_DEV XYZZ<F> xyzz_dbl(const XYZZ<F>& p) {
   if (p.is_inf()) return p;
-#if CSB_PAIRED
-  const F U = p.Y.dbl();
-  F V, X2, W, S, MM, T1, T2;
-  F::sqr2(U, p.X, V, X2);
-  F::mul2(U, V, p.X, V, W, S);
-  const F M = X2.dbl() + X2;
-  XYZZ<F> r;
-  F::mul2(M, M, W, p.ZZZ, MM, r.ZZZ);
-  r.X = MM - S.dbl();
-  F::mul2(M, S - r.X, W, p.Y, T1, T2);
-  r.Y = T1 - T2;
-  r.ZZ = V * p.ZZ;
-  return r;
-#else
-  const F U = p.Y.dbl();
-  const F V = U.sqr();
-  const F W = U * V;
-  const F S = p.X * V;
-  const F X2 = p.X.sqr();
-  const F M = X2.dbl() + X2;
-  XYZZ<F> r;
-  r.X = M.sqr() - S.dbl();
-  r.Y = M * (S - r.X) - W * p.Y;
-  r.ZZ = V * p.ZZ;
-  r.ZZZ = W * p.ZZZ;
-  return r;
-#endif
+  if constexpr (PAIR) {
+    using O = PairOps<F, true>;
+    const F U = p.Y.dbl();
+    F V, X2, W, S, MM, T1, T2;
+    O::sqr2(U, p.X, V, X2);
+    O::mul2(U, V, p.X, V, W, S);
+    const F M = X2.dbl() + X2;
+    XYZZ<F> r;
+    O::mul2(M, M, W, p.ZZZ, MM, r.ZZZ);
+    r.X = MM - S.dbl();
+    O::mul2(M, S - r.X, W, p.Y, T1, T2);
+    r.Y = T1 - T2;
+    r.ZZ = V * p.ZZ;
+    return r;
+  } else {
+    const F U = p.Y.dbl();
+    const F V = U.sqr();
+    const F W = U * V;
+    const F S = p.X * V;
+    const F X2 = p.X.sqr();
+    const F M = X2.dbl() + X2;
+    XYZZ<F> r;
+    r.X = M.sqr() - S.dbl();
+    r.Y = M * (S - r.X) - W * p.Y;
+    r.ZZ = V * p.ZZ;
+    r.ZZZ = W * p.ZZZ;
+    return r;
+  }
 }
 
 // mdbl-2008-s-1: double an affine point
@@ -84,95 +98,97 @@ CSB_DEV XYZZ<F> xyzz_mdbl(const Affine<F>& p) {
 }
 
 // madd-2008-s: p (XYZZ) + q (affine, not infinity)
-template <class F>
+template <class F, bool PAIR = (CSB_PAIRED != 0)>
 CSB_DEV XYZZ<F> xyzz_madd(const XYZZ<F>& p, const Affine<F>& q) {
   if (p.is_inf()) return XYZZ<F>::from_affine(q);
-#if CSB_PAIRED
-  // the ten products go in five independent pairs (F::mul2 interleaves each pair)
-  F U2, S2;
-  F::mul2(q.x, p.ZZ, q.y, p.ZZZ, U2, S2);
-  const F P = U2 - p.X;
-  const F R = S2 - p.Y;
-  if (P.is_zero()) {
-    if (R.is_zero()) return xyzz_mdbl(q);
-    return XYZZ<F>::inf();
+  if constexpr (PAIR) {
+    // the ten products in five independent pairs
+    using O = PairOps<F, true>;
+    F U2, S2;
+    O::mul2(q.x, p.ZZ, q.y, p.ZZZ, U2, S2);
+    const F P = U2 - p.X;
+    const F R = S2 - p.Y;
+    if (P.is_zero()) {
+      if (R.is_zero()) return xyzz_mdbl(q);
+      return XYZZ<F>::inf();
+    }
+    F PP, RR, PPP, Q, T1, T2;
+    O::sqr2(P, R, PP, RR);
+    O::mul2(P, PP, p.X, PP, PPP, Q);
+    XYZZ<F> r;
+    r.X = RR - PPP - Q.dbl();
+    O::mul2(R, Q - r.X, p.Y, PPP, T1, T2);
+    r.Y = T1 - T2;
+    O::mul2(p.ZZ, PP, p.ZZZ, PPP, r.ZZ, r.ZZZ);
+    return r;
+  } else {
+    const F U2 = q.x * p.ZZ;
+    const F S2 = q.y * p.ZZZ;
+    const F P = U2 - p.X;
+    const F R = S2 - p.Y;
+    if (P.is_zero()) {
+      if (R.is_zero()) return xyzz_mdbl(q);
+      return XYZZ<F>::inf();
+    }
+    const F PP = P.sqr();
+    const F PPP = P * PP;
+    const F Q = p.X * PP;
+    XYZZ<F> r;
+    r.X = R.sqr() - PPP - Q.dbl();
+    r.Y = R * (Q - r.X) - p.Y * PPP;
+    r.ZZ = p.ZZ * PP;
+    r.ZZZ = p.ZZZ * PPP;
+    return r;
   }
-  F PP, RR, PPP, Q, T1, T2;
-  F::sqr2(P, R, PP, RR);
-  F::mul2(P, PP, p.X, PP, PPP, Q);
-  XYZZ<F> r;
-  r.X = RR - PPP - Q.dbl();
-  F::mul2(R, Q - r.X, p.Y, PPP, T1, T2);
-  r.Y = T1 - T2;
-  F::mul2(p.ZZ, PP, p.ZZZ, PPP, r.ZZ, r.ZZZ);
-  return r;
-#else
-  const F U2 = q.x * p.ZZ;
-  const F S2 = q.y * p.ZZZ;
-  const F P = U2 - p.X;
-  const F R = S2 - p.Y;
-  if (P.is_zero()) {
-    if (R.is_zero()) return xyzz_mdbl(q);
-    return XYZZ<F>::inf();
-  }
-  const F PP = P.sqr();
-  const F PPP = P * PP;
-  const F Q = p.X * PP;
-  XYZZ<F> r;
-  r.X = R.sqr() - PPP - Q.dbl();
-  r.Y = R * (Q - r.X) - p.Y * PPP;
-  r.ZZ = p.ZZ * PP;
-  r.ZZZ = p.ZZZ * PPP;
-  return r;
-#endif
 }
 
 // add-2008-s: p + q, both XYZZ
-template <class F>
+template <class F, bool PAIR = (CSB_PAIRED != 0)>
 CSB_DEV XYZZ<F> xyzz_add(const XYZZ<F>& p, const XYZZ<F>& q) {
   if (p.is_inf()) return q;
   if (q.is_inf()) return p;
-#if CSB_PAIRED
-  F U1, U2, S1, S2;
-  F::mul2(p.X, q.ZZ, q.X, p.ZZ, U1, U2);
-  F::mul2(p.Y, q.ZZZ, q.Y, p.ZZZ, S1, S2);
-  const F P = U2 - U1;
-  const F R = S2 - S1;
-  if (P.is_zero()) {
-    if (R.is_zero()) return xyzz_dbl(p);
-    return XYZZ<F>::inf();
+  if constexpr (PAIR) {
+    using O = PairOps<F, true>;
+    F U1, U2, S1, S2;
+    O::mul2(p.X, q.ZZ, q.X, p.ZZ, U1, U2);
+    O::mul2(p.Y, q.ZZZ, q.Y, p.ZZZ, S1, S2);
+    const F P = U2 - U1;
+    const F R = S2 - S1;
+    if (P.is_zero()) {
+      if (R.is_zero()) return xyzz_dbl<F, true>(p);
+      return XYZZ<F>::inf();
+    }
+    F PP, RR, PPP, Q, T1, T2, Z2, Z3;
+    O::sqr2(P, R, PP, RR);
+    O::mul2(P, PP, U1, PP, PPP, Q);
+    XYZZ<F> r;
+    r.X = RR - PPP - Q.dbl();
+    O::mul2(R, Q - r.X, S1, PPP, T1, T2);
+    r.Y = T1 - T2;
+    O::mul2(p.ZZ, q.ZZ, p.ZZZ, q.ZZZ, Z2, Z3);
+    O::mul2(Z2, PP, Z3, PPP, r.ZZ, r.ZZZ);
+    return r;
+  } else {
+    const F U1 = p.X * q.ZZ;
+    const F U2 = q.X * p.ZZ;
+    const F S1 = p.Y * q.ZZZ;
+    const F S2 = q.Y * p.ZZZ;
+    const F P = U2 - U1;
+    const F R = S2 - S1;
+    if (P.is_zero()) {
+      if (R.is_zero()) return xyzz_dbl<F, false>(p);
+      return XYZZ<F>::inf();
+    }
+    const F PP = P.sqr();
+    const F PPP = P * PP;
+    const F Q = U1 * PP;
+    XYZZ<F> r;
+    r.X = R.sqr() - PPP - Q.dbl();
+    r.Y = R * (Q - r.X) - S1 * PPP;
+    r.ZZ = p.ZZ * q.ZZ * PP;
+    r.ZZZ = p.ZZZ * q.ZZZ * PPP;
+    return r;
   }
-  F PP, RR, PPP, Q, T1, T2, Z2, Z3;
-  F::sqr2(P, R, PP, RR);
-  F::mul2(P, PP, U1, PP, PPP, Q);
-  XYZZ<F> r;
-  r.X = RR - PPP - Q.dbl();
-  F::mul2(R, Q - r.X, S1, PPP, T1, T2);
-  r.Y = T1 - T2;
-  F::mul2(p.ZZ, q.ZZ, p.ZZZ, q.ZZZ, Z2, Z3);
-  F::mul2(Z2, PP, Z3, PPP, r.ZZ, r.ZZZ);
-  return r;
-#else
-  const F U1 = p.X * q.ZZ;
-  const F U2 = q.X * p.ZZ;
-  const F S1 = p.Y * q.ZZZ;
-  const F S2 = q.Y * p.ZZZ;
-  const F P = U2 - U1;
-  const F R = S2 - S1;
-  if (P.is_zero()) {
-    if (R.is_zero()) return xyzz_dbl(p);
-    return XYZZ<F>::inf();
-  }
-  const F PP = P.sqr();
-  const F PPP = P * PP;
-  const F Q = U1 * PP;
-  XYZZ<F> r;
-  r.X = R.sqr() - PPP - Q.dbl();
-  r.Y = R * (Q - r.X) - S1 * PPP;
-  r.ZZ = p.ZZ * q.ZZ * PP;
-  r.ZZZ = p.ZZZ * q.ZZZ * PPP;
-  return r;
-#endif
 }
 
 // Out-of-line copies for kernels whose cost is latency, not throughput (bucket-sum
@@ -182,6 +198,19 @@ template <class F>
 __device__ __noinline__ XYZZ<F> xyzz_add_cold(const XYZZ<F> p, const XYZZ<F> q) { return xyzz_add(p, q); }
 template <class F>
 __device__ __noinline__ XYZZ<F> xyzz_dbl_cold(const XYZZ<F> p) { return xyzz_dbl(p); }
+// The same with paired out-of-line products (small code for a single-thread chain in a unit
+// whose products are inlined: the proof's GLV scalar multiplication, 2^12 proof 3.52 ->
+// 3.47 ms).  A pair costs about two products' latency: the two carry-flag chains do not
+// overlap, so the window Horner of the MSM units keeps single calls.
+#ifndef CSB_LAT_PAIR
+#define CSB_LAT_PAIR 1
+#endif
+template <class F>
+__device__ __noinline__ XYZZ<F> xyzz_add_lat(const XYZZ<F> p, const XYZZ<F> q) {
+  return xyzz_add<F, CSB_LAT_PAIR != 0>(p, q);
+}
+template <class F>
+__device__ __noinline__ XYZZ<F> xyzz_dbl_lat(const XYZZ<F> p) { return xyzz_dbl<F, CSB_LAT_PAIR != 0>(p); }
 
 template <class F>
 CSB_DEV XYZZ<F> xyzz_neg(const XYZZ<F>& p) {

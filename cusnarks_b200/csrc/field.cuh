@@ -246,13 +246,20 @@ struct Fp {
     for (int i = 0; i < 8; i++) { x.v[i] = r8[i]; y.v[i] = s8[i]; }
   }
 
-  // x = a*b, y = c*d.  In the MSM units (out-of-line products) one call computes both
-  // with interleaved rows; elsewhere the inlined products are scheduled together anyway.
-  static CSB_DEV void mul2(const Fp& a, const Fp& b, const Fp& c, const Fp& d, Fp& x, Fp& y) {
-#if CSB_PAIRED
+  // x = a*b, y = c*d in one out-of-line call with interleaved rows (any unit): about the
+  // latency of one product for two, where a single thread's chain is the cost.
+  static CSB_DEV void mul2_ool(const Fp& a, const Fp& b, const Fp& c, const Fp& d, Fp& x, Fp& y) {
     const FpPair<M> r = fp_mul2_call<M>(a, b, c, d);
     x = r.x;
     y = r.y;
+  }
+  static CSB_DEV void sqr2_ool(const Fp& a, const Fp& c, Fp& x, Fp& y) { mul2_ool(a, a, c, c, x, y); }
+
+  // x = a*b, y = c*d.  With CSB_PAIR one out-of-line call computes both with interleaved
+  // rows; otherwise two products (inlined ones are scheduled together anyway).
+  static CSB_DEV void mul2(const Fp& a, const Fp& b, const Fp& c, const Fp& d, Fp& x, Fp& y) {
+#if CSB_PAIRED
+    mul2_ool(a, b, c, d, x, y);
 #else
     const Fp xx = a * b;
     y = c * d;
@@ -528,33 +535,39 @@ struct Fq2 {
     return {v0 - v1, s - v0 - v1};
 #endif
   }
-  // x = a*b, y = c*d: six Fq products as three interleaved pairs
+  // x = a*b, y = c*d: six Fq products as three interleaved out-of-line pairs
+  static CSB_DEV void mul2_ool(const Fq2& a, const Fq2& b, const Fq2& c, const Fq2& d, Fq2& x, Fq2& y) {
+    Fq a0, a1, c0, c1, sa, sc;
+    Fq::mul2_ool(a.c0, b.c0, a.c1, b.c1, a0, a1);
+    Fq::mul2_ool(c.c0, d.c0, c.c1, d.c1, c0, c1);
+    Fq::mul2_ool(a.c0 + a.c1, b.c0 + b.c1, c.c0 + c.c1, d.c0 + d.c1, sa, sc);
+    x = {a0 - a1, sa - a0 - a1};
+    y = {c0 - c1, sc - c0 - c1};
+  }
+  // x = a^2, y = c^2: four Fq products as two out-of-line pairs
+  static CSB_DEV void sqr2_ool(const Fq2& a, const Fq2& c, Fq2& x, Fq2& y) {
+    Fq pa, pc, qa, qc;
+    Fq::mul2_ool(a.c0, a.c1, c.c0, c.c1, pa, pc);
+    Fq::mul2_ool(a.c0 + a.c1, a.c0 - a.c1, c.c0 + c.c1, c.c0 - c.c1, qa, qc);
+    x = {qa, pa + pa};
+    y = {qc, pc + pc};
+  }
   static CSB_DEV void mul2(const Fq2& a, const Fq2& b, const Fq2& c, const Fq2& d, Fq2& x, Fq2& y) {
-#if !CSB_PAIRED
+#if CSB_PAIRED
+    mul2_ool(a, b, c, d, x, y);
+#else
     const Fq2 xx = a * b;
     y = c * d;
     x = xx;
-#else
-    Fq a0, a1, c0, c1, sa, sc;
-    Fq::mul2(a.c0, b.c0, a.c1, b.c1, a0, a1);
-    Fq::mul2(c.c0, d.c0, c.c1, d.c1, c0, c1);
-    Fq::mul2(a.c0 + a.c1, b.c0 + b.c1, c.c0 + c.c1, d.c0 + d.c1, sa, sc);
-    x = {a0 - a1, sa - a0 - a1};
-    y = {c0 - c1, sc - c0 - c1};
 #endif
   }
-  // x = a^2, y = c^2: four Fq products as two pairs
   static CSB_DEV void sqr2(const Fq2& a, const Fq2& c, Fq2& x, Fq2& y) {
-#if !CSB_PAIRED
+#if CSB_PAIRED
+    sqr2_ool(a, c, x, y);
+#else
     const Fq2 xx = a.sqr();
     y = c.sqr();
     x = xx;
-#else
-    Fq pa, pc, qa, qc;
-    Fq::mul2(a.c0, a.c1, c.c0, c.c1, pa, pc);
-    Fq::mul2(a.c0 + a.c1, a.c0 - a.c1, c.c0 + c.c1, c.c0 - c.c1, qa, qc);
-    x = {qa, pa + pa};
-    y = {qc, pc + pc};
 #endif
   }
   // Karatsuba with lazy reduction: three 512-bit products, two Montgomery reductions.

@@ -217,11 +217,11 @@ __global__ void k_scale_point_glv(const uint32_t* __restrict__ P, const GlvSplit
     if (g.neg2) q.y = q.y.neg();
     const XYZZ<Fq> pq = xyzz_madd(XYZZ<Fq>::from_affine(p), q);  // P + phi(P) (never infinity)
     for (int b = 127; b >= 0; b--) {
-      acc = xyzz_dbl_cold(acc);
+      acc = xyzz_dbl_lat(acc);
       const uint32_t e1 = (g.k1[b >> 5] >> (b & 31)) & 1u, e2 = (g.k2[b >> 5] >> (b & 31)) & 1u;
-      if (e1 && e2) acc = xyzz_add_cold(acc, pq);
-      else if (e1) acc = xyzz_add_cold(acc, XYZZ<Fq>::from_affine(p));
-      else if (e2) acc = xyzz_add_cold(acc, XYZZ<Fq>::from_affine(q));
+      if (e1 && e2) acc = xyzz_add_lat(acc, pq);
+      else if (e1) acc = xyzz_add_lat(acc, XYZZ<Fq>::from_affine(p));
+      else if (e2) acc = xyzz_add_lat(acc, XYZZ<Fq>::from_affine(q));
     }
   }
   st_xyzz<Fq>(out, acc);
