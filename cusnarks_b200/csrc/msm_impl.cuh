@@ -538,15 +538,17 @@ __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restri
 template <class F>
 __global__ void k_finish(const uint32_t* __restrict__ wsum, int W, int c, uint32_t* __restrict__ out) {
   constexpr int XW = 4 * FieldWords<F>::value;
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (blockIdx.x != 0) return;
+  // one warp (launched with 32 threads): the independent products of each doubling and
+  // addition run on separate lanes
   XYZZ<F> r = ld_xyzz<F>(wsum + (size_t)(W - 1) * XW);
 #pragma unroll 1
   for (int j = W - 2; j >= 0; j--) {
 #pragma unroll 1
-    for (int d = 0; d < c; d++) r = xyzz_dbl_cold(r);
-    r = xyzz_add_cold(r, ld_xyzz<F>(wsum + (size_t)j * XW));
+    for (int d = 0; d < c; d++) r = xyzz_dbl_warp(r);
+    r = xyzz_add_warp(r, ld_xyzz<F>(wsum + (size_t)j * XW));
   }
-  st_affine<F>(out, xyzz_to_affine(r));
+  if (threadIdx.x == 0) st_affine<F>(out, xyzz_to_affine(r));
 }
 
 template <class F>

@@ -203,9 +203,10 @@ inline GlvSplit split(const uint32_t* k32) {
 }  // namespace glv
 
 // out (XYZZ) = k * P for P affine (G1), k given as its GLV split.
+// One warp (launched with 32 threads): the independent products of each doubling and
+// addition run on separate lanes; lane 0 stores.
 __global__ void k_scale_point_glv(const uint32_t* __restrict__ P, const GlvSplit* __restrict__ gs,
                                   uint32_t* __restrict__ out) {
-  if (threadIdx.x != 0) return;
   const Fq beta{{0xd782e155u, 0x71930c11u, 0xffbe3323u, 0xa6bb947cu, 0xd4741444u, 0xaa303344u, 0x26594943u,
                  0x2c3b3f0du}};
   const GlvSplit g = *gs;
@@ -217,14 +218,14 @@ __global__ void k_scale_point_glv(const uint32_t* __restrict__ P, const GlvSplit
     if (g.neg2) q.y = q.y.neg();
     const XYZZ<Fq> pq = xyzz_madd(XYZZ<Fq>::from_affine(p), q);  // P + phi(P) (never infinity)
     for (int b = 127; b >= 0; b--) {
-      acc = xyzz_dbl_lat(acc);
+      acc = xyzz_dbl_warp(acc);
       const uint32_t e1 = (g.k1[b >> 5] >> (b & 31)) & 1u, e2 = (g.k2[b >> 5] >> (b & 31)) & 1u;
-      if (e1 && e2) acc = xyzz_add_lat(acc, pq);
-      else if (e1) acc = xyzz_add_lat(acc, XYZZ<Fq>::from_affine(p));
-      else if (e2) acc = xyzz_add_lat(acc, XYZZ<Fq>::from_affine(q));
+      if (e1 && e2) acc = xyzz_add_warp(acc, pq);
+      else if (e1) acc = xyzz_add_warp(acc, XYZZ<Fq>::from_affine(p));
+      else if (e2) acc = xyzz_add_warp(acc, XYZZ<Fq>::from_affine(q));
     }
   }
-  st_xyzz<Fq>(out, acc);
+  if (threadIdx.x == 0) st_xyzz<Fq>(out, acc);
 }
 
 // pi_C = C2 + C + sA + rB1 (C2, C affine; sA, rB1 XYZZ) -> affine
