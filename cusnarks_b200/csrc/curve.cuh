@@ -212,82 +212,102 @@ __device__ __noinline__ XYZZ<F> xyzz_add_lat(const XYZZ<F> p, const XYZZ<F> q) {
 template <class F>
 __device__ __noinline__ XYZZ<F> xyzz_dbl_lat(const XYZZ<F> p) { return xyzz_dbl<F, CSB_LAT_PAIR != 0>(p); }
 
-// ------------------------------------------------ warp-parallel point operations -----
-// For chains that one point runs through alone (window Horner, scalar multiplication): the
-// 32 lanes of a warp hold the same point and each computes one of the independent products
-// of a dependency level, so a doubling costs 3 product latencies instead of 9 and an
-// addition 4 instead of 14.  Every lane of the warp must call these (full-mask shuffles);
-// all lanes return the same result.
+// ------------------------------------------------ quad-parallel point operations -----
+// For chains that a point runs through alone (window Horner, scalar multiplication, the
+// buckets of a small MSM): the 4 lanes of an aligned quad hold the same point and each
+// computes one of the independent products of a dependency level, so a doubling costs 3
+// product latencies instead of 9, an addition 4 instead of 14 and a mixed addition 4
+// instead of 10.  The shuffles use the full warp mask, so every lane of the warp must call
+// these together (the 8 quads may hold different points: the special cases -- infinity,
+// equal or opposite points -- are selected after the general formula, never branched
+// around it); every lane of a quad returns the same result.
 template <class F>
-CSB_DEV F warp_bcast(const F& v, int src) {
+CSB_DEV F quad_bcast(const F& v, int src) {
   constexpr int FW = sizeof(F) / 4;
   F o;
   uint32_t* ow = reinterpret_cast<uint32_t*>(&o);
   const uint32_t* vw = reinterpret_cast<const uint32_t*>(&v);
 #pragma unroll
-  for (int w = 0; w < FW; w++) ow[w] = __shfl_sync(0xffffffffu, vw[w], src);
+  for (int w = 0; w < FW; w++) ow[w] = __shfl_sync(0xffffffffu, vw[w], src, 4);
   return o;
 }
 
 template <class F>
-CSB_DEV F pick4(int lane, const F& v0, const F& v1, const F& v2, const F& v3) {
-  return lane == 0 ? v0 : lane == 1 ? v1 : lane == 2 ? v2 : v3;
+CSB_DEV F pick4(int k, const F& v0, const F& v1, const F& v2, const F& v3) {
+  return k == 0 ? v0 : k == 1 ? v1 : k == 2 ? v2 : v3;
 }
 
-// lane i < 4 computes a_i * b_i; returns the four products to every lane
 template <class F>
-CSB_DEV void warp_mul4(const F& a0, const F& b0, const F& a1, const F& b1, const F& a2, const F& b2,
+CSB_DEV XYZZ<F> xyzz_select(bool c, const XYZZ<F>& a, const XYZZ<F>& b) { return c ? a : b; }
+
+// quad lane k computes a_k * b_k; every lane gets the four products
+template <class F>
+CSB_DEV void quad_mul4(const F& a0, const F& b0, const F& a1, const F& b1, const F& a2, const F& b2,
                        const F& a3, const F& b3, F& r0, F& r1, F& r2, F& r3) {
-  const int lane = threadIdx.x & 31;
-  const int k = lane & 3;
+  const int k = threadIdx.x & 3;
   const F r = pick4(k, a0, a1, a2, a3) * pick4(k, b0, b1, b2, b3);
-  r0 = warp_bcast(r, 0);
-  r1 = warp_bcast(r, 1);
-  r2 = warp_bcast(r, 2);
-  r3 = warp_bcast(r, 3);
+  r0 = quad_bcast(r, 0);
+  r1 = quad_bcast(r, 1);
+  r2 = quad_bcast(r, 2);
+  r3 = quad_bcast(r, 3);
 }
 
 // dbl-2008-s-1, three levels of products
 template <class F>
-CSB_DEV XYZZ<F> xyzz_dbl_warp(const XYZZ<F>& p) {
-  if (p.is_inf()) return p;
+CSB_DEV XYZZ<F> xyzz_dbl_quad(const XYZZ<F>& p) {
   const F U = p.Y.dbl();
   F V, X2, W, S, MM, ZZ3, T1, T2, ZZZ3, unused;
-  warp_mul4(U, U, p.X, p.X, U, U, p.X, p.X, V, X2, unused, unused);
+  quad_mul4(U, U, p.X, p.X, U, U, p.X, p.X, V, X2, unused, unused);
   const F M = X2.dbl() + X2;
-  warp_mul4(U, V, p.X, V, M, M, V, p.ZZ, W, S, MM, ZZ3);
+  quad_mul4(U, V, p.X, V, M, M, V, p.ZZ, W, S, MM, ZZ3);
   XYZZ<F> r;
   r.X = MM - S.dbl();
-  warp_mul4(M, S - r.X, W, p.Y, W, p.ZZZ, W, p.ZZZ, T1, T2, ZZZ3, unused);
+  quad_mul4(M, S - r.X, W, p.Y, W, p.ZZZ, W, p.ZZZ, T1, T2, ZZZ3, unused);
   r.Y = T1 - T2;
   r.ZZ = ZZ3;
   r.ZZZ = ZZZ3;
-  return r;
+  return xyzz_select(p.is_inf(), p, r);
 }
 
 // add-2008-s, four levels of products
 template <class F>
-CSB_DEV XYZZ<F> xyzz_add_warp(const XYZZ<F>& p, const XYZZ<F>& q) {
-  if (p.is_inf()) return q;
-  if (q.is_inf()) return p;
+CSB_DEV XYZZ<F> xyzz_add_quad(const XYZZ<F>& p, const XYZZ<F>& q) {
   F U1, U2, S1, S2;
-  warp_mul4(p.X, q.ZZ, q.X, p.ZZ, p.Y, q.ZZZ, q.Y, p.ZZZ, U1, U2, S1, S2);
+  quad_mul4(p.X, q.ZZ, q.X, p.ZZ, p.Y, q.ZZZ, q.Y, p.ZZZ, U1, U2, S1, S2);
   const F P = U2 - U1;
   const F R = S2 - S1;
-  if (P.is_zero()) {
-    if (R.is_zero()) return xyzz_dbl_warp(p);
-    return XYZZ<F>::inf();
-  }
   F PP, RR, Z2, Z3, PPP, Q, ZZ3, ZZZ3, T1, T2, unused;
-  warp_mul4(P, P, R, R, p.ZZ, q.ZZ, p.ZZZ, q.ZZZ, PP, RR, Z2, Z3);
-  warp_mul4(P, PP, U1, PP, Z2, PP, Z3, P, PPP, Q, ZZ3, unused);
+  quad_mul4(P, P, R, R, p.ZZ, q.ZZ, p.ZZZ, q.ZZZ, PP, RR, Z2, Z3);
+  quad_mul4(P, PP, U1, PP, Z2, PP, Z3, P, PPP, Q, ZZ3, unused);
   XYZZ<F> r;
   r.X = RR - PPP - Q.dbl();
-  warp_mul4(R, Q - r.X, S1, PPP, Z3, PPP, Z3, PPP, T1, T2, ZZZ3, unused);
+  quad_mul4(R, Q - r.X, S1, PPP, Z3, PPP, Z3, PPP, T1, T2, ZZZ3, unused);
   r.Y = T1 - T2;
   r.ZZ = ZZ3;
   r.ZZZ = ZZZ3;
-  return r;
+  if (P.is_zero() && !p.is_inf() && !q.is_inf())  // equal or opposite points (rare): no shuffles
+    r = R.is_zero() ? xyzz_dbl<F, false>(p) : XYZZ<F>::inf();
+  return p.is_inf() ? q : (q.is_inf() ? p : r);
+}
+
+// madd-2008-s, four levels of products
+template <class F>
+CSB_DEV XYZZ<F> xyzz_madd_quad(const XYZZ<F>& p, const Affine<F>& q) {
+  F U2, S2, PP, RR, PPP, Q, ZZ3, T1, T2, ZZZ3, unused;
+  quad_mul4(q.x, p.ZZ, q.y, p.ZZZ, q.x, p.ZZ, q.y, p.ZZZ, U2, S2, unused, unused);
+  const F P = U2 - p.X;
+  const F R = S2 - p.Y;
+  quad_mul4(P, P, R, R, P, P, R, R, PP, RR, unused, unused);
+  quad_mul4(P, PP, p.X, PP, p.ZZ, PP, p.ZZ, PP, PPP, Q, ZZ3, unused);
+  XYZZ<F> r;
+  r.X = RR - PPP - Q.dbl();
+  quad_mul4(R, Q - r.X, p.Y, PPP, p.ZZZ, PPP, p.ZZZ, PPP, T1, T2, ZZZ3, unused);
+  r.Y = T1 - T2;
+  r.ZZ = ZZ3;
+  r.ZZZ = ZZZ3;
+  if (P.is_zero() && !p.is_inf())  // equal or opposite points (rare): no shuffles
+    r = R.is_zero() ? xyzz_mdbl(q) : XYZZ<F>::inf();
+  return p.is_inf() ? XYZZ<F>::from_affine(q) : r;
 }
 
 template <class F>

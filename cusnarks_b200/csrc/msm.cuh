@@ -75,10 +75,6 @@ struct MsmConfig {
   int c = 0;          // window bits; 0 = pick from N
   int task = 64;      // max points per accumulation task
   int affine = -1;    // batch-affine halving rounds before the XYZZ accumulation: -1 auto, 0 off
-  // bucket-reduction levels above level 0: 1 = one thread per 8 segments (least work: for
-  // proofs and batches, where other MSMs fill the GPU), 0 = 8 lanes per segment (shortest
-  // dependent chain: for a lone MSM), -1 = auto (1 for G1, 0 for G2)
-  int reduce_serial = -1;
   // optional events recorded around the bucket-accumulation kernels (phase timing)
   cudaEvent_t acc_start = nullptr, acc_stop = nullptr;
 };

@@ -12,7 +12,7 @@
 //     the work is split by bucket size, not by instance, so a 2^10 instance next to a 2^20
 //     one costs its share and no launch;
 //   * reduction per window group (instances with equal c are contiguous: one level chain and
-//     one k_window_sum launch per distinct c), and k_bfinish: one thread per instance for the
+//     one k_window_sum launch per distinct c), and k_bfinish: one warp per instance for the
 //     window Horner and the affine result.
 // The sequence contains no allocation and no host synchronisation, so it can be captured in a
 // CUDA graph once and replayed (cs_msm_batch_run).
@@ -64,22 +64,23 @@ __global__ void k_bscatter(const BatchJob* __restrict__ jobs, uint32_t njobs, ui
   });
 }
 
-// One thread per instance: sum_j 2^(c j) S_j over its windows, affine result.
+// One warp per instance (quad point operations; the warp's 8 quads compute the same):
+// sum_j 2^(c j) S_j over its windows, affine result.
 template <class F>
 __global__ void k_bfinish(const BatchJob* __restrict__ jobs, uint32_t njobs, const uint32_t* __restrict__ wsum) {
   constexpr int XW = 4 * FieldWords<F>::value;
-  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= njobs) return;
+  const uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (q >= njobs) return;  // whole warps leave together
   const BatchJob jb = jobs[q];
   const uint32_t* w = wsum + (size_t)jb.window0 * XW;
   XYZZ<F> r = ld_xyzz<F>(w + (size_t)(jb.W - 1) * XW);
 #pragma unroll 1
   for (int j = (int)jb.W - 2; j >= 0; j--) {
 #pragma unroll 1
-    for (uint32_t d = 0; d < jb.c; d++) r = xyzz_dbl_cold(r);
-    r = xyzz_add_cold(r, ld_xyzz<F>(w + (size_t)j * XW));
+    for (uint32_t d = 0; d < jb.c; d++) r = xyzz_dbl_quad(r);
+    r = xyzz_add_quad(r, ld_xyzz<F>(w + (size_t)j * XW));
   }
-  st_affine<F>(jb.out, xyzz_to_affine(r));
+  if ((threadIdx.x & 31) == 0) st_affine<F>(jb.out, xyzz_to_affine(r));
 }
 
 struct BatchLayout {
@@ -158,27 +159,19 @@ cudaError_t batch_impl(const MsmBatch& b, void* d_work, size_t work_bytes, cudaS
   k_combine_small<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);
   k_combine<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);
   note_launch(3);
+  const uint64_t resident = (uint64_t)accumulate_grid<F>(sms) * 128;
   // reduction per window group
   for (uint32_t g = 0; g < b.ngroups; g++) {
     const BatchGroup& G = b.groups[g];
     const uint32_t B = 1u << (G.c - 1);
     const uint32_t WR = G.windows;
     uint32_t nseg = (B + 7) / 8;
-    k_reduce_level<F><<<(WR * nseg + 127) / 128, 128, 0, st>>>(buckets + (size_t)G.bucket0 * XWD, nullptr, B, nseg,
-                                                               (int)WR, 0, lv_y, lv_z);
-    note_launch();
+    reduce_level<F>(buckets + (size_t)G.bucket0 * XWD, nullptr, B, nseg, (int)WR, 0, lv_y, lv_z, resident, st);
     int levels = 1;
     uint32_t *y = lv_y, *z = lv_z, *y2 = lv_y2, *z2 = lv_z2;
     while (nseg > kTopSegments) {
       const uint32_t nnext = (nseg + 7) / 8;
-      const uint32_t threads = WR * nnext * 8;
-      // large levels one thread per 8 segments (least work: the batch's groups fill the GPU),
-      // small top levels cooperative (short chains)
-      if ((uint64_t)WR * nseg > kSerialMinSegments)
-        k_reduce_level<F><<<(WR * nnext + 127) / 128, 128, 0, st>>>(y, z, nseg, nnext, (int)WR, levels, y2, z2);
-      else
-        k_reduce_level_coop<F><<<(threads + 127) / 128, 128, 0, st>>>(y, z, nseg, nnext, (int)WR, levels, y2, z2);
-      note_launch();
+      reduce_level<F>(y, z, nseg, nnext, (int)WR, levels, y2, z2, resident, st);
       uint32_t* ty = y; y = y2; y2 = ty;
       uint32_t* tz = z; z = z2; z2 = tz;
       nseg = nnext;
@@ -187,7 +180,7 @@ cudaError_t batch_impl(const MsmBatch& b, void* d_work, size_t work_bytes, cudaS
     k_window_sum<F, 256><<<WR, 256, 0, st>>>(y, z, nseg, 3 * levels, wsum + (size_t)G.window0 * XWD);
     note_launch();
   }
-  k_bfinish<F><<<(b.njobs + 31) / 32, 32, 0, st>>>(b.d_jobs, b.njobs, wsum);
+  k_bfinish<F><<<(32 * b.njobs + 127) / 128, 128, 0, st>>>(b.d_jobs, b.njobs, wsum);
   note_launch();
   return cudaGetLastError();
 }

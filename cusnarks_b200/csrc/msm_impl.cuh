@@ -2,7 +2,6 @@
 // instantiated for G1 in msm_g1.cu and for G2 in msm_g2.cu.
 #pragma once
 #include <algorithm>
-#include <type_traits>
 #include "msm.cuh"
 #include "curve.cuh"
 #include "scan.cuh"
@@ -269,6 +268,51 @@ __global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate(cons
   }
 }
 
+// Latency form of k_accumulate for an MSM too small to fill the GPU: one quad per task, each
+// lane computing one product of each level of the mixed addition (4 product latencies per
+// addition instead of 10).  Same tasks, same results.  The quad operations shuffle across
+// the whole warp, so the 8 quads of a warp step together: each walks the longest of the
+// warp's 8 tasks and keeps its accumulator past its own task's end (tasks are emitted
+// longest first, so neighbours are about as long).
+template <class F>
+__global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate_quad(
+    const Task* __restrict__ tasks, const uint32_t* __restrict__ counters, const uint32_t* __restrict__ entries,
+    const uint32_t* __restrict__ points, uint32_t nb, uint32_t* __restrict__ buckets,
+    uint32_t* __restrict__ partials) {
+  constexpr int PW = 2 * FieldWords<F>::value;
+  constexpr int XW = 4 * FieldWords<F>::value;
+  const uint32_t ntasks = counters[0];
+  const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t qw = (threadIdx.x & 31) >> 2;  // quad within the warp
+  for (uint32_t base = warp0 * 8; base < ntasks; base += nwarps * 8) {  // warp-uniform
+    const uint32_t t = base + qw;
+    const bool valid = t < ntasks;
+    const Task tk = valid ? tasks[t] : Task{0, 0, 0, 0};
+    const uint32_t steps = __reduce_max_sync(0xffffffffu, tk.len);
+    XYZZ<F> acc = XYZZ<F>::inf();
+#pragma unroll 1
+    for (uint32_t e = 0; e < steps; e++) {
+      const bool live = e < tk.len;
+      Affine<F> p;
+      if (entries) {
+        const uint32_t ent = live ? entries[tk.start + e] : 0u;
+        p = ld_affine<F>(points + (size_t)(ent & ~NEG_BIT) * PW);
+        if (ent & NEG_BIT) p.y = p.y.neg();
+      } else {
+        p = ld_affine<F>(points + (size_t)(live ? tk.start + e : 0u) * PW);
+      }
+      const XYZZ<F> nxt = xyzz_madd_quad(acc, p);
+      const bool take = live && (entries || !(p.x.is_zero() && p.y.is_zero()));
+      acc = xyzz_select(take, nxt, acc);
+    }
+    if (valid && (threadIdx.x & 3) == 0) {
+      uint32_t* dst = tk.dst < nb ? buckets + (size_t)tk.dst * XW : partials + (size_t)(tk.dst - nb) * XW;
+      st_xyzz<F>(dst, acc);
+    }
+  }
+}
+
 // Split buckets with at most kCombineSerial partials: one thread each, a serial sum.
 // (The top window of a scalar has fewer bits, so its digits crowd into fewer buckets and
 // many of those split into two or three tasks.)
@@ -377,6 +421,49 @@ __global__ void __launch_bounds__(128) k_reduce_level(const uint32_t* __restrict
 }
 
 
+// k_reduce_level with one quad per output segment (quad point operations): the latency form
+// for levels too small to fill the GPU.  Every lane of a launched warp runs the operations
+// (quads past the end work on points at infinity and store nothing).
+template <class F>
+__global__ void __launch_bounds__(128) k_reduce_level_quad(const uint32_t* __restrict__ y,
+                                                           const uint32_t* __restrict__ z, uint32_t n,
+                                                           uint32_t nout, int W, int level,
+                                                           uint32_t* __restrict__ yout,
+                                                           uint32_t* __restrict__ zout) {
+  constexpr int XW = 4 * FieldWords<F>::value;
+  const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 2;
+  const bool valid = g < (uint32_t)W * nout;
+  const uint32_t j = valid ? g / nout : 0u, t = valid ? g % nout : 0u;
+  const uint32_t* yj = y + (size_t)j * n * XW;
+  XYZZ<F> acc = XYZZ<F>::inf(), s = XYZZ<F>::inf();
+#pragma unroll 1
+  for (int i = 7; i >= 1; i--) {
+    const uint32_t idx = 8 * t + i;
+    const XYZZ<F> v = valid && idx < n ? ld_xyzz<F>(yj + (size_t)idx * XW) : XYZZ<F>::inf();
+    acc = xyzz_add_quad(acc, v);
+    s = xyzz_add_quad(s, acc);
+  }
+  {
+    const XYZZ<F> v = valid && 8 * t < n ? ld_xyzz<F>(yj + (size_t)(8 * t) * XW) : XYZZ<F>::inf();
+    acc = xyzz_add_quad(acc, v);
+  }
+#pragma unroll 1
+  for (int d = 0; d < 3 * level; d++) s = xyzz_dbl_quad(s);
+  if (z) {  // uniform: a kernel argument
+    const uint32_t* zj = z + (size_t)j * n * XW;
+#pragma unroll 1
+    for (int i = 0; i < 8; i++) {
+      const uint32_t idx = 8 * t + i;
+      const XYZZ<F> v = valid && idx < n ? ld_xyzz<F>(zj + (size_t)idx * XW) : XYZZ<F>::inf();
+      s = xyzz_add_quad(s, v);
+    }
+  }
+  if (valid && (threadIdx.x & 3) == 0) {
+    st_xyzz<F>(yout + ((size_t)j * nout + t) * XW, acc);
+    st_xyzz<F>(zout + ((size_t)j * nout + t) * XW, s);
+  }
+}
+
 template <class F>
 CSB_DEV XYZZ<F> shfl_down_xyzz(const XYZZ<F>& v, int d) {
   constexpr int XW = 4 * FieldWords<F>::value;
@@ -386,50 +473,6 @@ CSB_DEV XYZZ<F> shfl_down_xyzz(const XYZZ<F>& v, int d) {
 #pragma unroll
   for (int w = 0; w < XW; w++) ow[w] = __shfl_down_sync(0xffffffffu, vw[w], d);
   return o;
-}
-
-// Level k >= 1, warp-cooperative: one thread per element, the 8 lanes 8t..8t+7 hold
-// segment t (segments never straddle a warp).  With suf_i = sum_{i' >= i} y_i' (a 3-step
-// shuffle scan), the segment total is suf_0 and sum_i i*y_i = sum_{i >= 1} suf_i (a 3-step
-// tree), so the dependent chain is about 7 + 3k point operations instead of 26 + 3k.
-// Outputs as k_reduce_level.  Every lane runs the shuffles (no early return).
-template <class F>
-__global__ void __launch_bounds__(128) k_reduce_level_coop(const uint32_t* __restrict__ y,
-                                                           const uint32_t* __restrict__ z, uint32_t n,
-                                                           uint32_t nout, int W, int level,
-                                                           uint32_t* __restrict__ yout,
-                                                           uint32_t* __restrict__ zout) {
-  constexpr int XW = 4 * FieldWords<F>::value;
-  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t per = nout * 8;  // padded elements per window
-  const uint32_t j = g / per, e = g % per, t = e >> 3;
-  const int i = (int)(e & 7);
-  const bool valid = j < (uint32_t)W && e < n;
-  const bool head = j < (uint32_t)W && i == 0;
-  const uint32_t* yj = y + (size_t)j * n * XW;
-  const uint32_t* zj = z + (size_t)j * n * XW;
-  XYZZ<F> suf = valid ? ld_xyzz<F>(yj + (size_t)e * XW) : XYZZ<F>::inf();
-#pragma unroll 1
-  for (int d = 1; d < 8; d <<= 1) {
-    const XYZZ<F> o = shfl_down_xyzz(suf, d);
-    if (i + d < 8) suf = xyzz_add(suf, o);
-  }
-  if (head) st_xyzz<F>(yout + ((size_t)j * nout + t) * XW, suf);
-  XYZZ<F> w = i >= 1 ? suf : XYZZ<F>::inf();
-#pragma unroll 1
-  for (int d = 4; d >= 1; d >>= 1) {
-    const XYZZ<F> o = shfl_down_xyzz(w, d);
-    if (i < d) w = xyzz_add(w, o);
-  }
-#pragma unroll 1
-  for (int k = 0; k < 3 * level; k++) w = xyzz_dbl(w);
-  XYZZ<F> zz = valid ? ld_xyzz<F>(zj + (size_t)e * XW) : XYZZ<F>::inf();
-#pragma unroll 1
-  for (int d = 4; d >= 1; d >>= 1) {
-    const XYZZ<F> o = shfl_down_xyzz(zz, d);
-    if (i < d) zz = xyzz_add(zz, o);
-  }
-  if (head) st_xyzz<F>(zout + ((size_t)j * nout + t) * XW, xyzz_add(zz, w));
 }
 
 // Per-window sum after levels 0..L-1.  With y_t the segment totals and z_t the weighted
@@ -443,59 +486,62 @@ template <class F, int THREADS>
 __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restrict__ y,
                                                         const uint32_t* __restrict__ z, uint32_t n1,
                                                         int shift, uint32_t* __restrict__ wsum) {
+  // Quad form: each quad of lanes is one virtual thread u running quad point operations, so
+  // the block has VT = THREADS / 4 virtual threads, 8 per warp.
   constexpr int XW = 4 * FieldWords<F>::value;
   constexpr int NW = THREADS / 32;
+  constexpr uint32_t VT = THREADS / 4;
+  static_assert(NW <= 8, "the warp totals are scanned by the 8 quads of one warp");
   __shared__ uint32_t sh[NW][XW];
   const int j = blockIdx.x;
   const uint32_t* yj = y + (size_t)j * n1 * XW;
   const uint32_t* zj = z + (size_t)j * n1 * XW;
-  const uint32_t E = (n1 + THREADS - 1) / THREADS;  // n1 is a power of two
-  const uint32_t u = threadIdx.x;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t E = (n1 + VT - 1) / VT;  // n1 is a power of two
+  const uint32_t u = threadIdx.x >> 2;
+  const int vl = (threadIdx.x & 31) >> 2, warp = threadIdx.x >> 5, q = threadIdx.x & 3;
   XYZZ<F> acc = XYZZ<F>::inf(), ws = XYZZ<F>::inf(), zs = XYZZ<F>::inf();
 #pragma unroll 1
-  for (int i = (int)E - 1; i >= 0; i--) {
+  for (int i = (int)E - 1; i >= 0; i--) {  // uniform trip count; past n1 the terms are infinity
     const uint32_t idx = u * E + i;
-    if (idx < n1) {
-      acc = xyzz_add_cold(acc, ld_xyzz<F>(yj + (size_t)idx * XW));
-      zs = xyzz_add_cold(zs, ld_xyzz<F>(zj + (size_t)idx * XW));
-    }
-    if (i > 0) ws = xyzz_add_cold(ws, acc);
+    const bool in = idx < n1;
+    acc = xyzz_add_quad(acc, in ? ld_xyzz<F>(yj + (size_t)idx * XW) : XYZZ<F>::inf());
+    zs = xyzz_add_quad(zs, in ? ld_xyzz<F>(zj + (size_t)idx * XW) : XYZZ<F>::inf());
+    if (i > 0) ws = xyzz_add_quad(ws, acc);
   }
   // V = acc + zs + 2^shift ws
 #pragma unroll 1
-  for (int d = 0; d < shift; d++) ws = xyzz_dbl_cold(ws);
-  XYZZ<F> V = xyzz_add_cold(xyzz_add_cold(acc, zs), ws);
-  // inclusive suffix scan of acc across the block
+  for (int d = 0; d < shift; d++) ws = xyzz_dbl_quad(ws);
+  XYZZ<F> V = xyzz_add_quad(xyzz_add_quad(acc, zs), ws);
+  // inclusive suffix scan of acc over the 8 virtual lanes of the warp
   XYZZ<F> suf = acc;
 #pragma unroll 1
-  for (int d = 1; d < 32; d <<= 1) {
-    const XYZZ<F> o = shfl_down_xyzz(suf, d);
-    if (lane + d < 32) suf = xyzz_add_cold(suf, o);
+  for (int d = 1; d < 8; d <<= 1) {
+    const XYZZ<F> o = shfl_down_xyzz(suf, 4 * d);
+    suf = xyzz_select(vl + d < 8, xyzz_add_quad(suf, o), suf);
   }
-  if (lane == 0) {
+  if (vl == 0 && q == 0) {
     const uint32_t* w = reinterpret_cast<const uint32_t*>(&suf);
     for (int k = 0; k < XW; k++) sh[warp][k] = w[k];
   }
   __syncthreads();
   if (warp == 0) {
     XYZZ<F> t = XYZZ<F>::inf();
-    if (lane < NW) {
+    if (vl < NW) {
       uint32_t* w = reinterpret_cast<uint32_t*>(&t);
-      for (int k = 0; k < XW; k++) w[k] = sh[lane][k];
+      for (int k = 0; k < XW; k++) w[k] = sh[vl][k];
     }
-    // exclusive suffix over warp totals: lane w gets sum of totals of warps > w
+    // exclusive suffix over warp totals: virtual lane w gets the totals of warps > w
 #pragma unroll 1
-    for (int d = 1; d < 32; d <<= 1) {
-      const XYZZ<F> o = shfl_down_xyzz(t, d);
-      if (lane + d < 32) t = xyzz_add_cold(t, o);
+    for (int d = 1; d < 8; d <<= 1) {
+      const XYZZ<F> o = shfl_down_xyzz(t, 4 * d);
+      t = xyzz_select(vl + d < 8, xyzz_add_quad(t, o), t);
     }
-    XYZZ<F> excl = shfl_down_xyzz(t, 1);
-    if (lane == 31) excl = XYZZ<F>::inf();
+    XYZZ<F> excl = shfl_down_xyzz(t, 4);
+    if (vl == 7) excl = XYZZ<F>::inf();
     __syncwarp();
-    if (lane < NW) {
+    if (vl < NW && q == 0) {
       const uint32_t* w = reinterpret_cast<const uint32_t*>(&excl);
-      for (int k = 0; k < XW; k++) sh[lane][k] = w[k];
+      for (int k = 0; k < XW; k++) sh[vl][k] = w[k];
     }
   }
   __syncthreads();
@@ -503,34 +549,40 @@ __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restri
     XYZZ<F> off;
     uint32_t* w = reinterpret_cast<uint32_t*>(&off);
     for (int k = 0; k < XW; k++) w[k] = sh[warp][k];
-    suf = xyzz_add_cold(suf, off);
+    suf = xyzz_add_quad(suf, off);
   }
   __syncthreads();
   // C_u = V_u + 2^shift E * Suf(u) for u >= 1 (E is a power of two)
-  if (u >= 1 && u * E < n1) {
+  {  // computed by every quad (uniform), kept where u >= 1 and u E < n1
 #pragma unroll 1
-    for (uint32_t m = E; m > 1; m >>= 1) suf = xyzz_dbl_cold(suf);
+    for (uint32_t m = E; m > 1; m >>= 1) suf = xyzz_dbl_quad(suf);
 #pragma unroll 1
-    for (int d = 0; d < shift; d++) suf = xyzz_dbl_cold(suf);
-    V = xyzz_add_cold(V, suf);
+    for (int d = 0; d < shift; d++) suf = xyzz_dbl_quad(suf);
+    V = xyzz_select(u >= 1 && u * E < n1, xyzz_add_quad(V, suf), V);
   }
-  // block reduction of V
+  // block reduction of V: over the warp's virtual lanes, then over the warps
 #pragma unroll 1
-  for (int d = 16; d > 0; d >>= 1) V = xyzz_add_cold(V, shfl_down_xyzz(V, d));
-  if (lane == 0) {
+  for (int d = 4; d > 0; d >>= 1) {
+    const XYZZ<F> o = shfl_down_xyzz(V, 4 * d);
+    V = xyzz_add_quad(V, o);  // virtual lanes >= 8 - d add stray values; only lane 0's sum is kept
+  }
+  if (vl == 0 && q == 0) {
     const uint32_t* w = reinterpret_cast<const uint32_t*>(&V);
     for (int k = 0; k < XW; k++) sh[warp][k] = w[k];
   }
   __syncthreads();
   if (warp == 0) {
     XYZZ<F> t = XYZZ<F>::inf();
-    if (lane < NW) {
+    if (vl < NW) {
       uint32_t* w = reinterpret_cast<uint32_t*>(&t);
-      for (int k = 0; k < XW; k++) w[k] = sh[lane][k];
+      for (int k = 0; k < XW; k++) w[k] = sh[vl][k];
     }
 #pragma unroll 1
-    for (int d = 16; d > 0; d >>= 1) t = xyzz_add_cold(t, shfl_down_xyzz(t, d));
-    if (lane == 0) st_xyzz<F>(wsum + (size_t)j * XW, t);
+    for (int d = 4; d > 0; d >>= 1) {
+      const XYZZ<F> o = shfl_down_xyzz(t, 4 * d);
+      t = xyzz_add_quad(t, o);
+    }
+    if (vl == 0 && q == 0) st_xyzz<F>(wsum + (size_t)j * XW, t);
   }
 }
 
@@ -539,14 +591,14 @@ template <class F>
 __global__ void k_finish(const uint32_t* __restrict__ wsum, int W, int c, uint32_t* __restrict__ out) {
   constexpr int XW = 4 * FieldWords<F>::value;
   if (blockIdx.x != 0) return;
-  // one warp (launched with 32 threads): the independent products of each doubling and
-  // addition run on separate lanes
+  // one warp (launched with 32 threads; its 8 quads compute the same): the independent
+  // products of each doubling and addition run on the lanes of a quad
   XYZZ<F> r = ld_xyzz<F>(wsum + (size_t)(W - 1) * XW);
 #pragma unroll 1
   for (int j = W - 2; j >= 0; j--) {
 #pragma unroll 1
-    for (int d = 0; d < c; d++) r = xyzz_dbl_warp(r);
-    r = xyzz_add_warp(r, ld_xyzz<F>(wsum + (size_t)j * XW));
+    for (int d = 0; d < c; d++) r = xyzz_dbl_quad(r);
+    r = xyzz_add_quad(r, ld_xyzz<F>(wsum + (size_t)j * XW));
   }
   if (threadIdx.x == 0) st_affine<F>(out, xyzz_to_affine(r));
 }
@@ -724,8 +776,6 @@ static __global__ void k_half_counts(const uint32_t* __restrict__ off, uint32_t 
 constexpr int kCtrHist = 16, kCtrCursor = 96, kCtrWords = 192;
 // the reduction adds levels until a window has at most this many segments
 constexpr uint32_t kTopSegments = 256;
-// a reduction level over more input segments than this (all windows) may use the serial form
-constexpr uint64_t kSerialMinSegments = 8192;
 
 struct Layout {
   size_t counts, offsets, entries, tasks, multi, partials, buckets, lv_y, lv_z, lv_y2, lv_z2, wsum,
@@ -815,6 +865,21 @@ int accumulate_grid(int sms) {
   return blocks_per_sm * sms;
 }
 
+// One level of the bucket reduction (level 0: y = the buckets, z = null): one thread per
+// output segment while the level is too large to run four times over in the resident
+// threads (least work, for full GPUs), else one quad per segment (quad point operations:
+// about a third of the chain's latency for a fifth more work).
+template <class F>
+void reduce_level(const uint32_t* y, const uint32_t* z, uint32_t n, uint32_t nout, int W, int level,
+                  uint32_t* yout, uint32_t* zout, uint64_t resident, cudaStream_t st) {
+  const uint64_t outs = (uint64_t)W * nout;
+  if (outs * 4 <= resident)
+    k_reduce_level_quad<F><<<(uint32_t)((outs * 4 + 127) / 128), 128, 0, st>>>(y, z, n, nout, W, level, yout, zout);
+  else
+    k_reduce_level<F><<<(uint32_t)((outs + 127) / 128), 128, 0, st>>>(y, z, n, nout, W, level, yout, zout);
+  note_launch();
+}
+
 // One MSM.  Generic: d_points holds n points.  FIXED: d_points is a table of W*n points,
 // T[j*n + i] = 2^(c j) P_i, built with the same c (fixed_table_impl).
 template <class F, bool FIXED>
@@ -839,6 +904,14 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   if ((uint64_t)W * n >= (uint64_t)NEG_BIT) return cudaErrorInvalidValue;
   const uint32_t nb = FIXED ? (1u << (c - 1)) : (uint32_t)W << (c - 1);
   const int rounds_req = cfg.affine < 0 ? auto_affine_rounds<F>(n, W, nb) : cfg.affine;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // threads the accumulation keeps resident: an MSM whose tasks (at the shortest length) fit
+  // four times over runs in latency form (one quad per task, shortest tasks)
+  const uint64_t resident = (uint64_t)accumulate_grid<F>(sms) * 128;
+  const bool latency_mode = rounds_req == 0 && ((uint64_t)nb + (uint64_t)n * W / kMinTask + 1) * 4 <= resident;
+  if (latency_mode) task_len = kMinTask;
   const Layout L = make_layout(n, c, XB, kMinTask, FIXED, layout_affine(EC2, cfg.affine, n, c, FIXED));
   if (work_bytes < L.total || d_work == nullptr) return cudaErrorInvalidValue;
   char* base = static_cast<char*>(d_work);
@@ -909,12 +982,13 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   k_task_emit<F><<<(nb + T - 1) / T, T, 0, st>>>(acc_off, nb, task_len, counters + kCtrCursor, tasks,
                                                   counters, multi);
   note_launch();
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (cfg.acc_start) cudaEventRecord(cfg.acc_start, st);
-  k_accumulate<F><<<accumulate_grid<F>(sms), 128, 0, st>>>(tasks, counters, acc_entries, acc_points, nb,
-                                                           buckets, partials);
+  if (latency_mode)
+    k_accumulate_quad<F><<<accumulate_grid<F>(sms), 128, 0, st>>>(tasks, counters, acc_entries, acc_points, nb,
+                                                                  buckets, partials);
+  else
+    k_accumulate<F><<<accumulate_grid<F>(sms), 128, 0, st>>>(tasks, counters, acc_entries, acc_points, nb,
+                                                             buckets, partials);
   note_launch();
   k_combine_small<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);
   k_combine<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);
@@ -924,27 +998,13 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   const int WR = FIXED ? 1 : W;
   const uint32_t B = 1u << (c - 1);
   uint32_t nseg = (B + 7) / 8;
-  k_reduce_level<F><<<((uint32_t)WR * nseg + 127) / 128, 128, 0, st>>>(buckets, nullptr, B, nseg, WR, 0,
-                                                                      lv_y, lv_z);
-  note_launch();
+  reduce_level<F>(buckets, nullptr, B, nseg, WR, 0, lv_y, lv_z, resident, st);
   int levels = 1;
   uint32_t *y = lv_y, *z = lv_z, *y2 = lv_y2, *z2 = lv_z2;
-  // more levels until the top block's chain is short.  Measured at 2^20 (B200): a proof
-  // (five MSMs sharing the GPU) 30.5 -> 29.2 ms with one thread per 8 segments, which does a
-  // quarter of the cooperative levels' work; a lone G2 fixed-base MSM is 0.47 ms faster with
-  // the cooperative levels' shorter chains; a lone G1 MSM is equal or faster serial.
-  const bool serial_levels = cfg.reduce_serial >= 0 ? cfg.reduce_serial != 0 : !std::is_same<F, Fq2>::value;
+  // more levels until the top block's chain is short
   while (nseg > kTopSegments) {
     const uint32_t nnext = (nseg + 7) / 8;
-    const uint32_t threads = (uint32_t)WR * nnext * 8;
-    // the serial form only while the level is large (where its saving is); the small top
-    // levels keep the cooperative form's short chains (2^20 G1: fixed 5.27 -> 5.10 ms,
-    // generic 7.11 -> 7.02 ms; proofs unchanged)
-    if (serial_levels && (uint64_t)WR * nseg > kSerialMinSegments)
-      k_reduce_level<F><<<((uint32_t)WR * nnext + 127) / 128, 128, 0, st>>>(y, z, nseg, nnext, WR, levels, y2, z2);
-    else
-      k_reduce_level_coop<F><<<(threads + 127) / 128, 128, 0, st>>>(y, z, nseg, nnext, WR, levels, y2, z2);
-    note_launch();
+    reduce_level<F>(y, z, nseg, nnext, WR, levels, y2, z2, resident, st);
     uint32_t* ty = y; y = y2; y2 = ty;
     uint32_t* tz = z; z = z2; z2 = tz;
     nseg = nnext;

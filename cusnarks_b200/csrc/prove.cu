@@ -203,8 +203,8 @@ inline GlvSplit split(const uint32_t* k32) {
 }  // namespace glv
 
 // out (XYZZ) = k * P for P affine (G1), k given as its GLV split.
-// One warp (launched with 32 threads): the independent products of each doubling and
-// addition run on separate lanes; lane 0 stores.
+// One warp (launched with 32 threads; its 8 quads compute the same): the independent
+// products of each doubling and addition run on the lanes of a quad; lane 0 stores.
 __global__ void k_scale_point_glv(const uint32_t* __restrict__ P, const GlvSplit* __restrict__ gs,
                                   uint32_t* __restrict__ out) {
   const Fq beta{{0xd782e155u, 0x71930c11u, 0xffbe3323u, 0xa6bb947cu, 0xd4741444u, 0xaa303344u, 0x26594943u,
@@ -218,11 +218,11 @@ __global__ void k_scale_point_glv(const uint32_t* __restrict__ P, const GlvSplit
     if (g.neg2) q.y = q.y.neg();
     const XYZZ<Fq> pq = xyzz_madd(XYZZ<Fq>::from_affine(p), q);  // P + phi(P) (never infinity)
     for (int b = 127; b >= 0; b--) {
-      acc = xyzz_dbl_warp(acc);
+      acc = xyzz_dbl_quad(acc);
       const uint32_t e1 = (g.k1[b >> 5] >> (b & 31)) & 1u, e2 = (g.k2[b >> 5] >> (b & 31)) & 1u;
-      if (e1 && e2) acc = xyzz_add_warp(acc, pq);
-      else if (e1) acc = xyzz_add_warp(acc, XYZZ<Fq>::from_affine(p));
-      else if (e2) acc = xyzz_add_warp(acc, XYZZ<Fq>::from_affine(q));
+      if (e1 && e2) acc = xyzz_add_quad(acc, pq);
+      else if (e1) acc = xyzz_add_quad(acc, XYZZ<Fq>::from_affine(p));
+      else if (e2) acc = xyzz_add_quad(acc, XYZZ<Fq>::from_affine(q));
     }
   }
   if (threadIdx.x == 0) st_xyzz<Fq>(out, acc);
@@ -460,7 +460,6 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
   if ((e = domain_get(ctx, pk->log_m + 1, &dom2)) != cudaSuccess || (e = domain_get(ctx, pk->log_m, &dom1)) != cudaSuccess)
     return fail(ctx, e, "prove tables");
   MsmConfig cfg;
-  cfg.reduce_serial = 1;
   const GlvSplit glv_rs[2] = {glv::split(s), glv::split(r)};  // s * pi_A, r * pi_B1
   cudaEventRecord(ctx->ev_start, s0);
   // scalars: w ++ [1, r] and w ++ [1, s]; r, s, -rs
@@ -484,7 +483,6 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
     if (pk->has_fixed()) {
       MsmConfig fcfg;
       fcfg.c = f.c;
-      fcfg.reduce_serial = 1;  // the proof's MSMs share the GPU: least reduction work
       return ec2 ? msm_fixed_g2(sc, f.table, n, out, at(off), bytes, fcfg, st)
                  : msm_fixed_g1(sc, f.table, n, out, at(off), bytes, fcfg, st);
     }
