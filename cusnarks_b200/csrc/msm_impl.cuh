@@ -440,22 +440,22 @@ __global__ void __launch_bounds__(128) k_reduce_level_quad(const uint32_t* __res
   for (int i = 7; i >= 1; i--) {
     const uint32_t idx = 8 * t + i;
     const XYZZ<F> v = valid && idx < n ? ld_xyzz<F>(yj + (size_t)idx * XW) : XYZZ<F>::inf();
-    acc = xyzz_add_quad(acc, v);
-    s = xyzz_add_quad(s, acc);
+    acc = add_q(acc, v);
+    s = add_q(s, acc);
   }
   {
     const XYZZ<F> v = valid && 8 * t < n ? ld_xyzz<F>(yj + (size_t)(8 * t) * XW) : XYZZ<F>::inf();
-    acc = xyzz_add_quad(acc, v);
+    acc = add_q(acc, v);
   }
 #pragma unroll 1
-  for (int d = 0; d < 3 * level; d++) s = xyzz_dbl_quad(s);
+  for (int d = 0; d < 3 * level; d++) s = dbl_q(s);
   if (z) {  // uniform: a kernel argument
     const uint32_t* zj = z + (size_t)j * n * XW;
 #pragma unroll 1
     for (int i = 0; i < 8; i++) {
       const uint32_t idx = 8 * t + i;
       const XYZZ<F> v = valid && idx < n ? ld_xyzz<F>(zj + (size_t)idx * XW) : XYZZ<F>::inf();
-      s = xyzz_add_quad(s, v);
+      s = add_q(s, v);
     }
   }
   if (valid && (threadIdx.x & 3) == 0) {
@@ -504,20 +504,20 @@ __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restri
   for (int i = (int)E - 1; i >= 0; i--) {  // uniform trip count; past n1 the terms are infinity
     const uint32_t idx = u * E + i;
     const bool in = idx < n1;
-    acc = xyzz_add_quad(acc, in ? ld_xyzz<F>(yj + (size_t)idx * XW) : XYZZ<F>::inf());
-    zs = xyzz_add_quad(zs, in ? ld_xyzz<F>(zj + (size_t)idx * XW) : XYZZ<F>::inf());
-    if (i > 0) ws = xyzz_add_quad(ws, acc);
+    acc = add_q(acc, in ? ld_xyzz<F>(yj + (size_t)idx * XW) : XYZZ<F>::inf());
+    zs = add_q(zs, in ? ld_xyzz<F>(zj + (size_t)idx * XW) : XYZZ<F>::inf());
+    if (i > 0) ws = add_q(ws, acc);
   }
   // V = acc + zs + 2^shift ws
 #pragma unroll 1
-  for (int d = 0; d < shift; d++) ws = xyzz_dbl_quad(ws);
-  XYZZ<F> V = xyzz_add_quad(xyzz_add_quad(acc, zs), ws);
+  for (int d = 0; d < shift; d++) ws = dbl_q(ws);
+  XYZZ<F> V = add_q(add_q(acc, zs), ws);
   // inclusive suffix scan of acc over the 8 virtual lanes of the warp
   XYZZ<F> suf = acc;
 #pragma unroll 1
   for (int d = 1; d < 8; d <<= 1) {
     const XYZZ<F> o = shfl_down_xyzz(suf, 4 * d);
-    suf = xyzz_select(vl + d < 8, xyzz_add_quad(suf, o), suf);
+    suf = xyzz_select(vl + d < 8, add_q(suf, o), suf);
   }
   if (vl == 0 && q == 0) {
     const uint32_t* w = reinterpret_cast<const uint32_t*>(&suf);
@@ -534,7 +534,7 @@ __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restri
 #pragma unroll 1
     for (int d = 1; d < 8; d <<= 1) {
       const XYZZ<F> o = shfl_down_xyzz(t, 4 * d);
-      t = xyzz_select(vl + d < 8, xyzz_add_quad(t, o), t);
+      t = xyzz_select(vl + d < 8, add_q(t, o), t);
     }
     XYZZ<F> excl = shfl_down_xyzz(t, 4);
     if (vl == 7) excl = XYZZ<F>::inf();
@@ -549,22 +549,22 @@ __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restri
     XYZZ<F> off;
     uint32_t* w = reinterpret_cast<uint32_t*>(&off);
     for (int k = 0; k < XW; k++) w[k] = sh[warp][k];
-    suf = xyzz_add_quad(suf, off);
+    suf = add_q(suf, off);
   }
   __syncthreads();
   // C_u = V_u + 2^shift E * Suf(u) for u >= 1 (E is a power of two)
   {  // computed by every quad (uniform), kept where u >= 1 and u E < n1
 #pragma unroll 1
-    for (uint32_t m = E; m > 1; m >>= 1) suf = xyzz_dbl_quad(suf);
+    for (uint32_t m = E; m > 1; m >>= 1) suf = dbl_q(suf);
 #pragma unroll 1
-    for (int d = 0; d < shift; d++) suf = xyzz_dbl_quad(suf);
-    V = xyzz_select(u >= 1 && u * E < n1, xyzz_add_quad(V, suf), V);
+    for (int d = 0; d < shift; d++) suf = dbl_q(suf);
+    V = xyzz_select(u >= 1 && u * E < n1, add_q(V, suf), V);
   }
   // block reduction of V: over the warp's virtual lanes, then over the warps
 #pragma unroll 1
   for (int d = 4; d > 0; d >>= 1) {
     const XYZZ<F> o = shfl_down_xyzz(V, 4 * d);
-    V = xyzz_add_quad(V, o);  // virtual lanes >= 8 - d add stray values; only lane 0's sum is kept
+    V = add_q(V, o);  // virtual lanes >= 8 - d add stray values; only lane 0's sum is kept
   }
   if (vl == 0 && q == 0) {
     const uint32_t* w = reinterpret_cast<const uint32_t*>(&V);
@@ -580,7 +580,7 @@ __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restri
 #pragma unroll 1
     for (int d = 4; d > 0; d >>= 1) {
       const XYZZ<F> o = shfl_down_xyzz(t, 4 * d);
-      t = xyzz_add_quad(t, o);
+      t = add_q(t, o);
     }
     if (vl == 0 && q == 0) st_xyzz<F>(wsum + (size_t)j * XW, t);
   }
