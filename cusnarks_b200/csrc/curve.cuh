@@ -198,19 +198,6 @@ template <class F>
 __device__ __noinline__ XYZZ<F> xyzz_add_cold(const XYZZ<F> p, const XYZZ<F> q) { return xyzz_add(p, q); }
 template <class F>
 __device__ __noinline__ XYZZ<F> xyzz_dbl_cold(const XYZZ<F> p) { return xyzz_dbl(p); }
-// The same with paired out-of-line products (small code for a single-thread chain in a unit
-// whose products are inlined: the proof's GLV scalar multiplication, 2^12 proof 3.52 ->
-// 3.47 ms).  A pair costs about two products' latency: the two carry-flag chains do not
-// overlap, so the window Horner of the MSM units keeps single calls.
-#ifndef CSB_LAT_PAIR
-#define CSB_LAT_PAIR 1
-#endif
-template <class F>
-__device__ __noinline__ XYZZ<F> xyzz_add_lat(const XYZZ<F> p, const XYZZ<F> q) {
-  return xyzz_add<F, CSB_LAT_PAIR != 0>(p, q);
-}
-template <class F>
-__device__ __noinline__ XYZZ<F> xyzz_dbl_lat(const XYZZ<F> p) { return xyzz_dbl<F, CSB_LAT_PAIR != 0>(p); }
 
 // ------------------------------------------------ quad-parallel point operations -----
 // For chains that a point runs through alone (window Horner, scalar multiplication, the

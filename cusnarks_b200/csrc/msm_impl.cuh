@@ -699,11 +699,8 @@ CSB_DEV uint32_t bucket_of_slot(const uint32_t* off, uint32_t nb, uint32_t s) {
   return lo;
 }
 
-#ifndef CSB_AFF_MINB
-#define CSB_AFF_MINB 0
-#endif
 template <class F, bool FIRST>
-__global__ void __launch_bounds__(128, CSB_AFF_MINB) k_affine_round(const uint32_t* __restrict__ in_off,
+__global__ void __launch_bounds__(128) k_affine_round(const uint32_t* __restrict__ in_off,
                                                       const uint32_t* __restrict__ out_off, uint32_t nb,
                                                       const uint32_t* __restrict__ entries,
                                                       const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
@@ -832,10 +829,9 @@ inline int auto_affine_rounds_rt(bool ec2, uint32_t n, int W, size_t nb) {
   // pairs (>= 2^22, i.e. N W >= 2^23 entries) to fill the GPU, or its chain sets the latency
   // (2 rounds cost 2.5 ms in a 2^12-term G2 MSM)
   if ((uint64_t)n * W < (1ull << 23)) return 0;
-#ifndef CSB_AFF_G1_CAP
-#define CSB_AFF_G1_CAP 0
-#endif
-  const int cap = ec2 ? 2 : CSB_AFF_G1_CAP;
+  // G1 rounds measured slower, alone and inside proofs (2^20 proof 29.1 -> 30.2 ms with one
+  // round, 30.7 ms with two): its mixed addition is cheap enough that the extra passes lose
+  const int cap = ec2 ? 2 : 0;
   const double avg = (double)n * W / (double)nb;
   int r = 0;
   while (r < cap && avg >= (double)(8u << r)) r++;
