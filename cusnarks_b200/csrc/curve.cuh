@@ -142,6 +142,31 @@ CSB_DEV XYZZ<F> xyzz_madd(const XYZZ<F>& p, const Affine<F>& q) {
   }
 }
 
+// madd-2008-s over Fq with lazily reduced coordinates (values in [0, 2p), products without
+// the final conditional subtraction): the G1 bucket accumulation's addition.  Inputs may be
+// lazy; q canonical; callers canonicalise before storing (xyzz_canon).
+CSB_DEV XYZZ<Fq> xyzz_madd_lazy(const XYZZ<Fq>& p, const Affine<Fq>& q) {
+  if (p.ZZ.is_zero_lazy()) return XYZZ<Fq>::from_affine(q);
+  const Fq U2 = Fq::mul_lazy(q.x, p.ZZ);
+  const Fq S2 = Fq::mul_lazy(q.y, p.ZZZ);
+  const Fq P = Fq::sub_lazy(U2, p.X);
+  const Fq R = Fq::sub_lazy(S2, p.Y);
+  if (P.is_zero_lazy()) {
+    if (R.is_zero_lazy()) return xyzz_mdbl(q);
+    return XYZZ<Fq>::inf();
+  }
+  const Fq PP = Fq::mul_lazy(P, P);
+  const Fq PPP = Fq::mul_lazy(P, PP);
+  const Fq Q = Fq::mul_lazy(p.X, PP);
+  XYZZ<Fq> r;
+  r.X = Fq::sub_lazy(Fq::sub_lazy(Fq::mul_lazy(R, R), PPP), Fq::add_lazy(Q, Q));
+  r.Y = Fq::sub_lazy(Fq::mul_lazy(R, Fq::sub_lazy(Q, r.X)), Fq::mul_lazy(p.Y, PPP));
+  r.ZZ = Fq::mul_lazy(p.ZZ, PP);
+  r.ZZZ = Fq::mul_lazy(p.ZZZ, PPP);
+  return r;
+}
+CSB_DEV XYZZ<Fq> xyzz_canon(const XYZZ<Fq>& p) { return {p.X.canon(), p.Y.canon(), p.ZZ.canon(), p.ZZZ.canon()}; }
+
 // add-2008-s: p + q, both XYZZ
 template <class F, bool PAIR = (CSB_PAIRED != 0)>
 CSB_DEV XYZZ<F> xyzz_add(const XYZZ<F>& p, const XYZZ<F>& q) {

@@ -246,6 +246,79 @@ struct Fp {
     for (int i = 0; i < 8; i++) { x.v[i] = r8[i]; y.v[i] = s8[i]; }
   }
 
+  // ---- lazily reduced values in [0, 2p) (BN254: 4p < 2^256) --------------------------
+  // CIOS without the final conditional subtraction: for a, b < 2p the result is below
+  // (a b + m p) / 2^256 < (4p^2 + 2^256 p) / 2^256 < 2p.
+  static CSB_DEV Fp mul_wide_lazy(const Fp& a, const Fp& b) {
+    const uint32_t P[8] = {M::P0, M::P1, M::P2, M::P3, M::P4, M::P5, M::P6, M::P7};
+    uint32_t t[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) t[i] = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      row_mad_wide(t, a.v, b.v[i]);
+      const uint32_t m = t[0] * M::NP0;
+      row_mad_wide(t, P, m);
+#pragma unroll
+      for (int j = 0; j < 8; j++) t[j] = t[j + 1];
+      t[8] = 0;
+    }
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = t[i];
+    return r;
+  }
+  static CSB_DEV Fp mul_lazy(const Fp& a, const Fp& b);
+  // 2p, limb i
+  static CSB_DEV uint32_t p2(int i) {
+    const uint32_t P[8] = {M::P0, M::P1, M::P2, M::P3, M::P4, M::P5, M::P6, M::P7};
+    return (P[i] << 1) | (i > 0 ? P[i - 1] >> 31 : 0u);
+  }
+  // a + b for a, b < 2p, result < 2p
+  static CSB_DEV Fp add_lazy(const Fp& a, const Fp& b) {
+    uint32_t t[8], u[8], br;
+    ADD_CC(t[0], a.v[0], b.v[0]);  ADDC_CC(t[1], a.v[1], b.v[1]); ADDC_CC(t[2], a.v[2], b.v[2]);
+    ADDC_CC(t[3], a.v[3], b.v[3]); ADDC_CC(t[4], a.v[4], b.v[4]); ADDC_CC(t[5], a.v[5], b.v[5]);
+    ADDC_CC(t[6], a.v[6], b.v[6]); ADDC(t[7], a.v[7], b.v[7]);
+    SUB_CC(u[0], t[0], p2(0)); SUBC_CC(u[1], t[1], p2(1)); SUBC_CC(u[2], t[2], p2(2));
+    SUBC_CC(u[3], t[3], p2(3)); SUBC_CC(u[4], t[4], p2(4)); SUBC_CC(u[5], t[5], p2(5));
+    SUBC_CC(u[6], t[6], p2(6)); SUBC_CC(u[7], t[7], p2(7)); SUBC(br, 0u, 0u);
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = (t[i] & br) | (u[i] & ~br);
+    return r;
+  }
+  // a - b for a, b < 2p, result < 2p
+  static CSB_DEV Fp sub_lazy(const Fp& a, const Fp& b) {
+    uint32_t t[8], br;
+    SUB_CC(t[0], a.v[0], b.v[0]);  SUBC_CC(t[1], a.v[1], b.v[1]); SUBC_CC(t[2], a.v[2], b.v[2]);
+    SUBC_CC(t[3], a.v[3], b.v[3]); SUBC_CC(t[4], a.v[4], b.v[4]); SUBC_CC(t[5], a.v[5], b.v[5]);
+    SUBC_CC(t[6], a.v[6], b.v[6]); SUBC_CC(t[7], a.v[7], b.v[7]); SUBC(br, 0u, 0u);
+    Fp r;
+    ADD_CC(r.v[0], t[0], p2(0) & br);  ADDC_CC(r.v[1], t[1], p2(1) & br); ADDC_CC(r.v[2], t[2], p2(2) & br);
+    ADDC_CC(r.v[3], t[3], p2(3) & br); ADDC_CC(r.v[4], t[4], p2(4) & br); ADDC_CC(r.v[5], t[5], p2(5) & br);
+    ADDC_CC(r.v[6], t[6], p2(6) & br); ADDC(r.v[7], t[7], p2(7) & br);
+    return r;
+  }
+  // zero mod p for a value < 2p: 0 or p
+  CSB_DEV bool is_zero_lazy() const {
+    const uint32_t z = v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7];
+    const uint32_t e = (v[0] ^ M::P0) | (v[1] ^ M::P1) | (v[2] ^ M::P2) | (v[3] ^ M::P3) | (v[4] ^ M::P4) |
+                       (v[5] ^ M::P5) | (v[6] ^ M::P6) | (v[7] ^ M::P7);
+    return z == 0 || e == 0;
+  }
+  // the canonical representative in [0, p) of a value < 2p
+  CSB_DEV Fp canon() const {
+    uint32_t t[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) t[i] = v[i];
+    reduce_once(t);
+    Fp r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = t[i];
+    return r;
+  }
+
   // x = a*b, y = c*d in one out-of-line call with interleaved rows (any unit): about the
   // latency of one product for two, where a single thread's chain is the cost.
   static CSB_DEV void mul2_ool(const Fp& a, const Fp& b, const Fp& c, const Fp& d, Fp& x, Fp& y) {
@@ -491,6 +564,20 @@ __device__ __noinline__ Fp<M> fp_mul_call(Fp<M> a, Fp<M> b) {
   return Fp<M>::mul_lohi(a, b);
 #else
   return Fp<M>::mul_wide(a, b);
+#endif
+}
+
+template <class M>
+__device__ __noinline__ Fp<M> fp_mul_lazy_call(Fp<M> a, Fp<M> b) {
+  return Fp<M>::mul_wide_lazy(a, b);
+}
+
+template <class M>
+CSB_DEV Fp<M> Fp<M>::mul_lazy(const Fp<M>& a, const Fp<M>& b) {
+#if defined(CSB_MUL_NOINLINE)
+  return fp_mul_lazy_call<M>(a, b);
+#else
+  return mul_wide_lazy(a, b);
 #endif
 }
 

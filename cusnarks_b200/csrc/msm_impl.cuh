@@ -233,6 +233,29 @@ __global__ void k_task_emit(const uint32_t* __restrict__ offsets, uint32_t nb, u
 template <class F> struct AccMinBlocks { static constexpr int value = CSB_ACC_G1_MINB; };
 template <> struct AccMinBlocks<Fq2> { static constexpr int value = CSB_ACC_G2_MINB; };
 
+// The accumulation's mixed addition: over Fq with lazily reduced coordinates (no final
+// conditional subtraction per product; the bucket is canonicalised when stored), over Fq2
+// the canonical one.
+#ifndef CSB_LAZY_G1
+#define CSB_LAZY_G1 1
+#endif
+CSB_DEV XYZZ<Fq> madd_acc(const XYZZ<Fq>& acc, const Affine<Fq>& p) {
+#if CSB_LAZY_G1
+  return xyzz_madd_lazy(acc, p);
+#else
+  return xyzz_madd(acc, p);
+#endif
+}
+CSB_DEV XYZZ<Fq2> madd_acc(const XYZZ<Fq2>& acc, const Affine<Fq2>& p) { return xyzz_madd(acc, p); }
+CSB_DEV XYZZ<Fq> canon_acc(const XYZZ<Fq>& a) {
+#if CSB_LAZY_G1
+  return xyzz_canon(a);
+#else
+  return a;
+#endif
+}
+CSB_DEV XYZZ<Fq2> canon_acc(const XYZZ<Fq2>& a) { return a; }
+
 template <class F>
 __global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate(const Task* __restrict__ tasks,
                                                     const uint32_t* __restrict__ counters,
@@ -254,17 +277,17 @@ __global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate(cons
         const uint32_t ent = entries[tk.start + e];
         Affine<F> p = ld_affine<F>(base + (size_t)(ent & ~NEG_BIT) * PW);
         if (ent & NEG_BIT) p.y = p.y.neg();
-        acc = xyzz_madd(acc, p);
+        acc = madd_acc(acc, p);
       }
     } else {  // after batch-affine rounds: points in bucket order, (0, 0) = infinity
 #pragma unroll 1
       for (uint32_t e = 0; e < tk.len; e++) {
         const Affine<F> p = ld_affine<F>(base + (size_t)(tk.start + e) * PW);
-        if (!(p.x.is_zero() && p.y.is_zero())) acc = xyzz_madd(acc, p);
+        if (!(p.x.is_zero() && p.y.is_zero())) acc = madd_acc(acc, p);
       }
     }
     uint32_t* dst = tk.dst < nb ? buckets + (size_t)tk.dst * XW : partials + (size_t)(tk.dst - nb) * XW;
-    st_xyzz<F>(dst, acc);
+    st_xyzz<F>(dst, canon_acc(acc));
   }
 }
 
