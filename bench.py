@@ -60,7 +60,7 @@ PRODUCTS_PER_MONT = 136
 MONT_PER_MADD = 11     # mixed addition, 7M + 4S (the canonical count of the MSM cost model)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_accumulate launch of
 # the 2^20 G1 MSM (window 16), from an ncu capture of that launch
-ACC_TRAFFIC_BYTES = 437_851_392 + 61_300_736
+ACC_TRAFFIC_BYTES = 436_821_248 + 61_684_480
 L2_BYTES = 126 * 1024 * 1024
 LOG_M = 20
 CPU_SAMPLE_LOG_M = 16
