@@ -183,6 +183,10 @@ _SIGNATURES = [
     ("ec2_jacsc1mul_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
     ("ec_isoncurve_h", ctypes.c_uint32, [_vp, ctypes.c_uint32, ctypes.c_uint32]),
     ("ec2_isoncurve_h", ctypes.c_uint32, [_vp, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ec_inittable_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ec2_inittable_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ec_isinf", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ec2_isinf", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32]),
     ("sortu256_idx_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32]),
     ("ntt_build_h", None, [_vp, ctypes.c_uint32]),
     ("init_h", None, []),

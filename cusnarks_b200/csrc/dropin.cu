@@ -132,6 +132,37 @@ void jacscmul(bool ec2, uint32_t* z, const uint32_t* scl, const uint32_t* x, uin
                 });
 }
 
+// ectable <- ceil(n / order) subset-sum tables of 2^order Jacobian rows (Z = 1; infinity
+// (0, 1, 0)): rows of x are affine (add_last) or Jacobian points.
+void inittable(bool ec2, const uint32_t* x, uint32_t* ectable, uint32_t n, uint32_t order, uint32_t pidx,
+               uint32_t add_last) {
+  const char* what = ec2 ? "ec2_inittable_h" : "ec_inittable_h";
+  if (bad_pidx(pidx, what)) return;
+  if (order == 0 || order > 16) {
+    dropin_status(CS_ERR_ARG, (std::string(what) + ": table_order must be 1..16").c_str());
+    return;
+  }
+  const size_t fw = ec2 ? 16 : 8;
+  const uint32_t dims = add_last ? 2 : 3;
+  const size_t entries = (((size_t)n + order - 1) / order) << order;
+  // scratch: n affine points, then the affine table
+  run_on_device(what, x, (size_t)n * dims * fw, ectable, entries * 3 * fw, ((size_t)n + entries) * 2 * fw,
+                [&](uint32_t* d_in, uint32_t* d_out, uint32_t* d_scr, cudaStream_t st) {
+                  const uint32_t* d_aff = d_in;
+                  cudaError_t e = cudaSuccess;
+                  if (!add_last) {
+                    e = ec2 ? jac_to_affine_g2(d_in, n, d_scr, st) : jac_to_affine_g1(d_in, n, d_scr, st);
+                    d_aff = d_scr;
+                  }
+                  if (e != cudaSuccess) return e;
+                  uint32_t* d_tab = d_scr + (size_t)n * 2 * fw;
+                  e = ec2 ? subset_table_g2(d_aff, n, order, d_tab, st) : subset_table_g1(d_aff, n, order, d_tab, st);
+                  if (e != cudaSuccess) return e;
+                  return ec2 ? affine_to_jac_g2(d_tab, (uint32_t)entries, d_out, st)
+                             : affine_to_jac_g1(d_tab, (uint32_t)entries, d_out, st);
+                });
+}
+
 uint32_t isoncurve(bool ec2, const uint32_t* x, uint32_t is_affine, uint32_t pidx) {
   if (bad_pidx(pidx, "ec_isoncurve_h")) return 0;
   const size_t fw = ec2 ? 16 : 8;
@@ -181,6 +212,48 @@ void ec2_jacsc1mul_h(uint32_t* z, uint32_t* x, uint32_t n, uint32_t pidx, uint32
 }
 uint32_t ec_isoncurve_h(uint32_t* x, uint32_t is_affine, uint32_t pidx) { return isoncurve(false, x, is_affine, pidx); }
 uint32_t ec2_isoncurve_h(uint32_t* x, uint32_t is_affine, uint32_t pidx) { return isoncurve(true, x, is_affine, pidx); }
+void ec_inittable_h(uint32_t* x, uint32_t* ectable, uint32_t n, uint32_t table_order, uint32_t pidx,
+                    uint32_t add_last) {
+  inittable(false, x, ectable, n, table_order, pidx, add_last);
+}
+void ec2_inittable_h(uint32_t* x, uint32_t* ectable, uint32_t n, uint32_t table_order, uint32_t pidx,
+                     uint32_t add_last) {
+  inittable(true, x, ectable, n, table_order, pidx, add_last);
+}
+
+// ec.cpp:1153 / :1164, as the reference computes them: z[j] is the infinity test (first two
+// coordinates equal to the affine infinity's, (0, 1_mont) in G1 with the Montgomery one of
+// modulus pidx, X = 0 in G2) of the rows the reference reads, which start 2 j words into x
+// in G1 (it steps by the coordinate count) and 4 words into x for every j in G2.
+void ec_isinf(uint32_t* z, const uint32_t* x, const uint32_t n, const uint32_t pidx) {
+  // the Montgomery one of the modulus pidx selects (constants.cpp:264-292)
+  static const uint32_t ones[2][8] = {{0xc58f0d9du, 0xd35d438du, 0xf5c70b3du, 0x0a78eb28u,
+                                       0x7879462cu, 0x666ea36fu, 0x9a07df2fu, 0x0e0a77c1u},
+                                      {0x4ffffffbu, 0xac96341cu, 0x9f60cd29u, 0x36fc7695u,
+                                       0x7879462eu, 0x666ea36fu, 0x9a07df2fu, 0x0e0a77c1u}};
+  if (pidx > 1) {
+    dropin_status(CS_ERR_ARG, "ec_isinf: pidx must be 0 or 1");
+    return;
+  }
+  const uint32_t* one = ones[pidx];
+  for (uint32_t j = 0; j < n; j++) {
+    const uint32_t* r = x + (size_t)j * 2;
+    bool inf = true;
+    for (int k = 0; k < 8; k++) inf = inf && r[k] == 0 && r[8 + k] == one[k];
+    z[j] = inf ? 1u : 0u;
+  }
+  dropin_status(CS_OK, "");
+}
+void ec2_isinf(uint32_t* z, const uint32_t* x, const uint32_t n, const uint32_t pidx) {
+  if (pidx > 1) {
+    dropin_status(CS_ERR_ARG, "ec2_isinf: pidx must be 0 or 1");
+    return;
+  }
+  bool inf = true;
+  for (int k = 0; k < 16; k++) inf = inf && x[4 + k] == 0;
+  for (uint32_t j = 0; j < n; j++) z[j] = inf ? 1u : 0u;
+  dropin_status(CS_OK, "");
+}
 
 // ------------------------------------------------------------------ host routines ----
 // bigint.cpp:72: idx = 0..len-1, sorted (std::sort, unstable) by the most significant word

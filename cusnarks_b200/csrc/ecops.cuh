@@ -25,6 +25,10 @@ cudaError_t affine_to_jac_g2(const uint32_t* aff, uint32_t n, uint32_t* jac, cud
 cudaError_t point_sum_g1(const uint32_t* pts, uint32_t n, int dims, uint32_t* out, cudaStream_t st);
 cudaError_t point_sum_g2(const uint32_t* pts, uint32_t n, int dims, uint32_t* out, cudaStream_t st);
 cudaError_t on_curve_g1(const uint32_t* p, int jac, uint32_t* flag, cudaStream_t st);
+// Subset-sum tables (the reference's ec_inittable_h): ceil(n / order) tables of 2^order affine
+// entries, entry j of table t = sum of points t*order + b over the set bits b of j.
+cudaError_t subset_table_g1(const uint32_t* aff, uint32_t n, uint32_t order, uint32_t* out, cudaStream_t st);
+cudaError_t subset_table_g2(const uint32_t* aff, uint32_t n, uint32_t order, uint32_t* out, cudaStream_t st);
 cudaError_t on_curve_g2(const uint32_t* p, int jac, uint32_t* flag, cudaStream_t st);
 
 }  // namespace csb

@@ -18,4 +18,7 @@ cudaError_t point_sum_g1(const uint32_t* pts, uint32_t n, int dims, uint32_t* ou
 cudaError_t on_curve_g1(const uint32_t* p, int jac, uint32_t* flag, cudaStream_t st) {
   return ecops_detail::on_curve<Fq>(p, jac, flag, st);
 }
+cudaError_t subset_table_g1(const uint32_t* aff, uint32_t n, uint32_t order, uint32_t* out, cudaStream_t st) {
+  return ecops_detail::subset_table<Fq>(aff, n, order, out, st);
+}
 }  // namespace csb

@@ -149,6 +149,39 @@ __global__ void k_on_curve(const uint32_t* __restrict__ p, int jac, uint32_t* __
   *flag = (Y.sqr() == X.sqr() * X + curve_b<F>() * z6) ? 1u : 0u;
 }
 
+// Subset-sum tables of groups of `order` affine points (the reference's ec_inittable_h,
+// src/cuda/ec.cpp:574): entry j of table t is the sum of the points t*order + b over the set
+// bits b of j (points past n count as infinity); affine out, infinity (0, 1).
+template <class F>
+__global__ void __launch_bounds__(128) k_subset_table(const uint32_t* __restrict__ aff, uint32_t n, uint32_t order,
+                                                      uint64_t entries, uint32_t* __restrict__ out) {
+  constexpr int PW = 2 * FieldWords<F>::value;
+  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= entries) return;
+  const uint64_t t = g >> order;
+  const uint32_t j = (uint32_t)(g & ((1ull << order) - 1));
+  XYZZ<F> acc = XYZZ<F>::inf();
+#pragma unroll 1
+  for (uint32_t b = 0; b < order; b++) {
+    const uint64_t idx = t * order + b;
+    if (((j >> b) & 1u) && idx < n) {
+      const Affine<F> a = ld_affine<F>(aff + idx * PW);
+      if (!affine_is_inf(a)) acc = xyzz_madd(acc, a);
+    }
+  }
+  st_affine<F>(out + g * PW, xyzz_to_affine(acc));
+}
+
+template <class F>
+cudaError_t subset_table(const uint32_t* aff, uint32_t n, uint32_t order, uint32_t* out, cudaStream_t st) {
+  if (n == 0 || order == 0 || order > 16) return n == 0 ? cudaSuccess : cudaErrorInvalidValue;
+  const uint64_t tables = ((uint64_t)n + order - 1) / order;
+  const uint64_t entries = tables << order;
+  k_subset_table<F><<<(unsigned)((entries + 127) / 128), 128, 0, st>>>(aff, n, order, entries, out);
+  note_launch();
+  return cudaGetLastError();
+}
+
 template <class F>
 cudaError_t scmul(const uint32_t* s, const uint32_t* p, uint32_t stride, uint32_t n, uint32_t* out,
                   cudaStream_t st) {

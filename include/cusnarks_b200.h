@@ -328,6 +328,18 @@ void ec2_jacsc1mul_h(uint32_t *z, uint32_t *x, uint32_t n, uint32_t pidx, uint32
 /* ec.cpp:1064 -- 2: the infinity encoding (X = 0, Y = 1), 1: on the curve, 0: not. */
 uint32_t ec_isoncurve_h(uint32_t *x, uint32_t is_affine, uint32_t pidx);
 uint32_t ec2_isoncurve_h(uint32_t *x, uint32_t is_affine, uint32_t pidx);
+/* ec.cpp:574 / ec2_inittable_h -- subset-sum tables: ectable <- ceil(n / table_order) tables
+ * of 2^table_order Jacobian rows, entry j of table t = sum of points t*table_order + b over the
+ * set bits b of j (points past n are infinity); x rows affine (add_last) or Jacobian.  Rows
+ * are returned normalised (Z = 1; infinity (0, 1, 0)): the same points as the reference's. */
+void ec_inittable_h(uint32_t *x, uint32_t *ectable, uint32_t n, uint32_t table_order, uint32_t pidx,
+                    uint32_t add_last);
+void ec2_inittable_h(uint32_t *x, uint32_t *ectable, uint32_t n, uint32_t table_order, uint32_t pidx,
+                     uint32_t add_last);
+/* ec.cpp:1153 / :1164 -- infinity flags with the reference's row addressing (G1: rows start
+ * 2 j words into x; G2: every flag tests the row at word 4). */
+void ec_isinf(uint32_t *z, const uint32_t *x, const uint32_t n, const uint32_t pidx);
+void ec2_isinf(uint32_t *z, const uint32_t *x, const uint32_t n, const uint32_t pidx);
 /* bigint.cpp:72 -- indices 0..len-1, sorted (std::sort) by the top word of v[i] if sort_en. */
 void sortu256_idx_h(uint32_t *idx, const uint32_t *v, uint32_t len, uint32_t sort_en);
 /* ntt.cpp:1116 -- transform decomposition of nsamples (types.h fft_params_t layout). */

@@ -7,6 +7,8 @@ by `make -C oracle ref`) for the binding's remaining host functions, on seeded i
   (Jacobian rows; affine rows with add_in), ec_jacscmul_h / ec2_jacscmul_h (Jacobian bases,
   one row per call: the reference's multi-row G1 call races), ec_jacsc1mul_h, ec_isoncurve_h / ec2_isoncurve_h, on Jacobian points made by
   the reference's own ec_jacscmul_h (so their Z are not 1) with a point at infinity mixed in.
+* ec_inittable_h / ec2_inittable_h (affine and Jacobian rows, a partial last table),
+  normalised by the reference's ec_jac2aff_h, and ec_isinf / ec2_isinf.
 * sortu256_idx_h (top words drawn from a small range, so the unstable sort meets ties) and
   ntt_build_h for a range of sizes.
 """
@@ -48,6 +50,10 @@ def main():
     oncurve = {0: fn(ref, "_Z14ec_isoncurve_hPjjj", _vp, u, u, res=u),
                1: fn(ref, "_Z15ec2_isoncurve_hPjjj", _vp, u, u, res=u)}
     sortidx = fn(ref, "_Z14sortu256_idx_hPjPKjjj", _vp, _vp, u, u)
+    inittable = {0: fn(ref, "_Z14ec_inittable_hPjS_jjjj", _vp, _vp, u, u, u, u),
+                 1: fn(ref, "_Z15ec2_inittable_hPjS_jjjj", _vp, _vp, u, u, u, u)}
+    isinf = {0: fn(ref, "_Z8ec_isinfPjPKjjj", _vp, _vp, u, u),
+             1: fn(ref, "_Z9ec2_isinfPjPKjjj", _vp, _vp, u, u)}
     build = fn(ref, "_Z11ntt_build_hP12fft_params_tj", _vp, u)
 
     rng = np.random.Generator(np.random.PCG64(31337))
@@ -106,6 +112,33 @@ def main():
         flags = [int(oncurve[ec2](np.ascontiguousarray(r).ctypes.data, 1, 0)) for r in list(aff) + [bad]]
         flags += [int(oncurve[ec2](np.ascontiguousarray(r).ctypes.data, 0, 0)) for r in jac]
         out[pre + "bad"], out[pre + "oncurve"] = bad, np.array(flags, np.uint32)
+        # subset-sum tables of affine (add_last 1) and Jacobian (add_last 0) rows, n not a
+        # multiple of the order (the last table has missing points), normalised by the
+        # reference's own ec_jac2aff_h (strip_last 1)
+        for add_last, rows, order in ((1, aff, 3), (0, jac, 4)):
+            src = np.ascontiguousarray(rows[:10])
+            ntab = (10 + order - 1) // order
+            ent = ntab << order
+            tab = np.zeros(ent * 3 * fw, np.uint32)
+            inittable[ec2](src.ctypes.data, tab.ctypes.data, 10, order, 0, add_last)
+            y = np.zeros((ent, 2 * fw), np.uint32)
+            jac2aff[ec2](y.ctypes.data, tab.ctypes.data, ent, 0, 1)
+            out[pre + f"inittable_{add_last}"] = y
+        # infinity flags, with the reference's row addressing: the affine rows, then a copy
+        # with the infinity pattern planted where the reference looks (G1: 2 j words in for
+        # j = 3; G2: X of the row at word 4)
+        for tag, pidx in (("", 0), ("_p1", 1)):
+            flat = np.ascontiguousarray(aff.reshape(-1)).copy()
+            if tag:
+                if ec2:
+                    flat[4:20] = 0
+                else:
+                    flat[6:14] = 0
+                    flat[14:22] = o.const(1)[0]      # Montgomery one mod r (pidx 1)
+            nrows = flat.size // (2 * fw)
+            z = np.zeros(nrows, np.uint32)
+            isinf[ec2](z.ctypes.data, flat.ctypes.data, nrows, pidx)
+            out[pre + "isinf_in" + tag], out[pre + "isinf" + tag] = flat, z
     v = random_field(rng, 200, 1)
     v[:, 7] = rng.integers(0, 9, 200)
     idx = np.zeros(200, np.uint32)

@@ -52,3 +52,16 @@ def test_file_routines(tmp_path):
     L.readWitnessFile_h(back.ctypes.data, wp, 1, 10)
     assert np.array_equal(back, w)
     assert L.get_nprocs_h() >= 1
+
+
+def test_isinf_matches_reference(golden):
+    """ec_isinf / ec2_isinf with the reference's row addressing, for both moduli."""
+    g = golden("dropin.npz")
+    for ec2, fn in ((0, lib().ec_isinf), (1, lib().ec2_isinf)):
+        pre = f"g{ec2 + 1}_"
+        for tag, pidx in (("", 0), ("_p1", 1)):
+            flat = np.ascontiguousarray(g[pre + "isinf_in" + tag])
+            want = g[pre + "isinf" + tag]
+            z = np.zeros(want.size, np.uint32)
+            fn(z.ctypes.data, flat.ctypes.data, want.size, pidx)
+            assert np.array_equal(z, want), (ec2, tag)

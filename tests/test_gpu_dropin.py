@@ -46,3 +46,24 @@ def test_point_routines_match_reference(golden, ec2):
     flags = [int(onc(np.ascontiguousarray(r).ctypes.data, 1, 0)) for r in rows]
     flags += [int(onc(np.ascontiguousarray(r).ctypes.data, 0, 0)) for r in jac]
     assert flags == list(g[pre + "oncurve"])
+
+
+@pytest.mark.parametrize("ec2", [0, 1])
+def test_inittable_matches_reference(golden, ec2):
+    """ec_inittable_h / ec2_inittable_h: subset-sum tables (affine and Jacobian rows, a
+    partial last table), compared as points with the reference's (normalised by its own
+    ec_jac2aff_h)."""
+    L = lib()
+    g = golden("dropin.npz")
+    pre = f"g{ec2 + 1}_"
+    fw = 16 if ec2 else 8
+    fn = L.ec2_inittable_h if ec2 else L.ec_inittable_h
+    for add_last, key, order in ((1, "aff", 3), (0, "jac", 4)):
+        src = np.ascontiguousarray(g[pre + key][:10])
+        ent = ((10 + order - 1) // order) << order
+        tab = np.zeros((ent, 3 * fw), np.uint32)
+        fn(src.ctypes.data, tab.ctypes.data, 10, order, 0, add_last)
+        assert L.cs_last_status() == 0
+        want = g[pre + f"inittable_{add_last}"]
+        # Z = 1 rows are affine; the Jacobian infinity (0, 1, 0) is the affine infinity (0, 1)
+        assert np.array_equal(tab[:, :2 * fw], want), add_last
