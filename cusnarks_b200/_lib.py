@@ -187,6 +187,16 @@ _SIGNATURES = [
     ("ec2_inittable_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
     ("ec_isinf", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32]),
     ("ec2_isinf", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32]),
+    ("ec_jacadd_h", None, [_vp, _vp, _vp, ctypes.c_uint32]),
+    ("ec2_jacadd_h", None, [_vp, _vp, _vp, ctypes.c_uint32]),
+    ("ec_jacdouble_h", None, [_vp, _vp, ctypes.c_uint32]),
+    ("ec2_jacdouble_h", None, [_vp, _vp, ctypes.c_uint32]),
+    ("mpoly_from_montgomery_h", None, [_vp, ctypes.c_uint32]),
+    ("mpoly_to_montgomery_h", None, [_vp, ctypes.c_uint32]),
+    ("addu256_h", None, [_vp, _vp, _vp]),
+    ("rangeu256_h", None, [_vp, ctypes.c_uint32, _vp, ctypes.c_uint32, _vp]),
+    ("readU256CircuitFileHeader_h", None, [_vp, ctypes.c_char_p]),
+    ("readU256PKFileHeader_h", None, [_vp, ctypes.c_char_p]),
     ("sortu256_idx_h", None, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32]),
     ("ntt_build_h", None, [_vp, ctypes.c_uint32]),
     ("init_h", None, []),

@@ -212,6 +212,97 @@ void ec2_jacsc1mul_h(uint32_t* z, uint32_t* x, uint32_t n, uint32_t pidx, uint32
 }
 uint32_t ec_isoncurve_h(uint32_t* x, uint32_t is_affine, uint32_t pidx) { return isoncurve(false, x, is_affine, pidx); }
 uint32_t ec2_isoncurve_h(uint32_t* x, uint32_t is_affine, uint32_t pidx) { return isoncurve(true, x, is_affine, pidx); }
+// ec.cpp:131 / :462 (and the G2 forms): one Jacobian addition / doubling, the result
+// normalised (Z = 1; infinity (0, 1, 0)) -- the same point as the reference's.
+static void jacadd2(bool ec2, uint32_t* z, const uint32_t* x, const uint32_t* y, uint32_t pidx, const char* what) {
+  if (bad_pidx(pidx, what)) return;
+  const size_t fw = ec2 ? 16 : 8;
+  std::vector<uint32_t> in(6 * fw);
+  std::memcpy(in.data(), x, 3 * fw * 4);
+  std::memcpy(in.data() + 3 * fw, y, 3 * fw * 4);
+  run_on_device(what, in.data(), in.size(), z, 3 * fw, 2 * fw,
+                [&](uint32_t* d_in, uint32_t* d_out, uint32_t* d_aff, cudaStream_t st) {
+                  cudaError_t e = ec2 ? point_sum_g2(d_in, 2, 3, d_aff, st) : point_sum_g1(d_in, 2, 3, d_aff, st);
+                  if (e != cudaSuccess) return e;
+                  return emit_rows(ec2, d_aff, 1, d_out, false, st);
+                });
+}
+void ec_jacadd_h(uint32_t* z, uint32_t* x, uint32_t* y, uint32_t pidx) { jacadd2(false, z, x, y, pidx, "ec_jacadd_h"); }
+void ec2_jacadd_h(uint32_t* z, uint32_t* x, uint32_t* y, uint32_t pidx) { jacadd2(true, z, x, y, pidx, "ec2_jacadd_h"); }
+void ec_jacdouble_h(uint32_t* z, uint32_t* x, uint32_t pidx) { jacadd2(false, z, x, x, pidx, "ec_jacdouble_h"); }
+void ec2_jacdouble_h(uint32_t* z, uint32_t* x, uint32_t pidx) { jacadd2(true, z, x, x, pidx, "ec2_jacdouble_h"); }
+
+// mpoly.cpp:266 / :278: the coefficient values of an mpoly (layout mpoly.cpp:195) to or from
+// Montgomery form, in place: gathered into one array, converted on the GPU, scattered back.
+static void mpoly_convert(uint32_t* x, uint32_t pidx, bool to_mont) {
+  std::vector<size_t> blocks;  // (offset, count) pairs
+  size_t total = 0;
+  size_t off = 1 + (size_t)x[0];
+  for (uint32_t i = 0; i < x[0]; i++) {
+    const uint32_t c = x[i + 1];
+    off += c;  // the constraint indices
+    blocks.push_back(off);
+    blocks.push_back(c);
+    total += c;
+    off += (size_t)c * 8;
+  }
+  std::vector<uint32_t> vals(total * 8);
+  size_t k = 0;
+  for (size_t b = 0; b < blocks.size(); b += 2) {
+    std::memcpy(&vals[k * 8], x + blocks[b], blocks[b + 1] * 32);
+    k += blocks[b + 1];
+  }
+  if (total) {
+    if (to_mont) to_montgomeryN_h(vals.data(), vals.data(), (uint32_t)total, pidx);
+    else from_montgomeryN_h(vals.data(), vals.data(), (uint32_t)total, pidx, 0);
+    if (cs_field_last_status() != CS_OK) {
+      dropin_status(cs_field_last_status(), to_mont ? "mpoly_to_montgomery_h" : "mpoly_from_montgomery_h");
+      return;
+    }
+  }
+  k = 0;
+  for (size_t b = 0; b < blocks.size(); b += 2) {
+    std::memcpy(x + blocks[b], &vals[k * 8], blocks[b + 1] * 32);
+    k += blocks[b + 1];
+  }
+  dropin_status(CS_OK, "");
+}
+void mpoly_to_montgomery_h(uint32_t* x, uint32_t pidx) { mpoly_convert(x, pidx, true); }
+void mpoly_from_montgomery_h(uint32_t* x, uint32_t pidx) { mpoly_convert(x, pidx, false); }
+
+// bigint.cpp / ff.cpp:626: U = A + B mod 2^256; samples[i] = start + i inc, reduced below mod
+// (when given) by repeated subtraction, as the reference does.
+void addu256_h(uint32_t* U, const uint32_t* A, const uint32_t* B) {
+  uint64_t c = 0;
+  for (int i = 0; i < 8; i++) {
+    c += (uint64_t)A[i] + B[i];
+    U[i] = (uint32_t)c;
+    c >>= 32;
+  }
+}
+static bool geq256(const uint32_t* a, const uint32_t* b) {
+  for (int i = 7; i >= 0; i--)
+    if (a[i] != b[i]) return a[i] > b[i];
+  return true;
+}
+void rangeu256_h(uint32_t* samples, uint32_t nsamples, const uint32_t* start, uint32_t inc, const uint32_t* mod) {
+  if (nsamples == 0) return;
+  const uint32_t step[8] = {inc, 0, 0, 0, 0, 0, 0, 0};
+  std::memcpy(samples, start, 32);
+  for (uint32_t i = 1; i < nsamples; i++) {
+    uint32_t* s = samples + (size_t)i * 8;
+    addu256_h(s, samples + (size_t)(i - 1) * 8, step);
+    while (mod && geq256(s, mod)) {
+      int64_t br = 0;
+      for (int k = 0; k < 8; k++) {
+        br += (int64_t)s[k] - mod[k];
+        s[k] = (uint32_t)br;
+        br >>= 32;
+      }
+    }
+  }
+}
+
 void ec_inittable_h(uint32_t* x, uint32_t* ectable, uint32_t n, uint32_t table_order, uint32_t pidx,
                     uint32_t add_last) {
   inittable(false, x, ectable, n, table_order, pidx, add_last);
@@ -325,6 +416,29 @@ void readU256CircuitFile_h(uint32_t* samples, const char* filename, unsigned lon
     while (std::fread(&samples[i], 4, 1, f) == 1) i++;
   }
   std::fclose(f);
+}
+// file_utils.cpp:49 / :447: the first header words of a circuit / proving-key file (the
+// proving-key reader takes the nine leading words in order, so its domainSize field holds
+// the file's domainBits word, as the reference's does).
+void readU256CircuitFileHeader_h(cirbin_hfile_t* h, const char* filename) {
+  FILE* f = std::fopen(filename, "rb");
+  if (!f) { dropin_status(CS_ERR_ARG, "readU256CircuitFileHeader_h: cannot open file"); return; }
+  unsigned long long w[9] = {0};
+  const size_t got = std::fread(w, sizeof(unsigned long long), 9, f);
+  std::fclose(f);
+  h->nWords = w[0]; h->nPubInputs = w[1]; h->nOutputs = w[2]; h->nVars = w[3]; h->nConstraints = w[4];
+  h->cirformat = w[5]; h->R1CSA_nWords = w[6]; h->R1CSB_nWords = w[7]; h->R1CSC_nWords = w[8];
+  dropin_status(got == 9 ? CS_OK : CS_ERR_ARG, got == 9 ? "" : "readU256CircuitFileHeader_h: short file");
+}
+void readU256PKFileHeader_h(pkbin_hfile_t* h, const char* filename) {
+  FILE* f = std::fopen(filename, "rb");
+  if (!f) { dropin_status(CS_ERR_ARG, "readU256PKFileHeader_h: cannot open file"); return; }
+  uint32_t w[9] = {0};
+  const size_t got = std::fread(w, 4, 9, f);
+  std::fclose(f);
+  h->nWords = w[0]; h->ftype = w[1]; h->protocol = w[2]; h->Rbitlen = w[3]; h->k_binformat = w[4];
+  h->k_ecformat = w[5]; h->nVars = w[6]; h->nPublic = w[7]; h->domainSize = w[8];
+  dropin_status(got == 9 ? CS_OK : CS_ERR_ARG, got == 9 ? "" : "readU256PKFileHeader_h: short file");
 }
 void readU256PKFile_h(uint32_t* samples, const char* filename, unsigned long long nwords) {
   readU256CircuitFile_h(samples, filename, nwords);

@@ -336,6 +336,20 @@ void ec_inittable_h(uint32_t *x, uint32_t *ectable, uint32_t n, uint32_t table_o
                     uint32_t add_last);
 void ec2_inittable_h(uint32_t *x, uint32_t *ectable, uint32_t n, uint32_t table_order, uint32_t pidx,
                      uint32_t add_last);
+/* ec.cpp:131 / :462 (and ec2_jacadd_h / ec2_jacdouble_h) -- one Jacobian addition / doubling;
+ * the result is returned normalised (Z = 1; infinity (0, 1, 0)): the reference's point. */
+void ec_jacadd_h(uint32_t *z, uint32_t *x, uint32_t *y, uint32_t pidx);
+void ec2_jacadd_h(uint32_t *z, uint32_t *x, uint32_t *y, uint32_t pidx);
+void ec_jacdouble_h(uint32_t *z, uint32_t *x, uint32_t pidx);
+void ec2_jacdouble_h(uint32_t *z, uint32_t *x, uint32_t pidx);
+/* mpoly.cpp:266 / :278 -- the mpoly's coefficient values (layout mpoly.cpp:195) from / to
+ * Montgomery form in place (converted on the GPU). */
+void mpoly_from_montgomery_h(uint32_t *x, uint32_t pidx);
+void mpoly_to_montgomery_h(uint32_t *x, uint32_t pidx);
+/* U = A + B mod 2^256 (the reference's addu256_h); ff.cpp:626 rangeu256_h: samples[i] =
+ * start + i inc, reduced below mod (if not NULL) by repeated subtraction. */
+void addu256_h(uint32_t *U, const uint32_t *A, const uint32_t *B);
+void rangeu256_h(uint32_t *samples, uint32_t nsamples, const uint32_t *start, uint32_t inc, const uint32_t *mod);
 /* ec.cpp:1153 / :1164 -- infinity flags with the reference's row addressing (G1: rows start
  * 2 j words into x; G2: every flag tests the row at word 4). */
 void ec_isinf(uint32_t *z, const uint32_t *x, const uint32_t n, const uint32_t pidx);
@@ -360,6 +374,18 @@ uint32_t get_nprocs_h(void);
  * (fmt 1), .dat values from byte 32 (fmt 0). */
 void readU256CircuitFile_h(uint32_t *samples, const char *filename, unsigned long long nwords);
 void readU256PKFile_h(uint32_t *samples, const char *filename, unsigned long long nwords);
+/* types.h cirbin_hfile_t / pkbin_hfile_t and file_utils.cpp:49 / :447: the leading header
+ * words of a circuit file (9 x uint64) and of a proving-key file (9 x uint32, read in order,
+ * so domainSize receives the file's domainBits word, as in the reference). */
+typedef struct {
+  unsigned long long nWords, nPubInputs, nOutputs, nVars, nConstraints, cirformat, R1CSA_nWords,
+      R1CSB_nWords, R1CSC_nWords;
+} cirbin_hfile_t;
+typedef struct {
+  uint32_t nWords, ftype, protocol, Rbitlen, k_binformat, k_ecformat, nVars, nPublic, domainSize;
+} pkbin_hfile_t;
+void readU256CircuitFileHeader_h(cirbin_hfile_t *hfile, const char *filename);
+void readU256PKFileHeader_h(pkbin_hfile_t *hfile, const char *filename);
 void readU256DataFile_h(uint32_t *samples, const char *filename, uint32_t insize, uint32_t outsize);
 void readU256DataFileFromOffset_h(uint32_t *samples, const char *filename, unsigned long long woffset,
                                   unsigned long long nwords);

@@ -7,8 +7,9 @@ by `make -C oracle ref`) for the binding's remaining host functions, on seeded i
   (Jacobian rows; affine rows with add_in), ec_jacscmul_h / ec2_jacscmul_h (Jacobian bases,
   one row per call: the reference's multi-row G1 call races), ec_jacsc1mul_h, ec_isoncurve_h / ec2_isoncurve_h, on Jacobian points made by
   the reference's own ec_jacscmul_h (so their Z are not 1) with a point at infinity mixed in.
-* ec_inittable_h / ec2_inittable_h (affine and Jacobian rows, a partial last table),
-  normalised by the reference's ec_jac2aff_h, and ec_isinf / ec2_isinf.
+* ec_inittable_h / ec2_inittable_h (affine and Jacobian rows, a partial last table) and
+  ec_jacadd_h / ec_jacdouble_h (G1, G2), normalised by the reference's ec_jac2aff_h;
+  ec_isinf / ec2_isinf; rangeu256_h; mpoly_to_montgomery_h / mpoly_from_montgomery_h.
 * sortu256_idx_h (top words drawn from a small range, so the unstable sort meets ties) and
   ntt_build_h for a range of sizes.
 """
@@ -54,6 +55,13 @@ def main():
                  1: fn(ref, "_Z15ec2_inittable_hPjS_jjjj", _vp, _vp, u, u, u, u)}
     isinf = {0: fn(ref, "_Z8ec_isinfPjPKjjj", _vp, _vp, u, u),
              1: fn(ref, "_Z9ec2_isinfPjPKjjj", _vp, _vp, u, u)}
+    jacadd = {0: fn(ref, "_Z11ec_jacadd_hPjS_S_j", _vp, _vp, _vp, u),
+              1: fn(ref, "_Z12ec2_jacadd_hPjS_S_j", _vp, _vp, _vp, u)}
+    jacdbl = {0: fn(ref, "_Z14ec_jacdouble_hPjS_j", _vp, _vp, u),
+              1: fn(ref, "_Z15ec2_jacdouble_hPjS_j", _vp, _vp, u)}
+    rangef = fn(ref, "_Z11rangeu256_hPjjPKjjS1_", _vp, u, _vp, u, _vp)
+    mpoly_to = fn(ref, "_Z21mpoly_to_montgomery_hPjj", _vp, u)
+    mpoly_from = fn(ref, "_Z23mpoly_from_montgomery_hPjj", _vp, u)
     build = fn(ref, "_Z11ntt_build_hP12fft_params_tj", _vp, u)
 
     rng = np.random.Generator(np.random.PCG64(31337))
@@ -124,6 +132,22 @@ def main():
             y = np.zeros((ent, 2 * fw), np.uint32)
             jac2aff[ec2](y.ctypes.data, tab.ctypes.data, ent, 0, 1)
             out[pre + f"inittable_{add_last}"] = y
+        # one Jacobian addition / doubling (rows with Z != 1, one at infinity), normalised by
+        # the reference's ec_jac2aff_h
+        adds = np.zeros((n, 3 * fw), np.uint32)
+        dbls = np.zeros((n, 3 * fw), np.uint32)
+        for i in range(n):
+            xi = np.ascontiguousarray(jac[i]); yi = np.ascontiguousarray(jac[(i + 1) % n])
+            zi = np.zeros(3 * fw, np.uint32)
+            jacadd[ec2](zi.ctypes.data, xi.ctypes.data, yi.ctypes.data, 0)
+            adds[i] = zi
+            zi = np.zeros(3 * fw, np.uint32)
+            jacdbl[ec2](zi.ctypes.data, xi.ctypes.data, 0)
+            dbls[i] = zi
+        for key, rows in (("jacadd", adds), ("jacdbl", dbls)):
+            y = np.zeros((n, 2 * fw), np.uint32)
+            jac2aff[ec2](y.ctypes.data, np.ascontiguousarray(rows).ctypes.data, n, 0, 1)
+            out[pre + key] = y
         # infinity flags, with the reference's row addressing: the affine rows, then a copy
         # with the infinity pattern planted where the reference looks (G1: 2 j words in for
         # j = 3; G2: X of the row at word 4)
@@ -151,6 +175,25 @@ def main():
         build(buf.ctypes.data, ns)
         params[k] = buf
     out["build_sizes"], out["build_params"] = np.array(sizes, np.uint64), params
+    # rangeu256_h: with and without a modulus, a start close to it
+    from oracle.oracle import ints_to_limbs as _limbs
+    R_ = 21888242871839275222246405745257275088548364400416034343698204186575808495617
+    start = np.ascontiguousarray(_limbs([R_ - 5])[0])
+    modv = np.ascontiguousarray(_limbs([R_])[0])
+    rg = np.zeros((12, 8), np.uint32)
+    rangef(rg.ctypes.data, 12, start.ctypes.data, 3, modv.ctypes.data)
+    rg0 = np.zeros((12, 8), np.uint32)
+    rangef(rg0.ctypes.data, 12, start.ctypes.data, 7, None)
+    out["range_start"], out["range_mod"], out["range_3"], out["range_7_nomod"] = start, modv, rg, rg0
+    # mpoly coefficients to / from Montgomery form (layout mpoly.cpp:195)
+    from cusnarks_b200.groth import mpoly_from_entries
+    nv, ents = 9, 30
+    pin = mpoly_from_entries(nv, rng.integers(0, nv, ents).astype(np.uint32),
+                             rng.integers(0, 16, ents).astype(np.uint32), random_field(rng, ents, 1))
+    pin = np.ascontiguousarray(pin, dtype=np.uint32)
+    p_to = pin.copy(); mpoly_to(p_to.ctypes.data, 1)
+    p_from = p_to.copy(); mpoly_from(p_from.ctypes.data, 1)
+    out["mpoly_in"], out["mpoly_to"], out["mpoly_from"] = pin, p_to, p_from
     np.savez_compressed(os.path.join(HERE, "dropin.npz"), **out)
     print("wrote", len(out), "arrays")
 

@@ -65,3 +65,48 @@ def test_isinf_matches_reference(golden):
             z = np.zeros(want.size, np.uint32)
             fn(z.ctypes.data, flat.ctypes.data, want.size, pidx)
             assert np.array_equal(z, want), (ec2, tag)
+
+
+def test_range_and_add_match_reference(golden):
+    g = golden("dropin.npz")
+    L = lib()
+    start = np.ascontiguousarray(g["range_start"]); mod = np.ascontiguousarray(g["range_mod"])
+    out = np.zeros((12, 8), np.uint32)
+    L.rangeu256_h(out.ctypes.data, 12, start.ctypes.data, 3, mod.ctypes.data)
+    assert np.array_equal(out, g["range_3"])
+    out = np.zeros((12, 8), np.uint32)
+    L.rangeu256_h(out.ctypes.data, 12, start.ctypes.data, 7, None)
+    assert np.array_equal(out, g["range_7_nomod"])
+    a = np.array([0xffffffff] * 8, np.uint32); b = np.array([2] + [0] * 7, np.uint32)
+    u = np.zeros(8, np.uint32)
+    L.addu256_h(u.ctypes.data, a.ctypes.data, b.ctypes.data)
+    assert list(u) == [1] + [0] * 7  # mod 2^256
+
+
+def test_file_headers(tmp_path):
+    """readU256PKFileHeader_h takes the nine leading words in order (its domainSize field gets
+    the file's domainBits word, as the reference's does); readU256CircuitFileHeader_h nine
+    uint64 words."""
+    from cusnarks_b200._lib import lib as _l
+    import ctypes as C
+
+    class PkHdr(C.Structure):
+        _fields_ = [(n, C.c_uint32) for n in ("nWords", "ftype", "protocol", "Rbitlen", "k_binformat",
+                                              "k_ecformat", "nVars", "nPublic", "domainSize")]
+
+    class CirHdr(C.Structure):
+        _fields_ = [(n, C.c_ulonglong) for n in ("nWords", "nPubInputs", "nOutputs", "nVars", "nConstraints",
+                                                 "cirformat", "R1CSA_nWords", "R1CSB_nWords", "R1CSC_nWords")]
+
+    words = np.array([1000, 1, 1, 256, 1, 2, 20, 1, 5, 32] + [0] * 8, np.uint32)
+    p = tmp_path / "pk.bin"
+    words.tofile(p)
+    h = PkHdr()
+    _l().readU256PKFileHeader_h(C.byref(h), str(p).encode())
+    assert [getattr(h, f) for f, _ in PkHdr._fields_] == list(words[:9])
+    w64 = np.arange(10, 19, dtype=np.uint64)
+    q = tmp_path / "c.bin"
+    w64.tofile(q)
+    c = CirHdr()
+    _l().readU256CircuitFileHeader_h(C.byref(c), str(q).encode())
+    assert [getattr(c, f) for f, _ in CirHdr._fields_] == list(w64)

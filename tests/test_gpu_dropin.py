@@ -67,3 +67,33 @@ def test_inittable_matches_reference(golden, ec2):
         want = g[pre + f"inittable_{add_last}"]
         # Z = 1 rows are affine; the Jacobian infinity (0, 1, 0) is the affine infinity (0, 1)
         assert np.array_equal(tab[:, :2 * fw], want), add_last
+
+
+@pytest.mark.parametrize("ec2", [0, 1])
+def test_jacadd_jacdouble_match_reference(golden, ec2):
+    L = lib()
+    g = golden("dropin.npz")
+    pre = f"g{ec2 + 1}_"
+    fw = 16 if ec2 else 8
+    jac = np.ascontiguousarray(g[pre + "jac"])
+    n = jac.shape[0]
+    add = L.ec2_jacadd_h if ec2 else L.ec_jacadd_h
+    dbl = L.ec2_jacdouble_h if ec2 else L.ec_jacdouble_h
+    for i in range(n):
+        z = np.zeros(3 * fw, np.uint32)
+        add(z.ctypes.data, np.ascontiguousarray(jac[i]).ctypes.data,
+            np.ascontiguousarray(jac[(i + 1) % n]).ctypes.data, 0)
+        assert np.array_equal(z[:2 * fw], g[pre + "jacadd"][i]), i
+        z = np.zeros(3 * fw, np.uint32)
+        dbl(z.ctypes.data, np.ascontiguousarray(jac[i]).ctypes.data, 0)
+        assert np.array_equal(z[:2 * fw], g[pre + "jacdbl"][i]), i
+
+
+def test_mpoly_montgomery_match_reference(golden):
+    L = lib()
+    g = golden("dropin.npz")
+    p = np.ascontiguousarray(g["mpoly_in"]).copy()
+    L.mpoly_to_montgomery_h(p.ctypes.data, 1)
+    assert np.array_equal(p, g["mpoly_to"])
+    L.mpoly_from_montgomery_h(p.ctypes.data, 1)
+    assert np.array_equal(p, g["mpoly_from"])
