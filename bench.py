@@ -495,7 +495,7 @@ def run_ours(args, world, rank, local):
     wall, lat_sat = served_run(srv, jobs)
     e2e_ms = max_over_ranks(wall * 1e3 / len(jobs), world)
     # latency under a Poisson stream at 70% of the saturated rate
-    wall_p, lat = served_run(srv, jobs * max(4, 40 // len(jobs)), rate_hz=0.7 * 1e3 / e2e_ms, seed=11)
+    wall_p, lat = served_run(srv, jobs * max(12, 120 // len(jobs)), rate_hz=0.7 * 1e3 / e2e_ms, seed=11)
     srv.close()
     # plain per-call path: the reference's flow through the drop-in entry points
     from cusnarks_b200.groth import pk_to_host
