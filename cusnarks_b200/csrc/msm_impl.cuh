@@ -854,7 +854,10 @@ inline int auto_affine_rounds_rt(bool ec2, uint32_t n, int W, size_t nb) {
   if ((uint64_t)n * W < (1ull << 23)) return 0;
   // G1 rounds measured slower, alone and inside proofs (2^20 proof 29.1 -> 30.2 ms with one
   // round, 30.7 ms with two): its mixed addition is cheap enough that the extra passes lose
-  const int cap = ec2 ? 2 : 0;
+#ifndef CSB_AFF_G2_CAP
+#define CSB_AFF_G2_CAP 2
+#endif
+  const int cap = ec2 ? CSB_AFF_G2_CAP : 0;
   const double avg = (double)n * W / (double)nb;
   int r = 0;
   while (r < cap && avg >= (double)(8u << r)) r++;
