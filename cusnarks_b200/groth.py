@@ -20,7 +20,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import lib, check, PkDesc
+from ._lib import lib, check, PkDesc, CsError, CS_ERR_NOMEM
 from .context import Context
 from . import synth
 
@@ -284,8 +284,16 @@ class Prover:
         self.n_vars = pk["n_vars"]
         self._keep.clear()
         del torch
+        self.fixed_base_note = None
         if fixed_base >= 0:
-            self.set_fixed_base(fixed_base)
+            try:
+                self.set_fixed_base(fixed_base)
+            except CsError as e:
+                # automatic tables (~13x the key's points) that do not fit in device memory:
+                # the key stays without them and proofs run the generic MSM over its points
+                if fixed_base != 0 or e.code != CS_ERR_NOMEM:
+                    raise
+                self.fixed_base_note = f"fixed-base tables left out: {e}"
 
     def set_fixed_base(self, window: int = 0):
         """Builds (window >= 0) or drops (window < 0) the key's fixed-base tables."""

@@ -118,3 +118,30 @@ def test_netserver_missing_witness(tmp_path):
         srv.close()
         prover.close()
         ctx.close()
+
+
+def test_prover_without_room_for_tables_proves_generically():
+    """Automatic fixed-base tables that cannot be allocated (injected failure) leave the key
+    without tables; the proofs then run the generic MSM and are the same bytes."""
+    from cusnarks_b200 import Context, lib
+    from cusnarks_b200.groth import SyntheticCircuit, setup_pk, Prover
+    ctx = Context(0)
+    circ = SyntheticCircuit(ctx, 8, seed=91)
+    pk = setup_pk(ctx, circ, seed=92)
+    r, s = ints_to_limbs([17])[0], ints_to_limbs([19])[0]
+    ref = Prover(ctx, pk)
+    assert ref.fixed_windows()[0] > 0 and ref.fixed_base_note is None
+    want = ref.prove(circ.w, r, s)
+    ref.close()
+    ctx2 = Context(0)              # fresh arenas: the table build must allocate scratch
+    try:
+        lib().cs_debug_fail_allocs(1)
+        p2 = Prover(ctx2, pk)
+        lib().cs_debug_fail_allocs(0)
+        assert p2.fixed_windows() == [0, 0, 0, 0, 0] and p2.fixed_base_note
+        assert np.array_equal(p2.prove(circ.w, r, s), want)
+        p2.close()
+    finally:
+        lib().cs_debug_fail_allocs(0)
+        ctx2.close()
+        ctx.close()
