@@ -4,10 +4,11 @@
 // x * 2^256 mod p, always fully reduced to [0, p) at the boundary of every operation, so
 // results are word-for-word the values the reference's host code produces
 // (src/cuda/ff.cpp montmult_h / addm_h / subm_h, same layout as src/cuda/types.h
-// NWORDS_256BIT).  Products are CIOS Montgomery multiplications built from
-// mad.lo.cc / madc.hi.cc carry chains (IMAD with carry-in/out).  BN254 moduli are below
-// 2^254, so the CIOS accumulator never needs a tenth limb and a single conditional
-// subtraction finishes every product.
+// NWORDS_256BIT).  Products are CIOS Montgomery multiplications on 32x32->64 wide
+// products folded by add-with-carry chains; BN254 moduli are below 2^254, so the CIOS
+// accumulator never needs a tenth limb and a single conditional subtraction finishes
+// every product.  Units that call products out of line (the G1 MSM) compute the same
+// Montgomery product in radix 2^52 on the FP64 pipe instead (namespace dp52).
 #pragma once
 #include <cstdint>
 
@@ -37,6 +38,12 @@ struct ModQ {  // base field q (the reference's MOD_GROUP, pidx 0)
                                 0x0348d21cu, 0x599a6f7cu, 0x763cbf9cu, 0x0925c4b8u};
     return k[i];
   }
+  // q in radix 2^52 and -q^-1 mod 2^52 (FP64-pipe product)
+  static CSB_DEV double L52(int i) {
+    return i == 0 ? 154029749239111.0 : i == 1 ? 2558044347618242.0 : i == 2 ? 423691504025962.0
+         : i == 3 ? 2817616741948264.0 : 53207371014449.0;
+  }
+  static constexpr double NP52 = 571208714576777.0;
 };
 struct ModR {  // scalar field r (the reference's MOD_FIELD, pidx 1)
   static constexpr uint32_t P0 = 0xf0000001u, P1 = 0x43e1f593u, P2 = 0x79b97091u, P3 = 0x2833e848u,
@@ -48,7 +55,114 @@ struct ModR {  // scalar field r (the reference's MOD_FIELD, pidx 1)
                             R24 = 0x53bb8085u, R25 = 0x8c49833du, R26 = 0x7f4e44a5u, R27 = 0x0216d0b1u;
   static constexpr uint32_t R30 = 0xb4bf0040u, R31 = 0x5e94d8e1u, R32 = 0x1cfbb6b8u, R33 = 0x2a489cbeu,
                             R34 = 0xa19fcfedu, R35 = 0x893cc664u, R36 = 0x7fcc657cu, R37 = 0x0cf8594bu;
+  static CSB_DEV double L52(int i) {
+    return i == 0 ? 551490712240129.0 : i == 1 ? 1275002230477886.0 : i == 2 ? 423691496731624.0
+         : i == 3 ? 2817616741948264.0 : 53207371014449.0;
+  }
+  static constexpr double NP52 = 551490712240127.0;
 };
+
+// ------------------------------------------------- products on the FP64 pipe ----------
+// Montgomery product in radix 2^52 (Emmart, Zheng and Weems, "Faster modular
+// exponentiation using double precision floating point arithmetic on the GPU", ARITH
+// 2018): limbs are exact integers held in doubles; a 52x52-bit product x*y < 2^104 splits
+// exactly into its high and low 52 bits with two round-toward-zero FMAs,
+//   h = fma_rz(x, y, 2^104)            = 2^104 + H 2^52   (bits of h: exponent | H)
+//   l = fma_rz(x, y, 2^104 + 2^52 - h) = 2^52 + L         (bits of l: exponent | L),
+// and the raw bit patterns are summed per column in 64-bit integers, the exponent bits
+// taken off in bulk by the column's starting value.  The multiplies run on the FP64 pipe
+// and the column sums on the integer ALU, which a 32-bit CIOS leaves saturated by its
+// add-with-carry chains (B200: 56 vs 46 G lazy products/s).
+// The 8x32-bit operands are re-cut into five 52-bit limbs, one of them shifted left by 4:
+// REDC in radix 2^52 divides by 2^260, so the result is a*b*2^-256 mod p, the same
+// Montgomery product as the 32-bit CIOS.  For a, b < 2p it is below
+// 16 a b / 2^260 + p < 2p (BN254: 64 p / 2^260 < 0.77), a lazily reduced value.
+#ifndef CSB_DP52
+#define CSB_DP52 1
+#endif
+namespace dp52 {
+constexpr uint64_t kMask = 0x000FFFFFFFFFFFFFull;
+constexpr uint64_t kBitsLo = 0x4330000000000000ull;  // bits of 2^52
+constexpr uint64_t kBitsHi = 0x4670000000000000ull;  // bits of 2^104
+// x*y into the column pair (lo: bits 0..51 of the product, hi: bits 52..103)
+CSB_DEV void acc_prod(double x, double y, uint64_t& lo, uint64_t& hi) {
+  const double h = __fma_rz(x, y, 0x1p104);
+  const double l = __fma_rz(x, y, 0x1.0000000000001p104 - h);
+  lo += (uint64_t)__double_as_longlong(l);
+  hi += (uint64_t)__double_as_longlong(h);
+}
+// products landing in column k of a 5x5 schoolbook product
+__host__ __device__ constexpr int terms(int k) { return (k < 0 || k > 8) ? 0 : (k < 4 ? k + 1 : 9 - k); }
+// column k starts at minus the exponent bits of its terms: a*b and m*p each put terms(k)
+// low halves and terms(k-1) high halves into it
+__host__ __device__ constexpr uint64_t col_start(int k) {
+  return (uint64_t)0 - (uint64_t)(2 * terms(k)) * kBitsLo - (uint64_t)(2 * terms(k - 1)) * kBitsHi;
+}
+// integer v < 2^52 as a double
+CSB_DEV double to_dbl(uint64_t v) { return __longlong_as_double((long long)(v | kBitsLo)) - 0x1p52; }
+CSB_DEV void words(const uint32_t (&x)[8], uint64_t (&w)[4]) {
+#pragma unroll
+  for (int i = 0; i < 4; i++) w[i] = x[2 * i] | (uint64_t)x[2 * i + 1] << 32;
+}
+// x = sum l_i 2^(52 i)
+CSB_DEV void cut(const uint32_t (&x)[8], double (&l)[5]) {
+  uint64_t w[4];
+  words(x, w);
+  l[0] = to_dbl(w[0] & kMask);
+  l[1] = to_dbl(((w[0] >> 52) | (w[1] << 12)) & kMask);
+  l[2] = to_dbl(((w[1] >> 40) | (w[2] << 24)) & kMask);
+  l[3] = to_dbl(((w[2] >> 28) | (w[3] << 36)) & kMask);
+  l[4] = to_dbl(w[3] >> 16);
+}
+// 16 x = sum l_i 2^(52 i)
+CSB_DEV void cut16(const uint32_t (&x)[8], double (&l)[5]) {
+  uint64_t w[4];
+  words(x, w);
+  l[0] = to_dbl((w[0] << 4) & kMask);
+  l[1] = to_dbl(((w[0] >> 48) | (w[1] << 16)) & kMask);
+  l[2] = to_dbl(((w[1] >> 36) | (w[2] << 28)) & kMask);
+  l[3] = to_dbl(((w[2] >> 24) | (w[3] << 40)) & kMask);
+  l[4] = to_dbl(w[3] >> 12);
+}
+// a*b*2^-256 mod p, lazily reduced (< 2p for a, b < 2p)
+template <class M>
+CSB_DEV void mont(const uint32_t (&x)[8], const uint32_t (&y)[8], uint32_t (&out)[8]) {
+  double a[5], b[5];
+  cut16(x, a);
+  cut(y, b);
+  uint64_t c[10];
+#pragma unroll
+  for (int k = 0; k < 10; k++) c[k] = col_start(k);
+#pragma unroll
+  for (int i = 0; i < 5; i++)
+#pragma unroll
+    for (int j = 0; j < 5; j++) acc_prod(a[i], b[j], c[i + j], c[i + j + 1]);
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    if (k > 0) c[k] += c[k - 1] >> 52;  // column k-1 is complete (and 0 mod 2^52)
+    // m = (c_k mod 2^52) * (-p^-1) mod 2^52: the low half of one more split product
+    const double t = to_dbl(c[k] & kMask);
+    const double h = __fma_rz(t, M::NP52, 0x1p104);
+    const double m = __fma_rz(t, M::NP52, 0x1.0000000000001p104 - h) - 0x1p52;
+#pragma unroll
+    for (int j = 0; j < 5; j++) acc_prod(m, M::L52(j), c[k + j], c[k + j + 1]);
+  }
+  uint64_t r[5];
+  uint64_t carry = c[4] >> 52;
+#pragma unroll
+  for (int j = 0; j < 5; j++) {
+    const uint64_t v = c[5 + j] + carry;
+    carry = v >> 52;
+    r[j] = j < 4 ? (v & kMask) : v;
+  }
+  const uint64_t w0 = r[0] | (r[1] << 52), w1 = (r[1] >> 12) | (r[2] << 40);
+  const uint64_t w2 = (r[2] >> 24) | (r[3] << 28), w3 = (r[3] >> 36) | (r[4] << 16);
+  out[0] = (uint32_t)w0; out[1] = (uint32_t)(w0 >> 32);
+  out[2] = (uint32_t)w1; out[3] = (uint32_t)(w1 >> 32);
+  out[4] = (uint32_t)w2; out[5] = (uint32_t)(w2 >> 32);
+  out[6] = (uint32_t)w3; out[7] = (uint32_t)(w3 >> 32);
+}
+}  // namespace dp52
 
 // Paired products (CSB_PAIR, opt-in; only with out-of-line products): Fp::mul2 computes two
 // independent products in one call with their rows interleaved.  Measured at 2^20: the G1
@@ -560,8 +674,12 @@ using Fr = Fp<ModR>;
 // ------------------------------------------------------------ Fq2 = Fq[u]/(u^2+1) ----
 template <class M>
 __device__ __noinline__ Fp<M> fp_mul_call(Fp<M> a, Fp<M> b) {
-#ifdef CSB_MUL_CALL_LOHI
+#if defined(CSB_MUL_CALL_LOHI)
   return Fp<M>::mul_lohi(a, b);
+#elif CSB_DP52
+  Fp<M> r;
+  dp52::mont<M>(a.v, b.v, r.v);
+  return r.canon();
 #else
   return Fp<M>::mul_wide(a, b);
 #endif
@@ -569,7 +687,13 @@ __device__ __noinline__ Fp<M> fp_mul_call(Fp<M> a, Fp<M> b) {
 
 template <class M>
 __device__ __noinline__ Fp<M> fp_mul_lazy_call(Fp<M> a, Fp<M> b) {
+#if CSB_DP52
+  Fp<M> r;
+  dp52::mont<M>(a.v, b.v, r.v);
+  return r;
+#else
   return Fp<M>::mul_wide_lazy(a, b);
+#endif
 }
 
 template <class M>

@@ -2,6 +2,11 @@
 // Montgomery products out of line: the accumulation loop body (one XYZZ + affine
 // addition, 10 products) then fits the instruction cache; measured faster at 2^20.
 #define CSB_MUL_NOINLINE
+// Fq products stay 32-bit CIOS here: the FP64-pipe product needs more registers than
+// the 168 the Fq2 kernels run at (G2 fixed-base MSM 13.1 -> 13.9 ms with it).
+#ifndef CSB_DP52
+#define CSB_DP52 0
+#endif
 #include "msm_impl.cuh"
 
 namespace csb {
