@@ -60,7 +60,7 @@ PRODUCTS_PER_MONT = 136
 MONT_PER_MADD = 11     # mixed addition, 7M + 4S (the canonical count of the MSM cost model)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_accumulate launch of
 # the 2^20 G1 MSM (window 16), from an ncu capture of that launch
-ACC_TRAFFIC_BYTES = 436_821_248 + 61_684_480
+ACC_TRAFFIC_BYTES = 439_780_864 + 60_918_784
 L2_BYTES = 126 * 1024 * 1024
 LOG_M = 20
 CPU_SAMPLE_LOG_M = 16
@@ -555,14 +555,16 @@ def run_ours(args, world, rank, local):
                                     "points copied per call; wall clock"},
         "served_vs_plain": round(e2e_val * plain_ms / 1e3, 2),
         "g1_msm_2^20_ms": round(statistics.median(msm_ms), 3),
-        "roofline": {"bound": "int (IMAD.WIDE pipe)", "kernel": "k_accumulate+k_combine (MSM bucket accumulation)",
+        "roofline": {"bound": "int issue (ALU column sums + FP64 split products)", "kernel": "k_accumulate+k_combine (MSM bucket accumulation)",
                      "achieved": round(achieved / 1e12, 4), "peak": round(peak_wide / 1e12, 4),
                      "unit": "T wide products/s", "frac": round(achieved / peak_wide, 4),
                      "traffic": ACC_TRAFFIC_BYTES, "kernel_ms": round(acc, 4), "units_per_launch": units,
                      "window": window,
                      "basis": "2^20 G1 MSM: N*W bucket entries x 11 Montgomery products x 136 32x32->64 "
                               "products / kernel ms (CUDA events around the kernels); peak = live "
-                              "mad.wide.u32 rate (cs_bench_pipe mode 3); traffic = ncu DRAM bytes per launch"},
+                              "mad.wide.u32 rate (cs_bench_pipe mode 3), the ceiling of a 32-bit CIOS "
+                              "product (this kernel computes products in radix 2^52 on the FP64 pipe); "
+                              "traffic = ncu DRAM bytes per launch"},
         "e2e": {"value": round(e2e_val, 3), "unit": UNIT, "ms": round(e2e_ms, 3),
                 "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes,
                 "basis": f"C-ABI prove server ({args.slots} slots), {len(jobs)} requests submitted at once, "

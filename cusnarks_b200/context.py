@@ -125,7 +125,7 @@ class Context:
 
     # -------------------------------------------------------------- field ops -----
     FOP = {"mul": 0, "add": 1, "sub": 2, "sqr": 3, "inv": 4, "to_mont": 5, "from_mont": 6,
-           "mul_lohi": 7, "fq2_mul": 8}
+           "mul_lohi": 7, "fq2_mul": 8, "mul_dp52": 9}
 
     def field_op_device(self, op: str, pidx: int, d_a: int, d_b: int, d_out: int, n: int):
         check(self._lib.cs_field_op_device(self.handle, self.FOP[op], pidx, ctypes.c_void_p(d_a),

@@ -269,6 +269,7 @@ int cs_msm_tuned_window(cs_ctx *ctx, int ec2, uint32_t n);
 #define CS_FOP_FROM_MONT 6 /* aR -> a */
 #define CS_FOP_MUL_LOHI 7  /* Montgomery product, mad.lo/mad.hi variant (cross-check) */
 #define CS_FOP_FQ2_MUL 8
+#define CS_FOP_MUL_DP52 9  /* Montgomery product, radix-2^52 FP64-pipe variant (cross-check) */
 int cs_field_op_device(cs_ctx *ctx, int op, int pidx, const uint32_t *d_a, const uint32_t *d_b,
                        uint32_t *d_out, uint32_t n);
 

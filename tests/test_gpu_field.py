@@ -41,6 +41,7 @@ def test_binary_ops(ctx, oracle, pidx):
     want_mul = oracle.montmult(a, b, pidx)
     assert np.array_equal(_run(ctx, "mul", pidx, a, b), want_mul)
     assert np.array_equal(_run(ctx, "mul_lohi", pidx, a, b), want_mul)
+    assert np.array_equal(_run(ctx, "mul_dp52", pidx, a, b), want_mul)
     z_add = np.zeros_like(a); z_sub = np.zeros_like(a)
     P = ctypes.POINTER(ctypes.c_uint32)
     for i in range(a.shape[0]):
@@ -97,3 +98,23 @@ def test_dropin_field_entry_points(oracle):
     assert np.array_equal(z, oracle.from_mont(a, 1))
     L.from_montgomeryN_h(z.ctypes.data, a.ctypes.data, 64, 1, 2)
     assert L.cs_field_last_status() == 4  # unsupported option reported, no exit
+
+
+@pytest.mark.parametrize("pidx", [0, 1])
+def test_mul_dp52_lazy_inputs(ctx, oracle, pidx):
+    """The radix-2^52 product takes lazily reduced operands in [0, 2p) (what the G1 bucket
+    accumulation feeds it): x + p and y + p give the same canonical product as x and y."""
+    rng = np.random.Generator(np.random.PCG64(51 + pidx))
+    p = MOD[pidx]
+    a = np.concatenate([random_field(rng, 2000, pidx), _edge(p)])
+    b = np.concatenate([random_field(rng, 2000, pidx), _edge(p)[::-1]])
+    want = oracle.montmult(a, b, pidx)
+
+    def plus_p(x):
+        vals = [int.from_bytes(r.tobytes(), "little") + p for r in x]
+        return ints_to_limbs(vals)
+    n = a.shape[0]
+    mix = np.arange(n)
+    a2 = np.where((mix & 1)[:, None] == 1, plus_p(a), a).astype(np.uint32)
+    b2 = np.where((mix & 2)[:, None] == 2, plus_p(b), b).astype(np.uint32)
+    assert np.array_equal(_run(ctx, "mul_dp52", pidx, a2, b2), want)
