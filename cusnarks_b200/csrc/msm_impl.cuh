@@ -853,11 +853,17 @@ inline int auto_affine_rounds_rt(bool ec2, uint32_t n, int W, size_t nb) {
   // (2 rounds cost 2.5 ms in a 2^12-term G2 MSM)
   if ((uint64_t)n * W < (1ull << 23)) return 0;
   // G1 rounds measured slower, alone and inside proofs (2^20 proof 29.1 -> 30.2 ms with one
-  // round, 30.7 ms with two): its mixed addition is cheap enough that the extra passes lose
+  // round, 30.7 ms with two; with the FP64-pipe products 26.5 -> 29.1 ms with one round, the
+  // 2^20 fixed-base MSM 4.28 -> 5.20 ms): its mixed addition is cheap enough that the extra
+  // passes lose.  L2 prefetching the round's gathers a few slots ahead did not help either
+  // (G2 fixed-base 13.10 ms without, 13.27 / 13.31 / 13.40 ms 2 / 4 / 8 slots ahead).
 #ifndef CSB_AFF_G2_CAP
 #define CSB_AFF_G2_CAP 2
 #endif
-  const int cap = ec2 ? CSB_AFF_G2_CAP : 0;
+#ifndef CSB_AFF_G1_CAP
+#define CSB_AFF_G1_CAP 0
+#endif
+  const int cap = ec2 ? CSB_AFF_G2_CAP : CSB_AFF_G1_CAP;
   const double avg = (double)n * W / (double)nb;
   int r = 0;
   while (r < cap && avg >= (double)(8u << r)) r++;
