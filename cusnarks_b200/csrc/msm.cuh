@@ -77,6 +77,14 @@ struct MsmConfig {
   int affine = -1;    // batch-affine halving rounds before the XYZZ accumulation: -1 auto, 0 off
   // optional events recorded around the bucket-accumulation kernels (phase timing)
   cudaEvent_t acc_start = nullptr, acc_stop = nullptr;
+  // Two fixed-base MSMs with the same window whose sums are added (a proof's C and H terms)
+  // share one bucket reduction.  bucket_out: the MSM accumulates into that array (2^(c-1)
+  // XYZZ buckets), skips the reduction and returns the point at infinity.  bucket_add: after
+  // its own accumulation (and after waiting for bucket_ready when given) the MSM adds that
+  // array into its buckets, so its result is the sum of both MSMs.
+  uint32_t* bucket_out = nullptr;
+  const uint32_t* bucket_add = nullptr;
+  cudaEvent_t bucket_ready = nullptr;
 };
 
 // Bytes of device scratch one MSM of n terms needs (G2 when ec2).

@@ -336,6 +336,18 @@ __global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate_quad
   }
 }
 
+// buckets[b] += add[b] (XYZZ, canonical): folds another fixed-base MSM's buckets (same window)
+// into this one's before the reduction.
+template <class F>
+__global__ void __launch_bounds__(128) k_add_buckets(uint32_t* __restrict__ buckets, const uint32_t* __restrict__ add,
+                                                     uint32_t nb) {
+  constexpr int XW = 4 * FieldWords<F>::value;
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const XYZZ<F> x = ld_xyzz<F>(buckets + (size_t)b * XW), y = ld_xyzz<F>(add + (size_t)b * XW);
+  st_xyzz<F>(buckets + (size_t)b * XW, xyzz_add(x, y));
+}
+
 // Split buckets with at most kCombineSerial partials: one thread each, a serial sum.
 // (The top window of a scalar has fewer bits, so its digits crowd into fewer buckets and
 // many of those split into two or three tasks.)
@@ -916,6 +928,10 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
                      cudaStream_t st) {
   constexpr bool EC2 = FieldWords<F>::value == 16;
   constexpr int XB = 4 * FieldWords<F>::value * 4;  // bytes per XYZZ point
+  // shared buckets: fixed-base MSMs (one bucket set) with terms (the accumulation is what
+  // writes every bucket of the array)
+  if ((cfg.bucket_out || cfg.bucket_add) && (!FIXED || n == 0)) return cudaErrorInvalidValue;
+  if (cfg.bucket_out && cfg.bucket_add) return cudaErrorInvalidValue;
   if (n == 0) {
     k_store_inf<F><<<1, 32, 0, st>>>(d_out);
     note_launch();
@@ -950,7 +966,7 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   Task* tasks = reinterpret_cast<Task*>(base + L.tasks);
   Multi* multi = reinterpret_cast<Multi*>(base + L.multi);
   uint32_t* partials = reinterpret_cast<uint32_t*>(base + L.partials);
-  uint32_t* buckets = reinterpret_cast<uint32_t*>(base + L.buckets);
+  uint32_t* buckets = cfg.bucket_out ? cfg.bucket_out : reinterpret_cast<uint32_t*>(base + L.buckets);
   uint32_t* lv_y = reinterpret_cast<uint32_t*>(base + L.lv_y);
   uint32_t* lv_z = reinterpret_cast<uint32_t*>(base + L.lv_z);
   uint32_t* lv_y2 = reinterpret_cast<uint32_t*>(base + L.lv_y2);
@@ -1022,9 +1038,19 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   k_combine<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);
   note_launch(2);
   if (cfg.acc_stop) cudaEventRecord(cfg.acc_stop, st);
-  // level 0: segments of 8 buckets -> totals y and in-segment weighted sums z
   const int WR = FIXED ? 1 : W;
   const uint32_t B = 1u << (c - 1);
+  if (cfg.bucket_out) {  // buckets handed on: this MSM's own result is the point at infinity
+    k_store_inf<F><<<1, 32, 0, st>>>(d_out);
+    note_launch();
+    return cudaGetLastError();
+  }
+  if (cfg.bucket_add) {
+    if (cfg.bucket_ready) cudaStreamWaitEvent(st, cfg.bucket_ready, 0);
+    k_add_buckets<F><<<(B + 127) / 128, 128, 0, st>>>(buckets, cfg.bucket_add, B);
+    note_launch();
+  }
+  // level 0: segments of 8 buckets -> totals y and in-segment weighted sums z
   uint32_t nseg = (B + 7) / 8;
   reduce_level<F>(buckets, nullptr, B, nseg, WR, 0, lv_y, lv_z, resident, st);
   int levels = 1;

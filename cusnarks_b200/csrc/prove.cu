@@ -12,7 +12,10 @@
 //   pi_C2 = MSM(polH ++ [-r s], hExps[0 .. m-2] ++ [delta_1])
 //   pi_C <- pi_C2 + pi_C + s pi_A + r pi_B1
 // The four witness MSMs run on separate streams and overlap the QAP/H-step chain; the
-// scalings s pi_A and r pi_B1 start as soon as their MSM finishes.
+// scalings s pi_A and r pi_B1 start as soon as their MSM finishes.  With fixed-base tables
+// of one window for C and H, the C MSM accumulates its buckets early (beside the H step) and
+// hands them to the H MSM, which adds them to its own before its reduction: pi_C + pi_C2 from
+// one bucket reduction instead of two (the same group element, so the same affine proof).
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -255,8 +258,11 @@ uint32_t ilog2_exact(uint32_t m) {
 
 // Layout of the per-call prove scratch.
 struct ProvePlan {
-  size_t wA, wB, pA, pB, M, hscr, ms_a, ms_b1, ms_b2, ms_c, ms_h, pts, rs, total;
+  size_t wA, wB, pA, pB, M, hscr, ms_a, ms_b1, ms_b2, ms_c, ms_h, pts, rs, cbk, total;
   size_t bytes_a, bytes_b1, bytes_b2, bytes_c, bytes_h;
+  // C and H share one bucket reduction: both fixed-base with the same window, C's buckets
+  // (cbk) folded into H's before H reduces (pi_C only needs their sum)
+  bool share_ch;
 };
 
 ProvePlan plan_prove(const cs_pk* pk) {
@@ -290,6 +296,9 @@ ProvePlan plan_prove(const cs_pk* pk) {
   P.ms_h = o; o += al256(P.bytes_h);
   P.pts = o; o += 2048;   // outA 64, outB1 64, outB2 128, outC 64, outH 64, sA 128, rB1 128, piC 64
   P.rs = o; o += 256;     // r, s, -rs, then the GLV splits of s and r (2 x 64 B)
+  P.share_ch = pk->has_fixed() && pk->fc.c > 0 && pk->fc.c == pk->fh.c && pk->fc.n > 0 && pk->fh.n > 0;
+  P.cbk = o;
+  if (P.share_ch) o += al256(((size_t)1 << (pk->fc.c - 1)) * 128);  // G1 XYZZ buckets
   P.total = o;
   return P;
 }
@@ -479,21 +488,29 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
   for (int i = 0; i < 4; i++) cudaStreamWaitEvent(ctx->aux[i], ev_w, 0);
   // resident fixed-base tables when the key has them, else the generic MSM over the points
   auto run_msm = [&](bool ec2, const uint32_t* sc, const uint32_t* pts, const cs_pk::Fixed& f, uint32_t n,
-                     uint32_t* out, size_t off, size_t bytes, cudaStream_t st) {
+                     uint32_t* out, size_t off, size_t bytes, cudaStream_t st, const MsmConfig* share = nullptr) {
     if (pk->has_fixed()) {
-      MsmConfig fcfg;
+      MsmConfig fcfg = share ? *share : MsmConfig{};
       fcfg.c = f.c;
       return ec2 ? msm_fixed_g2(sc, f.table, n, out, at(off), bytes, fcfg, st)
                  : msm_fixed_g1(sc, f.table, n, out, at(off), bytes, fcfg, st);
     }
     return ec2 ? msm_g2(sc, pts, n, out, at(off), bytes, cfg, st) : msm_g1(sc, pts, n, out, at(off), bytes, cfg, st);
   };
+  // C hands its buckets to H (outC is then the point at infinity, and outH the sum of both)
+  MsmConfig share_c, share_h;
+  if (P.share_ch) {
+    share_c.bucket_out = at(P.cbk);
+    share_h.bucket_add = at(P.cbk);
+    share_h.bucket_ready = ctx->aux_ev[7];
+  }
   ok = (e = run_msm(false, wA, pk->a_ext, pk->fa, nv + 2, outA, P.ms_a, P.bytes_a, sa)) == cudaSuccess &&
        (e = run_msm(false, wB, pk->b1_ext, pk->fb1, nv + 2, outB1, P.ms_b1, P.bytes_b1, sb1)) == cudaSuccess &&
        (e = run_msm(true, wB, pk->b2_ext, pk->fb2, nv + 2, outB2, P.ms_b2, P.bytes_b2, sb2)) == cudaSuccess &&
        (e = run_msm(false, wA + (size_t)np1 * 8, pk->c + (size_t)np1 * 16, pk->fc, nv - np1, outC, P.ms_c, P.bytes_c,
-                    sc)) == cudaSuccess;
+                    sc, &share_c)) == cudaSuccess;
   if (!ok) return fail(ctx, e, "prove witness MSMs");
+  if (P.share_ch && (e = cudaEventRecord(ctx->aux_ev[7], sc)) != cudaSuccess) return fail(ctx, e, "prove C buckets");
   {
     const GlvSplit* gsp = reinterpret_cast<const GlvSplit*>(rs + 32);
     k_scale_point_glv<<<1, 32, 0, sa>>>(outA, gsp, sA);        // s * pi_A
@@ -510,7 +527,7 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
        (e = cudaEventRecord(ctx->aux_ev[6], sh)) == cudaSuccess &&  // H step done (stage times)
        // polH = M[m .. 2m-2]; M[2m-1] (always zero) becomes the -rs term for delta_1
        (e = cudaMemcpyAsync(M + (size_t)(2 * m - 1) * 8, rs + 16, 32, cudaMemcpyDeviceToDevice, sh)) == cudaSuccess &&
-       (e = run_msm(false, M + (size_t)m * 8, pk->h_ext, pk->fh, m, outH, P.ms_h, P.bytes_h, sh)) == cudaSuccess;
+       (e = run_msm(false, M + (size_t)m * 8, pk->h_ext, pk->fh, m, outH, P.ms_h, P.bytes_h, sh, &share_h)) == cudaSuccess;
   if (!ok) return fail(ctx, e, "prove QAP/H");
   for (int i = 0; i < 4; i++) {
     cudaEventRecord(ctx->aux_ev[1 + i], ctx->aux[i]);
