@@ -3,7 +3,10 @@
 // addition, 10 products) then fits the instruction cache; measured faster at 2^20.
 #define CSB_MUL_NOINLINE
 // Fq products stay 32-bit CIOS here: the FP64-pipe product needs more registers than
-// the 168 the Fq2 kernels run at (G2 fixed-base MSM 13.1 -> 13.9 ms with it).
+// the 168 the Fq2 kernels run at (G2 fixed-base MSM 13.1 -> 13.9 ms with it).  With the
+// accumulation uncapped and the batch-affine rounds kept at 168 registers the G2 MSM alone
+// gains a little (fixed-base 13.21 -> 13.02 ms), but a 2^20 proof loses (26.1 -> 26.3-26.6 ms):
+// its G1 MSMs already fill the FP64 pipe, and G2 on the integer pipes runs beside them.
 #ifndef CSB_DP52
 #define CSB_DP52 0
 #endif
