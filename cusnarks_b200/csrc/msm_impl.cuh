@@ -470,9 +470,12 @@ __global__ void __launch_bounds__(128) k_reduce_level_quad(const uint32_t* __res
   const bool valid = g < (uint32_t)W * nout;
   const uint32_t j = valid ? g / nout : 0u, t = valid ? g % nout : 0u;
   const uint32_t* yj = y + (size_t)j * n * XW;
-  XYZZ<F> acc = XYZZ<F>::inf(), s = XYZZ<F>::inf();
+  // running sum acc and sum of running sums s over the segment's buckets 7..1, starting at
+  // bucket 7 (no additions to infinity)
+  XYZZ<F> acc = valid && 8 * t + 7 < n ? ld_xyzz<F>(yj + (size_t)(8 * t + 7) * XW) : XYZZ<F>::inf();
+  XYZZ<F> s = acc;
 #pragma unroll 1
-  for (int i = 7; i >= 1; i--) {
+  for (int i = 6; i >= 1; i--) {
     const uint32_t idx = 8 * t + i;
     const XYZZ<F> v = valid && idx < n ? ld_xyzz<F>(yj + (size_t)idx * XW) : XYZZ<F>::inf();
     acc = add_q(acc, v);
@@ -517,6 +520,12 @@ CSB_DEV XYZZ<F> shfl_down_xyzz(const XYZZ<F>& v, int d) {
 //   sum_t t*y_t = sum_u [sum_i i*y_{uE+i}] + E * sum_{u>=1} Suf(u),  Suf(u) = sum_{v>=u} Y_v
 // so S_j = sum_u (V_u + G E * Suf(u) [u >= 1]): a block suffix scan and a block reduction,
 // about 2E + 25 dependent point operations instead of a serial pass over the segments.
+// Threads of the per-window sum (one block per window).  128 (4 warps, one per SM
+// sub-partition) shortens each dependent point operation enough to pay for the longer chains
+// of 32 virtual threads: 2^12 proof 2.00 -> 1.91 ms, G2 2^12 fixed-base MSM 1.68 -> 1.58 ms.
+#ifndef CSB_WSUM_THREADS
+#define CSB_WSUM_THREADS 128
+#endif
 template <class F, int THREADS>
 __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restrict__ y,
                                                         const uint32_t* __restrict__ z, uint32_t n1,
@@ -534,19 +543,29 @@ __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restri
   const uint32_t E = (n1 + VT - 1) / VT;  // n1 is a power of two
   const uint32_t u = threadIdx.x >> 2;
   const int vl = (threadIdx.x & 31) >> 2, warp = threadIdx.x >> 5, q = threadIdx.x & 3;
-  XYZZ<F> acc = XYZZ<F>::inf(), ws = XYZZ<F>::inf(), zs = XYZZ<F>::inf();
+  // the sums start at the thread's last segment (no additions to infinity)
+  XYZZ<F> acc, zs, ws = XYZZ<F>::inf();
+  {
+    const uint32_t idx = u * E + (E - 1);
+    const bool in = idx < n1;
+    acc = in ? ld_xyzz<F>(yj + (size_t)idx * XW) : XYZZ<F>::inf();
+    zs = in ? ld_xyzz<F>(zj + (size_t)idx * XW) : XYZZ<F>::inf();
+  }
 #pragma unroll 1
-  for (int i = (int)E - 1; i >= 0; i--) {  // uniform trip count; past n1 the terms are infinity
+  for (int i = (int)E - 2; i >= 0; i--) {  // uniform trip count; past n1 the terms are infinity
     const uint32_t idx = u * E + i;
     const bool in = idx < n1;
+    ws = add_q(ws, acc);  // acc = sum of the thread's segments above i
     acc = add_q(acc, in ? ld_xyzz<F>(yj + (size_t)idx * XW) : XYZZ<F>::inf());
     zs = add_q(zs, in ? ld_xyzz<F>(zj + (size_t)idx * XW) : XYZZ<F>::inf());
-    if (i > 0) ws = add_q(ws, acc);
   }
-  // V = acc + zs + 2^shift ws
+  // V = acc + zs + 2^shift ws (ws is infinity with one segment per thread)
+  XYZZ<F> V = add_q(acc, zs);
+  if (E > 1) {  // uniform
 #pragma unroll 1
-  for (int d = 0; d < shift; d++) ws = dbl_q(ws);
-  XYZZ<F> V = add_q(add_q(acc, zs), ws);
+    for (int d = 0; d < shift; d++) ws = dbl_q(ws);
+    V = add_q(V, ws);
+  }
   // inclusive suffix scan of acc over the 8 virtual lanes of the warp
   XYZZ<F> suf = acc;
 #pragma unroll 1
@@ -1064,7 +1083,7 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
     nseg = nnext;
     levels++;
   }
-  constexpr int WT = 256;
+  constexpr int WT = CSB_WSUM_THREADS;
   k_window_sum<F, WT><<<WR, WT, 0, st>>>(y, z, nseg, 3 * levels, wsum);
   note_launch();
   k_finish<F><<<1, 32, 0, st>>>(wsum, WR, c, d_out);
