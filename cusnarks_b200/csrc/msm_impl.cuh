@@ -513,6 +513,61 @@ CSB_DEV XYZZ<F> shfl_down_xyzz(const XYZZ<F>& v, int d) {
   return o;
 }
 
+// k_reduce_level_quad for the levels that carry weighted sums z (levels >= 1): two quads per
+// output segment, side by side in one warp.  The even quad runs the running sums of the segment
+// totals y and then the doublings; the odd quad sums the segment's eight z values meanwhile (each
+// step is the same point addition on operands picked by role, so the warp does not diverge), and
+// one shuffle and one addition join them: 13 + 3L + 1 dependent point operations instead of
+// 13 + 3L + 8.  Same sums as k_reduce_level_quad.
+template <class F>
+__global__ void __launch_bounds__(128) k_reduce_level_quad2(const uint32_t* __restrict__ y,
+                                                            const uint32_t* __restrict__ z, uint32_t n,
+                                                            uint32_t nout, int W, int level,
+                                                            uint32_t* __restrict__ yout,
+                                                            uint32_t* __restrict__ zout) {
+  constexpr int XW = 4 * FieldWords<F>::value;
+  const uint32_t gq = (blockIdx.x * blockDim.x + threadIdx.x) >> 2;
+  const uint32_t g = gq >> 1;
+  const bool zq = (gq & 1) != 0;  // the odd quad of the pair sums the z values
+  const bool valid = g < (uint32_t)W * nout;
+  const uint32_t j = valid ? g / nout : 0u, t = valid ? g % nout : 0u;
+  const uint32_t* yj = y + (size_t)j * n * XW;
+  const uint32_t* zj = z + (size_t)j * n * XW;
+  auto ld = [&](const uint32_t* base, uint32_t i) {
+    const uint32_t idx = 8 * t + i;
+    return valid && idx < n ? ld_xyzz<F>(base + (size_t)idx * XW) : XYZZ<F>::inf();
+  };
+  // even quad: a = running sum from bucket 7 down, s = sum of the running sums 7..1;
+  // odd quad: a = z_0 + ... + z_7
+  XYZZ<F> a = zq ? ld(zj, 0) : ld(yj, 7);
+  XYZZ<F> s = a;
+#pragma unroll 1
+  for (int step = 0; step < 13; step++) {
+    // even quad: even steps a += y_i (i = 6..0), odd steps s += a; odd quad: a += z_{step+1}
+    const bool even_step = (step & 1) == 0;
+    XYZZ<F> p, q;
+    if (zq) {
+      p = a;
+      q = step < 7 ? ld(zj, step + 1) : XYZZ<F>::inf();
+    } else if (even_step) {
+      p = a;
+      q = ld(yj, 6 - (step >> 1));
+    } else {
+      p = s;
+      q = a;
+    }
+    const XYZZ<F> r = add_q(p, q);  // every lane of the warp, every step
+    if (zq || even_step) a = r; else s = r;
+  }
+#pragma unroll 1
+  for (int d = 0; d < 3 * level; d++) s = dbl_q(s);
+  s = add_q(s, shfl_down_xyzz(a, 4));  // even quads: + the odd neighbour's z sum
+  if (valid && !zq && (threadIdx.x & 3) == 0) {
+    st_xyzz<F>(yout + ((size_t)j * nout + t) * XW, a);
+    st_xyzz<F>(zout + ((size_t)j * nout + t) * XW, s);
+  }
+}
+
 // Per-window sum after levels 0..L-1.  With y_t the segment totals and z_t the weighted
 // carries of the last level, S_j = sum_t (y_t + z_t) + G * sum_t t * y_t with G = 8^L =
 // 2^shift.  One block per window, E consecutive segments per thread u:
@@ -932,7 +987,9 @@ template <class F>
 void reduce_level(const uint32_t* y, const uint32_t* z, uint32_t n, uint32_t nout, int W, int level,
                   uint32_t* yout, uint32_t* zout, uint64_t resident, cudaStream_t st) {
   const uint64_t outs = (uint64_t)W * nout;
-  if (outs * 4 <= resident)
+  if (z && outs * 8 <= resident)
+    k_reduce_level_quad2<F><<<(uint32_t)((outs * 8 + 127) / 128), 128, 0, st>>>(y, z, n, nout, W, level, yout, zout);
+  else if (outs * 4 <= resident)
     k_reduce_level_quad<F><<<(uint32_t)((outs * 4 + 127) / 128), 128, 0, st>>>(y, z, n, nout, W, level, yout, zout);
   else
     k_reduce_level<F><<<(uint32_t)((outs + 127) / 128), 128, 0, st>>>(y, z, n, nout, W, level, yout, zout);
