@@ -31,11 +31,22 @@ terms in one batch plan per group (autotuned windows, CUDA graph replay) vs one 
 instance.  Also one BN128 G1 MSM of 2^20 terms (``g1_msm_2^20_ms``),
 whose bucket-accumulation kernel -- the dominant kernel of every proof -- carries the roofline.
 
-``cpu_baseline`` / ``--impl reference``: the reference's own CPU library (oracle/_ref,
-built from the reference sources; the C restatement when that library is absent) runs the
-reference's proving sequence on all host cores for a 2^16-constraint sample of the same
-circuit family; the time is scaled x16 to the 2^20 unit (every step of the sequence is
-linear or N log N in the size; the scale is stated in the line).
+``proof_check``: every proof of the timed served run and of the e2e run equals the
+one-proof-per-call proof byte for byte; on rank 0 at N = 1 that proof also equals the
+reference's CPU proving sequence run in the reference's own library on the same key,
+witness, r and s, and passes the Groth16 pairing check.
+
+``cpu_baseline``: that CPU proof, timed -- one whole 2^20-constraint proof of the
+benchmark circuit through the reference's own CPU implementation (oracle/_ref, built from
+the reference sources; the C restatement when that library is absent) on all host cores,
+stage by stage (QAP, H step, five multi-exponentiations).
+
+``--impl reference``: the same CPU prover alone, in a process that never loads this
+library: the 2^20 circuit and key are built on the CPU (oracle/synth_cpu.py, word for word
+the GPU builder's), untimed; each step is the next stage of the 2^20 proving sequence (7
+stages make one proof), so the K steps are bounded samples of the workload, and ``value`` is
+1 / (the sum of the stages' mean times).  ``proof_sha256`` in both lines names the proof
+each arm made from the same inputs.
 """
 from __future__ import annotations
 
@@ -63,7 +74,8 @@ MONT_PER_MADD = 11     # mixed addition, 7M + 4S (the canonical count of the MSM
 ACC_TRAFFIC_BYTES = 439_780_864 + 60_918_784
 L2_BYTES = 126 * 1024 * 1024
 LOG_M = 20
-CPU_SAMPLE_LOG_M = 16
+R_INT, S_INT = 0x1234567890abcdef, 0xfedcba0987654321
+CIRCUIT_SEED, KEY_SEED = 100, 101
 
 
 # ----------------------------------------------------------------- clocks sampler ---
@@ -163,23 +175,26 @@ def pct(xs, q):
 
 
 # ---------------------------------------------------------------- CPU reference ------
-def cpu_reference_prove_sample(ctx, log_m: int, seed: int, repeats: int = 1):
-    """Seconds per proof of the reference's CPU proving sequence (oracle/_ref on all host
-    threads) on a 2^log_m-constraint circuit of the benchmark family.  The circuit and key
-    are generated with this library; only the CPU proving is timed."""
-    from cusnarks_b200.groth import SyntheticCircuit, setup_pk, pk_to_host
+def cpu_reference_prove(pk_host: dict, w: np.ndarray):
+    """One proof of the benchmark circuit by the reference's CPU proving sequence in the
+    reference's own library (oracle/_ref; the restatement where it is absent), all host
+    threads, timed stage by stage.  Returns (proof, seconds per stage, kind, threads)."""
     from oracle.oracle import Oracle, RefLib
-    from oracle.prover import cpu_prove
-    circ = SyntheticCircuit(ctx, log_m, seed=seed)
-    pk = pk_to_host(setup_pk(ctx, circ, seed=seed + 1))
+    from oracle.prover import cpu_prove_stages
     o = Oracle()
     ref = RefLib.get() if RefLib.available() else None
-    cpu_prove(o, pk, circ.w, 1234567, 7654321, ref=ref)  # warm the caches / thread pools
-    t0 = time.perf_counter()
-    for _ in range(repeats):
-        cpu_prove(o, pk, circ.w, 1234567, 7654321, ref=ref)
-    sec = (time.perf_counter() - t0) / repeats
-    return sec, ("reference" if ref else "port"), (os.cpu_count() or 1)
+    stages, st = cpu_prove_stages(o, pk_host, w, R_INT, S_INT, ref=ref)
+    times = {}
+    for name, fn in stages:
+        t0 = time.perf_counter()
+        fn()
+        times[name] = time.perf_counter() - t0
+    return st["proof"], times, ("reference" if ref else "port"), (os.cpu_count() or 1)
+
+
+def proof_sha256(proof: np.ndarray) -> str:
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(proof, dtype=np.uint32).tobytes()).hexdigest()
 
 
 # ----------------------------------------------------------------------- workloads ---
@@ -193,7 +208,7 @@ class ProveWorkload:
         self.circ = SyntheticCircuit(ctx, log_m, seed=seed)
         self.pk = setup_pk(ctx, self.circ, seed=seed + 1)
         self.prover = Prover(ctx, self.pk)
-        self.r, self.s = to_limbs(0x1234567890abcdef), to_limbs(0xfedcba0987654321)
+        self.r, self.s = to_limbs(R_INT), to_limbs(S_INT)
         dev = torch.device("cuda", ctx.device)
         self.d_w = self.circ.d_w
         self.d_proof = torch.zeros(64, dtype=torch.int32, device=dev)
@@ -289,22 +304,22 @@ class ServedDevice:
     """Proofs from a device-resident witness overlapped across `slots` contexts (each with
     its own streams and scratch): the served engine without the host copies."""
 
-    def __init__(self, wl, slots: int):
+    def __init__(self, wl, slots: int, max_requests: int):
         import torch
         from cusnarks_b200 import Context
         self.wl = wl
         self.ctxs = [wl.ctx] + [Context(wl.ctx.device) for _ in range(slots - 1)]
         dev = torch.device("cuda", wl.ctx.device)
-        self.proofs = [torch.zeros(64, dtype=torch.int32, device=dev) for _ in self.ctxs]
+        # one output per request, so every proof of a run can be checked afterwards
+        self.proofs = torch.zeros((max(max_requests, slots), 64), dtype=torch.int32, device=dev)
 
     def run(self, k: int):
         from cusnarks_b200._lib import lib, check
         wl = self.wl
         for i in range(k):
-            j = i % len(self.ctxs)
-            c = self.ctxs[j]
+            c = self.ctxs[i % len(self.ctxs)]
             check(lib().cs_prove_device(c.handle, wl.prover.handle, _vp(wl.d_w.data_ptr()), wl.r.ctypes.data,
-                                        wl.s.ctypes.data, _vp(self.proofs[j].data_ptr())), c.handle)
+                                        wl.s.ctypes.data, _vp(self.proofs[i].data_ptr())), c.handle)
         for c in self.ctxs:
             c.sync()
 
@@ -332,9 +347,10 @@ def device_span_ms(fn):
     return a.elapsed_time(b)
 
 
-def served_run(srv, jobs, rate_hz=None, seed=0):
+def served_run(srv, jobs, rate_hz=None, seed=0, proofs=None):
     """Submits jobs [(key, w, r, s)] all at once (rate_hz None) or as a Poisson stream;
-    returns (wall seconds first submit -> last proof, latencies ms)."""
+    returns (wall seconds first submit -> last proof, latencies ms); appends the proofs to
+    `proofs` when given."""
     rng = np.random.Generator(np.random.PCG64(seed))
     t0 = time.perf_counter()
     tickets = []
@@ -348,8 +364,10 @@ def served_run(srv, jobs, rate_hz=None, seed=0):
         tickets.append(srv.submit(key, w, r, s))
     lat = []
     for t in tickets:
-        _, info = srv.wait(t)
+        pr, info = srv.wait(t)
         lat.append(info["latency_ms"])
+        if proofs is not None:
+            proofs.append(pr)
     return time.perf_counter() - t0, lat
 
 
@@ -460,8 +478,8 @@ def run_ours(args, world, rank, local):
     from cusnarks_b200.context import kernel_launches
     ctx = Context(local)
     peak_wide = ctx.pipe_rate(3)
-    wl = ProveWorkload(ctx, LOG_M, seed=100 + rank)
-    sd = ServedDevice(wl, args.slots)
+    wl = ProveWorkload(ctx, args.log_m, seed=CIRCUIT_SEED + rank)
+    sd = ServedDevice(wl, args.slots, args.steps)
     # one proof per call (resident key): lone-proof device latency
     for _ in range(args.warmup):
         wl.step()
@@ -469,6 +487,7 @@ def run_ours(args, world, rank, local):
     for _ in range(args.steps):
         wl.l2_flush()
         single.append(wl.step())
+    ref_proof = wl.d_proof.cpu().numpy().view(np.uint32).copy()
     # served engine, device witness: `steps` proofs overlapped across the slots
     for _ in range(args.warmup):
         sd.run(args.slots)
@@ -485,6 +504,8 @@ def run_ours(args, world, rank, local):
     total_ms = max_over_ranks(span, world)
     ms_per_step = total_ms / args.steps
     value = world * 1e3 / ms_per_step
+    served_proofs = sd.proofs[:args.steps].cpu().numpy().view(np.uint32)
+    served_equal = bool((served_proofs == ref_proof[None, :]).all())
     sd.close()
     # end to end: the C-ABI server, host witness in, proof out to host
     from cusnarks_b200.server import ProveServer
@@ -493,7 +514,9 @@ def run_ours(args, world, rank, local):
     # at least 30 requests: with fewer, the pipeline's fill and drain dominate the wall clock
     jobs = [(key, wl.circ.w, wl.r, wl.s)] * max(30, args.steps)
     served_run(srv, jobs[:args.slots])
-    wall, lat_sat = served_run(srv, jobs)
+    e2e_proofs = []
+    wall, lat_sat = served_run(srv, jobs, proofs=e2e_proofs)
+    e2e_equal = all(np.array_equal(pr, ref_proof) for pr in e2e_proofs)
     e2e_ms = max_over_ranks(wall * 1e3 / len(jobs), world)
     # latency under a Poisson stream at 70% of the saturated rate
     wall_p, lat = served_run(srv, jobs[:1] * 120, rate_hz=0.7 * 1e3 / e2e_ms, seed=11)
@@ -540,7 +563,7 @@ def run_ours(args, world, rank, local):
                 "GPU-generated key",
         "config": {"workload": "Groth16 prove, synthetic R1CS 2^20 constraints (domain 2^20), proving key "
                                "and fixed-base tables resident in HBM, fixed r,s",
-                   "n_vars": wl.circ.n_vars, "domain": 1 << LOG_M,
+                   "n_vars": wl.circ.n_vars, "domain": 1 << args.log_m,
                    "path": f"served engine: proofs overlapped over {args.slots} slots, device witness",
                    "l2": "inputs larger than L2 (proving key + tables ~6 GB)"},
         "latency_ms": {"p50": round(pct(lat, 50), 3), "p99": round(pct(lat, 99), 3),
@@ -549,10 +572,12 @@ def run_ours(args, world, rank, local):
         "single_proof": {"proofs_per_s": round(1e3 / statistics.median(single), 3),
                          "p50_ms": round(pct(single, 50), 3), "p99_ms": round(pct(single, 99), 3),
                          "basis": "one proof per call (cs_prove_device), device time"},
+        "served_vs_single": round(value / world * statistics.median(single) / 1e3, 3),
         "plain_per_call": {"proofs_per_s": round(1e3 / plain_ms, 3), "ms": round(plain_ms, 1),
                            "basis": "the reference's flow through the drop-in entry points: mpoly_eval, "
-                                    "ntt_interpolandmul, 6 ec_jacreduce calls with host scalars and key "
-                                    "points copied per call; wall clock"},
+                                    "ntt_interpolandmul, 6 ec_jacreduce calls; the key's point arrays are "
+                                    "built once per key on the host and copied to the GPU by every call, "
+                                    "with the call's scalars; wall clock"},
         "served_vs_plain": round(e2e_val * plain_ms / 1e3, 2),
         "g1_msm_2^20_ms": round(statistics.median(msm_ms), 3),
         "roofline": {"bound": "int issue (ALU column sums + FP64 split products)", "kernel": "k_accumulate+k_combine (MSM bucket accumulation)",
@@ -571,6 +596,11 @@ def run_ours(args, world, rank, local):
                          "host witness in, proof out; wall clock"},
         "gpu_launches": launches,
         "clocks": clocks,
+        "proof_check": {"served_bytes_equal": served_equal, "served_proofs": int(served_proofs.shape[0]),
+                        "e2e_bytes_equal": bool(e2e_equal), "e2e_proofs": len(e2e_proofs),
+                        "proof_sha256": proof_sha256(ref_proof),
+                        "basis": "every proof of the timed served run and of the e2e run equals the "
+                                 "one-proof-per-call proof (cs_prove_device) byte for byte"},
     }
     if world > 1:  # every rank takes part (collective)
         line["sharded_g1_msm_2^20"] = sharded_msm_leg(ctx, world, rank, reps=max(3, args.steps))
@@ -579,12 +609,21 @@ def run_ours(args, world, rank, local):
     if rank == 0 and not args.no_mix:
         line["served_mix"] = served_mix(ctx, args.slots, args.mix_requests)
     if rank == 0 and world == 1 and not args.no_cpu:
-        sec, kind, threads = cpu_reference_prove_sample(ctx, CPU_SAMPLE_LOG_M, seed=55)
-        scaled = sec * (1 << (LOG_M - CPU_SAMPLE_LOG_M))
-        line["cpu_baseline"] = {"value": round(1.0 / scaled, 6), "unit": UNIT, "cores": threads, "kind": kind,
-                                "sample": f"one Groth16 proof of a 2^{CPU_SAMPLE_LOG_M}-constraint circuit of the "
-                                          f"same family ({sec:.2f} s), x{1 << (LOG_M - CPU_SAMPLE_LOG_M)} to 2^20",
-                                "s_per_proof_scaled": round(scaled, 2)}
+        from cusnarks_b200.groth import pk_to_host
+        from oracle.prover import verify
+        host = pk_to_host(wl.pk)
+        cpu_proof, stage_s, kind, threads = cpu_reference_prove(host, wl.circ.w)
+        sec = sum(stage_s.values())
+        line["cpu_baseline"] = {"value": round(1.0 / sec, 6), "unit": UNIT, "cores": threads, "kind": kind,
+                                "sample": "one whole proof of the 2^20-constraint benchmark circuit (same key, "
+                                          "witness, r, s as the GPU proofs): the reference's CPU proving "
+                                          "sequence in its own library, all host threads",
+                                "s_per_proof": round(sec, 2),
+                                "stages_s": {k: round(v, 3) for k, v in stage_s.items()}}
+        line["proof_check"]["cpu_reference_bytes_equal"] = bool(np.array_equal(cpu_proof, ref_proof))
+        line["proof_check"]["pairing"] = bool(verify(host["vk"], ref_proof, wl.circ.public_inputs))
+        line["proof_check"]["basis"] += ("; on rank 0 it also equals the reference library's CPU proof and "
+                                         "passes the Groth16 pairing check")
     if rank == 0:
         print(json.dumps(line), flush=True)
     wl.prover.close()
@@ -592,28 +631,68 @@ def run_ours(args, world, rank, local):
 
 
 def run_reference(args, world, rank):
+    """The reference's own CPU prover on the 2^20 workload, in a process that never loads this
+    library: the circuit and key are built on the CPU (untimed); step i runs stage i mod 7 of
+    the proving sequence (QAP, H step, five multi-exponentiations), all host threads."""
     if rank != 0:
         return
-    from cusnarks_b200 import Context
-    ctx = Context(0)
-    times, kind, threads = [], "reference", os.cpu_count() or 1
+    from oracle.oracle import Oracle, RefLib
+    from oracle.prover import cpu_prove_stages, verify
+    from oracle.synth_cpu import CpuCircuit, cpu_setup_pk
+    o = Oracle()
+    t0 = time.perf_counter()
+    circ = CpuCircuit(o, args.log_m, seed=CIRCUIT_SEED)
+    pk = cpu_setup_pk(o, circ, seed=KEY_SEED)
+    prep_s = time.perf_counter() - t0
+    ref = RefLib.get() if RefLib.available() else None
+    kind, threads = ("reference" if ref else "port"), (os.cpu_count() or 1)
+    stages, st = cpu_prove_stages(o, pk, circ.w, R_INT, S_INT, ref=ref)
+    per = {name: [] for name, _ in stages}
+    warm = {name: [] for name, _ in stages}
+    timed = 0.0
+    proof = None
     for i in range(args.warmup + args.steps):
-        sec, kind, threads = cpu_reference_prove_sample(ctx, CPU_SAMPLE_LOG_M, seed=500 + i)
+        name, fn = stages[i % len(stages)]
+        t = time.perf_counter()
+        fn()
+        dt = time.perf_counter() - t
+        (per if i >= args.warmup else warm)[name].append(dt)
         if i >= args.warmup:
-            times.append(sec * (1 << (LOG_M - CPU_SAMPLE_LOG_M)))
-    per = statistics.mean(times)
-    val = 1.0 / per
+            timed += dt
+        if proof is None and "proof" in st:
+            proof = st["proof"].copy()
+    for name, _, in stages:  # a stage the timed steps did not reach: its warm-up time
+        if not per[name]:
+            if not warm[name]:
+                fn = dict(stages)[name]
+                t = time.perf_counter()
+                fn()
+                warm[name].append(time.perf_counter() - t)
+            per[name] = warm[name]
+    stage_s = {k: statistics.mean(v) for k, v in per.items()}
+    s_proof = sum(stage_s.values())
+    val = 1.0 / s_proof
+    if proof is None:
+        proof = st.get("proof")
     line = {"metric": METRIC, "impl": "reference", "value": round(val, 6), "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(per * 1e3, 1), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32x8 (256-bit Montgomery integers)", "data": "synthetic",
-            "config": {"workload": "Groth16 prove, synthetic R1CS 2^20 constraints (timed on 2^16-constraint "
-                                   "samples of the same family, x16)"},
+            "ms_per_step": round(timed * 1e3 / args.steps, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32x8 (256-bit Montgomery integers)",
+            "data": "synthetic: the benchmark circuit and key, built on the CPU from the same seeds",
+            "config": {"workload": f"Groth16 prove, synthetic R1CS 2^{args.log_m} constraints "
+                                   f"(domain 2^{args.log_m}), fixed r,s",
+                       "n_vars": circ.n_vars, "domain": 1 << args.log_m,
+                       "step": "one stage of the proving sequence; 7 stages make one proof"},
+            "steps_per_proof": len(stages), "s_per_proof": round(s_proof, 2),
+            "stages_s": {k: round(v, 3) for k, v in stage_s.items()},
+            "prep_s": round(prep_s, 1),
             "cpu_baseline": {"value": round(val, 6), "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": f"one 2^{CPU_SAMPLE_LOG_M}-constraint proof per step, x16 to 2^20"},
+                             "sample": "stages of 2^20-constraint proofs, one per step, all host threads"},
             "e2e": {"value": round(val, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if proof is not None:
+        line["proof_sha256"] = proof_sha256(proof)
+        line["pairing"] = bool(verify(pk["vk"], proof, circ.public_inputs))
     print(json.dumps(line), flush=True)
-    ctx.close()
 
 
 def main():
@@ -627,6 +706,8 @@ def main():
     ap.add_argument("--no-mix", action="store_true", help="skip the mixed-size served leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-MSM leg")
     ap.add_argument("--mix-requests", type=int, default=96)
+    ap.add_argument("--log-m", type=int, default=LOG_M,
+                    help="constraint domain of the proving workload (the metric is quoted on 2^20)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

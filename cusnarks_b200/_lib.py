@@ -116,10 +116,7 @@ _SIGNATURES = [
     ("cs_msm_tuned_window", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_uint32]),
     ("cs_scmul_device", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, ctypes.c_uint32, _vp]),
     ("cs_point_sum_device", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_uint32, ctypes.c_int, _vp]),
-    ("cs_bench_imad_peak", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     ("cs_bench_pipe", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
-    ("cs_bench_mulmod", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
-    ("cs_bench_mul_latency", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     ("cs_kernel_launches", ctypes.c_ulonglong, []),
     ("cs_field_op_device", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_uint32]),
     ("cs_field_last_status", ctypes.c_int, []),

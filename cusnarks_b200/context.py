@@ -125,7 +125,7 @@ class Context:
 
     # -------------------------------------------------------------- field ops -----
     FOP = {"mul": 0, "add": 1, "sub": 2, "sqr": 3, "inv": 4, "to_mont": 5, "from_mont": 6,
-           "mul_lohi": 7, "fq2_mul": 8, "mul_dp52": 9}
+           "fq2_mul": 8, "mul_dp52": 9}
 
     def field_op_device(self, op: str, pidx: int, d_a: int, d_b: int, d_out: int, n: int):
         check(self._lib.cs_field_op_device(self.handle, self.FOP[op], pidx, ctypes.c_void_p(d_a),
@@ -157,11 +157,6 @@ class Context:
         """d_out = the affine sum of n points (rows of dims = 2 affine / 3 Jacobian coordinates)."""
         check(self._lib.cs_point_sum_device(self.handle, int(bool(ec2)), ctypes.c_void_p(d_points), n, dims,
                                             ctypes.c_void_p(d_out)), self.handle)
-
-    def imad_peak(self) -> float:
-        v = ctypes.c_double()
-        check(self._lib.cs_bench_imad_peak(self.handle, ctypes.byref(v)), self.handle)
-        return float(v.value)
 
     def pipe_rate(self, mode: int) -> float:
         """Measured instruction rate per second of one pipe probe (cs_bench_pipe): 1 mad.lo,

@@ -33,38 +33,11 @@ CSB_DEV bool affine_is_inf(const Affine<F>& a) {
   return a.x.is_zero() && a.y == F::one();
 }
 
-// Paired-product helpers of the formulas below: PAIR = true computes each independent pair
-// of products in one out-of-line call with interleaved rows (F::mul2_ool), which shortens a
-// single thread's dependent chain; false uses F::mul2 (two products unless CSB_PAIR).
-template <class F, bool PAIR>
-struct PairOps {
-  static CSB_DEV void mul2(const F& a, const F& b, const F& c, const F& d, F& x, F& y) {
-    if constexpr (PAIR) F::mul2_ool(a, b, c, d, x, y); else F::mul2(a, b, c, d, x, y);
-  }
-  static CSB_DEV void sqr2(const F& a, const F& c, F& x, F& y) {
-    if constexpr (PAIR) F::sqr2_ool(a, c, x, y); else F::sqr2(a, c, x, y);
-  }
-};
-
 // dbl-2008-s-1 (a = 0)
-template <class F, bool PAIR = (CSB_PAIRED != 0)>
+template <class F>
 CSB_DEV XYZZ<F> xyzz_dbl(const XYZZ<F>& p) {
   if (p.is_inf()) return p;
-  if constexpr (PAIR) {
-    using O = PairOps<F, true>;
-    const F U = p.Y.dbl();
-    F V, X2, W, S, MM, T1, T2;
-    O::sqr2(U, p.X, V, X2);
-    O::mul2(U, V, p.X, V, W, S);
-    const F M = X2.dbl() + X2;
-    XYZZ<F> r;
-    O::mul2(M, M, W, p.ZZZ, MM, r.ZZZ);
-    r.X = MM - S.dbl();
-    O::mul2(M, S - r.X, W, p.Y, T1, T2);
-    r.Y = T1 - T2;
-    r.ZZ = V * p.ZZ;
-    return r;
-  } else {
+  {
     const F U = p.Y.dbl();
     const F V = U.sqr();
     const F W = U * V;
@@ -98,30 +71,10 @@ CSB_DEV XYZZ<F> xyzz_mdbl(const Affine<F>& p) {
 }
 
 // madd-2008-s: p (XYZZ) + q (affine, not infinity)
-template <class F, bool PAIR = (CSB_PAIRED != 0)>
+template <class F>
 CSB_DEV XYZZ<F> xyzz_madd(const XYZZ<F>& p, const Affine<F>& q) {
   if (p.is_inf()) return XYZZ<F>::from_affine(q);
-  if constexpr (PAIR) {
-    // the ten products in five independent pairs
-    using O = PairOps<F, true>;
-    F U2, S2;
-    O::mul2(q.x, p.ZZ, q.y, p.ZZZ, U2, S2);
-    const F P = U2 - p.X;
-    const F R = S2 - p.Y;
-    if (P.is_zero()) {
-      if (R.is_zero()) return xyzz_mdbl(q);
-      return XYZZ<F>::inf();
-    }
-    F PP, RR, PPP, Q, T1, T2;
-    O::sqr2(P, R, PP, RR);
-    O::mul2(P, PP, p.X, PP, PPP, Q);
-    XYZZ<F> r;
-    r.X = RR - PPP - Q.dbl();
-    O::mul2(R, Q - r.X, p.Y, PPP, T1, T2);
-    r.Y = T1 - T2;
-    O::mul2(p.ZZ, PP, p.ZZZ, PPP, r.ZZ, r.ZZZ);
-    return r;
-  } else {
+  {
     const F U2 = q.x * p.ZZ;
     const F S2 = q.y * p.ZZZ;
     const F P = U2 - p.X;
@@ -168,32 +121,11 @@ CSB_DEV XYZZ<Fq> xyzz_madd_lazy(const XYZZ<Fq>& p, const Affine<Fq>& q) {
 CSB_DEV XYZZ<Fq> xyzz_canon(const XYZZ<Fq>& p) { return {p.X.canon(), p.Y.canon(), p.ZZ.canon(), p.ZZZ.canon()}; }
 
 // add-2008-s: p + q, both XYZZ
-template <class F, bool PAIR = (CSB_PAIRED != 0)>
+template <class F>
 CSB_DEV XYZZ<F> xyzz_add(const XYZZ<F>& p, const XYZZ<F>& q) {
   if (p.is_inf()) return q;
   if (q.is_inf()) return p;
-  if constexpr (PAIR) {
-    using O = PairOps<F, true>;
-    F U1, U2, S1, S2;
-    O::mul2(p.X, q.ZZ, q.X, p.ZZ, U1, U2);
-    O::mul2(p.Y, q.ZZZ, q.Y, p.ZZZ, S1, S2);
-    const F P = U2 - U1;
-    const F R = S2 - S1;
-    if (P.is_zero()) {
-      if (R.is_zero()) return xyzz_dbl<F, true>(p);
-      return XYZZ<F>::inf();
-    }
-    F PP, RR, PPP, Q, T1, T2, Z2, Z3;
-    O::sqr2(P, R, PP, RR);
-    O::mul2(P, PP, U1, PP, PPP, Q);
-    XYZZ<F> r;
-    r.X = RR - PPP - Q.dbl();
-    O::mul2(R, Q - r.X, S1, PPP, T1, T2);
-    r.Y = T1 - T2;
-    O::mul2(p.ZZ, q.ZZ, p.ZZZ, q.ZZZ, Z2, Z3);
-    O::mul2(Z2, PP, Z3, PPP, r.ZZ, r.ZZZ);
-    return r;
-  } else {
+  {
     const F U1 = p.X * q.ZZ;
     const F U2 = q.X * p.ZZ;
     const F S1 = p.Y * q.ZZZ;
@@ -201,7 +133,7 @@ CSB_DEV XYZZ<F> xyzz_add(const XYZZ<F>& p, const XYZZ<F>& q) {
     const F P = U2 - U1;
     const F R = S2 - S1;
     if (P.is_zero()) {
-      if (R.is_zero()) return xyzz_dbl<F, false>(p);
+      if (R.is_zero()) return xyzz_dbl(p);
       return XYZZ<F>::inf();
     }
     const F PP = P.sqr();
@@ -298,7 +230,7 @@ CSB_DEV XYZZ<F> xyzz_add_quad(const XYZZ<F>& p, const XYZZ<F>& q) {
   r.ZZ = ZZ3;
   r.ZZZ = ZZZ3;
   if (P.is_zero() && !p.is_inf() && !q.is_inf())  // equal or opposite points (rare): no shuffles
-    r = R.is_zero() ? xyzz_dbl<F, false>(p) : XYZZ<F>::inf();
+    r = R.is_zero() ? xyzz_dbl(p) : XYZZ<F>::inf();
   return p.is_inf() ? q : (q.is_inf() ? p : r);
 }
 

@@ -15,9 +15,6 @@
 namespace csb {
 
 #define CSB_DEV __device__ __forceinline__
-#ifndef CSB_FQ2_MODE
-#define CSB_FQ2_MODE 0  // Fq2 product: 0 CIOS x3, 1 carry-flag-free CIOS x3, 2 lazy reduction
-#endif
 
 // ---------------------------------------------------------------- moduli ------------
 struct ModQ {  // base field q (the reference's MOD_GROUP, pidx 0)
@@ -30,14 +27,6 @@ struct ModQ {  // base field q (the reference's MOD_GROUP, pidx 0)
                             R24 = 0x0a417ff6u, R25 = 0x47ab1effu, R26 = 0xcab8351fu, R27 = 0x06d89f71u;
   static constexpr uint32_t R30 = 0xda1530dfu, R31 = 0xb1cd6dafu, R32 = 0xa7283db6u, R33 = 0x62f210e6u,
                             R34 = 0x0ada0afbu, R35 = 0xef7f0b0cu, R36 = 0x2d592544u, R37 = 0x20fd6e90u;
-  // q^2, 16 limbs (lazy-reduction offset)
-  static CSB_DEV uint32_t P2_LIMB(int i) {
-    constexpr uint32_t k[16] = {0x275d69b1u, 0x3b5458a2u, 0x09eac101u, 0xa602072du,
-                                0x6d96cadcu, 0x4a50189cu, 0x7a1242c8u, 0x04689e95u,
-                                0x34c6b38du, 0x26edfa5cu, 0x16375606u, 0xb00b8551u,
-                                0x0348d21cu, 0x599a6f7cu, 0x763cbf9cu, 0x0925c4b8u};
-    return k[i];
-  }
   // q in radix 2^52 and -q^-1 mod 2^52 (FP64-pipe product)
   static CSB_DEV double L52(int i) {
     return i == 0 ? 154029749239111.0 : i == 1 ? 2558044347618242.0 : i == 2 ? 423691504025962.0
@@ -164,42 +153,15 @@ CSB_DEV void mont(const uint32_t (&x)[8], const uint32_t (&y)[8], uint32_t (&out
 }
 }  // namespace dp52
 
-// Paired products (CSB_PAIR, opt-in; only with out-of-line products): Fp::mul2 computes two
-// independent products in one call with their rows interleaved.  Measured at 2^20: the G1
-// MSM alone 3 % faster (accumulation capped at 128 registers), a whole proof 2.7 % slower
-// (its five MSMs share the SMs and the paired body doubles the multiply's code), so off.
-#if defined(CSB_PAIR) && defined(CSB_MUL_NOINLINE) && !defined(CSB_MUL_LOHI)
-#define CSB_PAIRED 1
-#else
-#define CSB_PAIRED 0
-#endif
-
 // ------------------------------------------------------------ carry-chain helpers ----
 // Each helper is one PTX instruction; `volatile` keeps the carry flag sequence in
 // program order.
-#define MAD_LO_CC(d, a, b)  asm volatile("mad.lo.cc.u32 %0, %1, %2, %0;" : "+r"(d) : "r"(a), "r"(b))
-#define MADC_LO_CC(d, a, b) asm volatile("madc.lo.cc.u32 %0, %1, %2, %0;" : "+r"(d) : "r"(a), "r"(b))
-#define MAD_HI_CC(d, a, b)  asm volatile("mad.hi.cc.u32 %0, %1, %2, %0;" : "+r"(d) : "r"(a), "r"(b))
-#define MADC_HI_CC(d, a, b) asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(d) : "r"(a), "r"(b))
-#define MADC_HI(d, a, b)    asm volatile("madc.hi.u32 %0, %1, %2, %0;" : "+r"(d) : "r"(a), "r"(b))
-#define ADDC_Z(d)           asm volatile("addc.u32 %0, 0, 0;" : "=r"(d))
 #define ADD_CC(d, a, b)     asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
 #define ADDC_CC(d, a, b)    asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
 #define ADDC(d, a, b)       asm volatile("addc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
 #define SUB_CC(d, a, b)     asm volatile("sub.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
 #define SUBC_CC(d, a, b)    asm volatile("subc.cc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
 #define SUBC(d, a, b)       asm volatile("subc.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b))
-
-// t[0..8] += a[0..7] * b.  Requires the true sum to fit in 9 limbs.
-CSB_DEV void row_mad(uint32_t (&t)[9], const uint32_t (&a)[8], uint32_t b) {
-  MAD_LO_CC(t[0], a[0], b);  MADC_LO_CC(t[1], a[1], b); MADC_LO_CC(t[2], a[2], b);
-  MADC_LO_CC(t[3], a[3], b); MADC_LO_CC(t[4], a[4], b); MADC_LO_CC(t[5], a[5], b);
-  MADC_LO_CC(t[6], a[6], b); MADC_LO_CC(t[7], a[7], b);
-  uint32_t c; ADDC_Z(c); t[8] += c;
-  MAD_HI_CC(t[1], a[0], b);  MADC_HI_CC(t[2], a[1], b); MADC_HI_CC(t[3], a[2], b);
-  MADC_HI_CC(t[4], a[3], b); MADC_HI_CC(t[5], a[4], b); MADC_HI_CC(t[6], a[5], b);
-  MADC_HI_CC(t[7], a[6], b); MADC_HI(t[8], a[7], b);
-}
 
 // t[0..8] += a[0..7] * b using 32x32->64 wide products (IMAD.WIDE): the even-index
 // products a0b, a2b, a4b, a6b tile limbs 0..7 without overlap and the odd ones tile
@@ -235,15 +197,10 @@ CSB_DEV void row_mad_wide(uint32_t (&t)[9], const uint32_t (&a)[8], uint32_t b) 
 
 template <class M>
 struct Fp;
-template <class M>
-struct FpPair;
 // Out-of-line Montgomery product (arguments and result in registers): keeps loop bodies
 // that chain many products small enough for the instruction cache.
 template <class M>
 __device__ __noinline__ Fp<M> fp_mul_call(Fp<M> a, Fp<M> b);
-// Out-of-line pair of independent products (a*b, c*d) with interleaved rows.
-template <class M>
-__device__ __noinline__ FpPair<M> fp_mul2_call(Fp<M> a, Fp<M> b, Fp<M> c, Fp<M> d);
 
 template <class M>
 struct Fp {
@@ -330,36 +287,6 @@ struct Fp {
     return r;
   }
 
-  // Two independent CIOS products x = a*b, y = c*d with their rows interleaved: the carry
-  // chains of one product fill the fixed-latency dependency stalls of the other, which a
-  // single product (one long serial chain) cannot.
-  static CSB_DEV void mul_wide2(const Fp& a, const Fp& b, const Fp& c, const Fp& d, Fp& x, Fp& y) {
-    const uint32_t P[8] = {M::P0, M::P1, M::P2, M::P3, M::P4, M::P5, M::P6, M::P7};
-    uint32_t t[9], u[9];
-#pragma unroll
-    for (int i = 0; i < 9; i++) { t[i] = 0; u[i] = 0; }
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-      row_mad_wide(t, a.v, b.v[i]);
-      row_mad_wide(u, c.v, d.v[i]);
-      const uint32_t mt = t[0] * M::NP0;
-      const uint32_t mu = u[0] * M::NP0;
-      row_mad_wide(t, P, mt);
-      row_mad_wide(u, P, mu);
-#pragma unroll
-      for (int j = 0; j < 8; j++) { t[j] = t[j + 1]; u[j] = u[j + 1]; }
-      t[8] = 0;
-      u[8] = 0;
-    }
-    uint32_t r8[8], s8[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) { r8[i] = t[i]; s8[i] = u[i]; }
-    reduce_once(r8);
-    reduce_once(s8);
-#pragma unroll
-    for (int i = 0; i < 8; i++) { x.v[i] = r8[i]; y.v[i] = s8[i]; }
-  }
-
   // ---- lazily reduced values in [0, 2p) (BN254: 4p < 2^256) --------------------------
   // CIOS without the final conditional subtraction: for a, b < 2p the result is below
   // (a b + m p) / 2^256 < (4p^2 + 2^256 p) / 2^256 < 2p.
@@ -433,153 +360,14 @@ struct Fp {
     return r;
   }
 
-  // x = a*b, y = c*d in one out-of-line call with interleaved rows (any unit): about the
-  // latency of one product for two, where a single thread's chain is the cost.
-  static CSB_DEV void mul2_ool(const Fp& a, const Fp& b, const Fp& c, const Fp& d, Fp& x, Fp& y) {
-    const FpPair<M> r = fp_mul2_call<M>(a, b, c, d);
-    x = r.x;
-    y = r.y;
-  }
-  static CSB_DEV void sqr2_ool(const Fp& a, const Fp& c, Fp& x, Fp& y) { mul2_ool(a, a, c, c, x, y); }
-
-  // x = a*b, y = c*d.  With CSB_PAIR one out-of-line call computes both with interleaved
-  // rows; otherwise two products (inlined ones are scheduled together anyway).
-  static CSB_DEV void mul2(const Fp& a, const Fp& b, const Fp& c, const Fp& d, Fp& x, Fp& y) {
-#if CSB_PAIRED
-    mul2_ool(a, b, c, d, x, y);
-#else
-    const Fp xx = a * b;
-    y = c * d;
-    x = xx;
-#endif
-  }
-  // x = a^2, y = c^2
-  static CSB_DEV void sqr2(const Fp& a, const Fp& c, Fp& x, Fp& y) { mul2(a, a, c, c, x, y); }
-
-  // CIOS Montgomery product in plain 64-bit C++ arithmetic (no carry flag): independent
-  // products can be interleaved by the compiler.
-  static CSB_DEV Fp mul_c64(const Fp& a, const Fp& b) {
-    const uint32_t P[8] = {M::P0, M::P1, M::P2, M::P3, M::P4, M::P5, M::P6, M::P7};
-    uint32_t t[10];
-#pragma unroll
-    for (int i = 0; i < 10; i++) t[i] = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-      uint64_t c = 0;
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        const uint64_t s = (uint64_t)a.v[j] * b.v[i] + t[j] + c;
-        t[j] = (uint32_t)s;
-        c = s >> 32;
-      }
-      const uint64_t s8 = (uint64_t)t[8] + c;
-      t[8] = (uint32_t)s8;
-      t[9] = (uint32_t)(s8 >> 32);
-      const uint32_t m = t[0] * M::NP0;
-      uint64_t c2 = ((uint64_t)m * P[0] + t[0]) >> 32;
-#pragma unroll
-      for (int j = 1; j < 8; j++) {
-        const uint64_t s = (uint64_t)m * P[j] + t[j] + c2;
-        t[j - 1] = (uint32_t)s;
-        c2 = s >> 32;
-      }
-      const uint64_t s7 = (uint64_t)t[8] + c2;
-      t[7] = (uint32_t)s7;
-      t[8] = t[9] + (uint32_t)(s7 >> 32);
-    }
-    uint32_t r8[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) r8[i] = t[i];
-    reduce_once(r8);
-    Fp r;
-#pragma unroll
-    for (int i = 0; i < 8; i++) r.v[i] = r8[i];
-    return r;
-  }
-
-  // Full 512-bit product a*b (16 limbs), 64-bit C++ arithmetic.
-  static CSB_DEV void mul_full(uint32_t (&t)[16], const Fp& a, const Fp& b) {
-#pragma unroll
-    for (int i = 0; i < 16; i++) t[i] = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-      uint64_t c = 0;
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        const uint64_t s = (uint64_t)a.v[j] * b.v[i] + t[i + j] + c;
-        t[i + j] = (uint32_t)s;
-        c = s >> 32;
-      }
-      t[i + 8] = (uint32_t)c;
-    }
-  }
-
-  // Montgomery reduction T * 2^-256 mod p for T < p * 2^256 (16 limbs, consumed).
-  static CSB_DEV Fp redc(uint32_t (&t)[16]) {
-    const uint32_t P[8] = {M::P0, M::P1, M::P2, M::P3, M::P4, M::P5, M::P6, M::P7};
-    uint32_t hi = 0;  // overflow of limb i+8, owed to limb i+9
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-      const uint32_t m = t[i] * M::NP0;
-      uint64_t c = 0;
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        const uint64_t s = (uint64_t)m * P[j] + t[i + j] + c;
-        t[i + j] = (uint32_t)s;
-        c = s >> 32;
-      }
-      // row carry into limb i+8; its own overflow goes to limb i+9 with the next row
-      const uint64_t s8 = (uint64_t)t[i + 8] + c + hi;
-      t[i + 8] = (uint32_t)s8;
-      hi = (uint32_t)(s8 >> 32);
-    }
-    // T < p 2^256 keeps the result below 2p < 2^256: hi is 0 here
-    uint32_t r8[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) r8[i] = t[8 + i];
-    reduce_once(r8);
-    Fp r;
-#pragma unroll
-    for (int i = 0; i < 8; i++) r.v[i] = r8[i];
-    return r;
-  }
-
   friend CSB_DEV Fp operator*(const Fp& a, const Fp& b) {
-#if defined(CSB_MUL_LOHI)
-    return mul_lohi(a, b);
-#elif defined(CSB_MUL_NOINLINE)
+#if defined(CSB_MUL_NOINLINE)
     return fp_mul_call<M>(a, b);
 #else
     return mul_wide(a, b);
 #endif
   }
 
-  // CIOS Montgomery product with mad.lo / mad.hi carry chains.
-  static CSB_DEV Fp mul_lohi(const Fp& a, const Fp& b) {
-    const uint32_t (&A)[8] = a.v;
-    const uint32_t P[8] = {M::P0, M::P1, M::P2, M::P3, M::P4, M::P5, M::P6, M::P7};
-    uint32_t t[9];
-#pragma unroll
-    for (int i = 0; i < 9; i++) t[i] = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-      row_mad(t, A, b.v[i]);
-      const uint32_t m = t[0] * M::NP0;
-      row_mad(t, P, m);
-      // t[0] is now zero: shift one limb down
-#pragma unroll
-      for (int j = 0; j < 8; j++) t[j] = t[j + 1];
-      t[8] = 0;
-    }
-    uint32_t r8[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) r8[i] = t[i];
-    reduce_once(r8);
-    Fp r;
-#pragma unroll
-    for (int i = 0; i < 8; i++) r.v[i] = r8[i];
-    return r;
-  }
   CSB_DEV Fp sqr() const { return (*this) * (*this); }
 
   // x -> x * R mod p (normal form to Montgomery); any 256-bit x < 2^256 is accepted
@@ -674,9 +462,7 @@ using Fr = Fp<ModR>;
 // ------------------------------------------------------------ Fq2 = Fq[u]/(u^2+1) ----
 template <class M>
 __device__ __noinline__ Fp<M> fp_mul_call(Fp<M> a, Fp<M> b) {
-#if defined(CSB_MUL_CALL_LOHI)
-  return Fp<M>::mul_lohi(a, b);
-#elif CSB_DP52
+#if CSB_DP52
   Fp<M> r;
   dp52::mont<M>(a.v, b.v, r.v);
   return r.canon();
@@ -705,18 +491,6 @@ CSB_DEV Fp<M> Fp<M>::mul_lazy(const Fp<M>& a, const Fp<M>& b) {
 #endif
 }
 
-template <class M>
-struct FpPair {
-  Fp<M> x, y;
-};
-
-template <class M>
-__device__ __noinline__ FpPair<M> fp_mul2_call(Fp<M> a, Fp<M> b, Fp<M> c, Fp<M> d) {
-  FpPair<M> r;
-  Fp<M>::mul_wide2(a, b, c, d, r.x, r.y);
-  return r;
-}
-
 struct Fq2 {
   Fq c0, c1;
   static CSB_DEV Fq2 zero() { return {Fq::zero(), Fq::zero()}; }
@@ -727,104 +501,15 @@ struct Fq2 {
   friend CSB_DEV Fq2 operator-(const Fq2& a, const Fq2& b) { return {a.c0 - b.c0, a.c1 - b.c1}; }
   // Karatsuba, 3 products (src/cuda/ff.cpp montmult_ext_h: same non-residue -1)
   friend CSB_DEV Fq2 operator*(const Fq2& a, const Fq2& b) {
-#if CSB_FQ2_MODE == 1
-    const Fq v0 = Fq::mul_c64(a.c0, b.c0);
-    const Fq v1 = Fq::mul_c64(a.c1, b.c1);
-    const Fq s = Fq::mul_c64(a.c0 + a.c1, b.c0 + b.c1);
-    return {v0 - v1, s - v0 - v1};
-#elif CSB_FQ2_MODE == 2
-    return mul_lazy(a, b);
-#elif CSB_PAIRED
-    Fq v0, v1;
-    Fq::mul2(a.c0, b.c0, a.c1, b.c1, v0, v1);
-    const Fq s = (a.c0 + a.c1) * (b.c0 + b.c1);
-    return {v0 - v1, s - v0 - v1};
-#else
     const Fq v0 = a.c0 * b.c0;
     const Fq v1 = a.c1 * b.c1;
     const Fq s = (a.c0 + a.c1) * (b.c0 + b.c1);
     return {v0 - v1, s - v0 - v1};
-#endif
-  }
-  // x = a*b, y = c*d: six Fq products as three interleaved out-of-line pairs
-  static CSB_DEV void mul2_ool(const Fq2& a, const Fq2& b, const Fq2& c, const Fq2& d, Fq2& x, Fq2& y) {
-    Fq a0, a1, c0, c1, sa, sc;
-    Fq::mul2_ool(a.c0, b.c0, a.c1, b.c1, a0, a1);
-    Fq::mul2_ool(c.c0, d.c0, c.c1, d.c1, c0, c1);
-    Fq::mul2_ool(a.c0 + a.c1, b.c0 + b.c1, c.c0 + c.c1, d.c0 + d.c1, sa, sc);
-    x = {a0 - a1, sa - a0 - a1};
-    y = {c0 - c1, sc - c0 - c1};
-  }
-  // x = a^2, y = c^2: four Fq products as two out-of-line pairs
-  static CSB_DEV void sqr2_ool(const Fq2& a, const Fq2& c, Fq2& x, Fq2& y) {
-    Fq pa, pc, qa, qc;
-    Fq::mul2_ool(a.c0, a.c1, c.c0, c.c1, pa, pc);
-    Fq::mul2_ool(a.c0 + a.c1, a.c0 - a.c1, c.c0 + c.c1, c.c0 - c.c1, qa, qc);
-    x = {qa, pa + pa};
-    y = {qc, pc + pc};
-  }
-  static CSB_DEV void mul2(const Fq2& a, const Fq2& b, const Fq2& c, const Fq2& d, Fq2& x, Fq2& y) {
-#if CSB_PAIRED
-    mul2_ool(a, b, c, d, x, y);
-#else
-    const Fq2 xx = a * b;
-    y = c * d;
-    x = xx;
-#endif
-  }
-  static CSB_DEV void sqr2(const Fq2& a, const Fq2& c, Fq2& x, Fq2& y) {
-#if CSB_PAIRED
-    sqr2_ool(a, c, x, y);
-#else
-    const Fq2 xx = a.sqr();
-    y = c.sqr();
-    x = xx;
-#endif
-  }
-  // Karatsuba with lazy reduction: three 512-bit products, two Montgomery reductions.
-  //   c0 = a0 b0 - a1 b1 + p^2 (in [0, 2p^2)),  c1 = (a0+a1)(b0+b1) - a0 b0 - a1 b1 (< 2p^2)
-  // with the sums a0+a1, b0+b1 unreduced (< 2^255); both stay below p 2^256.
-  static CSB_DEV Fq2 mul_lazy(const Fq2& a, const Fq2& b) {
-    uint32_t v0[16], v1[16], s[16];
-    Fq::mul_full(v0, a.c0, b.c0);
-    Fq::mul_full(v1, a.c1, b.c1);
-    Fq sa, sb;
-    {
-      uint64_t ca = 0, cb = 0;
-#pragma unroll
-      for (int i = 0; i < 8; i++) {
-        ca += (uint64_t)a.c0.v[i] + a.c1.v[i];
-        cb += (uint64_t)b.c0.v[i] + b.c1.v[i];
-        sa.v[i] = (uint32_t)ca;
-        sb.v[i] = (uint32_t)cb;
-        ca >>= 32;
-        cb >>= 32;
-      }
-    }
-    Fq::mul_full(s, sa, sb);
-    // s <- s - v0 - v1 ; v0 <- v0 - v1 + p^2
-    int64_t bs = 0, b0 = 0;
-#pragma unroll
-    for (int i = 0; i < 16; i++) {
-      bs += (int64_t)s[i] - v0[i] - v1[i];
-      b0 += (int64_t)v0[i] - v1[i] + ModQ::P2_LIMB(i);
-      s[i] = (uint32_t)bs;
-      v0[i] = (uint32_t)b0;
-      bs >>= 32;  // arithmetic shift: borrow in -2..0
-      b0 >>= 32;
-    }
-    return {Fq::redc(v0), Fq::redc(s)};
   }
   // (a0 + a1 u)^2 = (a0 + a1)(a0 - a1) + 2 a0 a1 u
   CSB_DEV Fq2 sqr() const {
-#if CSB_PAIRED
-    Fq p, q;
-    Fq::mul2(c0, c1, c0 + c1, c0 - c1, p, q);
-    return {q, p + p};
-#else
     const Fq p = c0 * c1;
     return {(c0 + c1) * (c0 - c1), p + p};
-#endif
   }
   CSB_DEV Fq2 neg() const { return {c0.neg(), c1.neg()}; }
   CSB_DEV Fq2 dbl() const { return {c0.dbl(), c1.dbl()}; }

@@ -22,8 +22,7 @@ __global__ void k_field_op(int op, const uint32_t* __restrict__ a, const uint32_
   using F = Fp<M>;
   F x = ld_fp<M>(a + (size_t)i * 8);
   F y = F::zero();
-  if (op == CS_FOP_MUL || op == CS_FOP_ADD || op == CS_FOP_SUB || op == CS_FOP_MUL_LOHI ||
-      op == CS_FOP_MUL_DP52)
+  if (op == CS_FOP_MUL || op == CS_FOP_ADD || op == CS_FOP_SUB || op == CS_FOP_MUL_DP52)
     y = ld_fp<M>(b + (size_t)i * 8);
   F r;
   switch (op) {
@@ -34,8 +33,7 @@ __global__ void k_field_op(int op, const uint32_t* __restrict__ a, const uint32_
     case CS_FOP_INV: r = x.inv(); break;
     case CS_FOP_TO_MONT: r = x.to_mont(); break;
     case CS_FOP_FROM_MONT: r = x.from_mont(); break;
-    case CS_FOP_MUL_DP52: dp52::mont<M>(x.v, y.v, r.v); r = r.canon(); break;
-    default: r = F::mul_lohi(x, y); break;
+    default: dp52::mont<M>(x.v, y.v, r.v); r = r.canon(); break;  // CS_FOP_MUL_DP52
   }
   st_fp<M>(out + (size_t)i * 8, r);
 }
@@ -108,7 +106,7 @@ extern "C" {
 
 int cs_field_op_device(cs_ctx* ctx, int op, int pidx, const uint32_t* d_a, const uint32_t* d_b,
                        uint32_t* d_out, uint32_t n) {
-  if (!ctx || op < 0 || op > CS_FOP_MUL_DP52 || (pidx != 0 && pidx != 1)) return CS_ERR_ARG;
+  if (!ctx || op < 0 || op > CS_FOP_MUL_DP52 || op == 7 || (pidx != 0 && pidx != 1)) return CS_ERR_ARG;
   if (n && (!d_a || !d_out)) return CS_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);

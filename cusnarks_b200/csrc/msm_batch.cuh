@@ -154,12 +154,12 @@ cudaError_t batch_impl(const MsmBatch& b, void* d_work, size_t work_bytes, cudaS
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_accumulate<F><<<accumulate_grid<F>(sms), 128, 0, st>>>(tasks, counters, entries, nullptr, nb, buckets, partials,
+  k_accumulate<F><<<accumulate_grid<F>(dev, sms), 128, 0, st>>>(tasks, counters, entries, nullptr, nb, buckets, partials,
                                                            b.d_jobs);
   k_combine_small<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);
   k_combine<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);
   note_launch(3);
-  const uint64_t resident = (uint64_t)accumulate_grid<F>(sms) * 128;
+  const uint64_t resident = (uint64_t)accumulate_grid<F>(dev, sms) * 128;
   // reduction per window group
   for (uint32_t g = 0; g < b.ngroups; g++) {
     const BatchGroup& G = b.groups[g];

@@ -2,6 +2,7 @@
 // instantiated for G1 in msm_g1.cu and for G2 in msm_g2.cu.
 #pragma once
 #include <algorithm>
+#include <atomic>
 #include "msm.cuh"
 #include "curve.cuh"
 #include "scan.cuh"
@@ -224,11 +225,7 @@ __global__ void k_task_emit(const uint32_t* __restrict__ offsets, uint32_t nb, u
 #define CSB_ACC_G2_MINB 3  // 168 registers: 12 warps per SM instead of 8 (measured faster)
 #endif
 #ifndef CSB_ACC_G1_MINB
-#if CSB_PAIRED
-#define CSB_ACC_G1_MINB 4  // paired products fit 128 registers without spills
-#else
 #define CSB_ACC_G1_MINB 0
-#endif
 #endif
 template <class F> struct AccMinBlocks { static constexpr int value = CSB_ACC_G1_MINB; };
 template <> struct AccMinBlocks<Fq2> { static constexpr int value = CSB_ACC_G2_MINB; };
@@ -236,24 +233,9 @@ template <> struct AccMinBlocks<Fq2> { static constexpr int value = CSB_ACC_G2_M
 // The accumulation's mixed addition: over Fq with lazily reduced coordinates (no final
 // conditional subtraction per product; the bucket is canonicalised when stored), over Fq2
 // the canonical one.
-#ifndef CSB_LAZY_G1
-#define CSB_LAZY_G1 1
-#endif
-CSB_DEV XYZZ<Fq> madd_acc(const XYZZ<Fq>& acc, const Affine<Fq>& p) {
-#if CSB_LAZY_G1
-  return xyzz_madd_lazy(acc, p);
-#else
-  return xyzz_madd(acc, p);
-#endif
-}
+CSB_DEV XYZZ<Fq> madd_acc(const XYZZ<Fq>& acc, const Affine<Fq>& p) { return xyzz_madd_lazy(acc, p); }
 CSB_DEV XYZZ<Fq2> madd_acc(const XYZZ<Fq2>& acc, const Affine<Fq2>& p) { return xyzz_madd(acc, p); }
-CSB_DEV XYZZ<Fq> canon_acc(const XYZZ<Fq>& a) {
-#if CSB_LAZY_G1
-  return xyzz_canon(a);
-#else
-  return a;
-#endif
-}
+CSB_DEV XYZZ<Fq> canon_acc(const XYZZ<Fq>& a) { return xyzz_canon(a); }
 CSB_DEV XYZZ<Fq2> canon_acc(const XYZZ<Fq2>& a) { return a; }
 
 template <class F>
@@ -559,6 +541,8 @@ __global__ void __launch_bounds__(128) k_reduce_level_quad2(const uint32_t* __re
     const XYZZ<F> r = add_q(p, q);  // every lane of the warp, every step
     if (zq || even_step) a = r; else s = r;
   }
+  // the odd quads double their own s too and drop it: the quad operations shuffle across
+  // the whole warp, so every lane takes part in the same steps (no extra latency)
 #pragma unroll 1
   for (int d = 0; d < 3 * level; d++) s = dbl_q(s);
   s = add_q(s, shfl_down_xyzz(a, 4));  // even quads: + the odd neighbour's z sum
@@ -943,13 +927,7 @@ inline int auto_affine_rounds_rt(bool ec2, uint32_t n, int W, size_t nb) {
   // 2^20 fixed-base MSM 4.28 -> 5.20 ms): its mixed addition is cheap enough that the extra
   // passes lose.  L2 prefetching the round's gathers a few slots ahead did not help either
   // (G2 fixed-base 13.10 ms without, 13.27 / 13.31 / 13.40 ms 2 / 4 / 8 slots ahead).
-#ifndef CSB_AFF_G2_CAP
-#define CSB_AFF_G2_CAP 2
-#endif
-#ifndef CSB_AFF_G1_CAP
-#define CSB_AFF_G1_CAP 0
-#endif
-  const int cap = ec2 ? CSB_AFF_G2_CAP : CSB_AFF_G1_CAP;
+  const int cap = ec2 ? 2 : 0;
   const double avg = (double)n * W / (double)nb;
   int r = 0;
   while (r < cap && avg >= (double)(8u << r)) r++;
@@ -967,16 +945,19 @@ inline bool layout_affine(bool ec2, int affine_mode, uint32_t n, int c, bool fix
   return auto_affine_rounds_rt(ec2, n, W, nb) > 0;
 }
 
+// Resident blocks of k_accumulate per SM, cached per device (callers on several threads and
+// devices: server slots, the allocation-free entry point).
 template <class F>
-int accumulate_grid(int sms) {
-  static int blocks_per_sm = 0;
-  if (blocks_per_sm == 0) {
-    int b = 0;
+int accumulate_grid(int dev, int sms) {
+  static std::atomic<int> blocks_per_sm[64];
+  const int slot = dev >= 0 && dev < 64 ? dev : 0;
+  int b = blocks_per_sm[slot].load(std::memory_order_relaxed);
+  if (b == 0) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_accumulate<F>, 128, 0) != cudaSuccess || b < 1)
       b = 1;
-    blocks_per_sm = b;
+    blocks_per_sm[slot].store(b, std::memory_order_relaxed);
   }
-  return blocks_per_sm * sms;
+  return b * sms;
 }
 
 // One level of the bucket reduction (level 0: y = the buckets, z = null): one thread per
@@ -1029,7 +1010,7 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   // threads the accumulation keeps resident: an MSM whose tasks (at the shortest length) fit
   // four times over runs in latency form (one quad per task, shortest tasks)
-  const uint64_t resident = (uint64_t)accumulate_grid<F>(sms) * 128;
+  const uint64_t resident = (uint64_t)accumulate_grid<F>(dev, sms) * 128;
   const bool latency_mode = rounds_req == 0 && ((uint64_t)nb + (uint64_t)n * W / kMinTask + 1) * 4 <= resident;
   if (latency_mode) task_len = kMinTask;
   const Layout L = make_layout(n, c, XB, kMinTask, FIXED, layout_affine(EC2, cfg.affine, n, c, FIXED));
@@ -1104,10 +1085,10 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   note_launch();
   if (cfg.acc_start) cudaEventRecord(cfg.acc_start, st);
   if (latency_mode)
-    k_accumulate_quad<F><<<accumulate_grid<F>(sms), 128, 0, st>>>(tasks, counters, acc_entries, acc_points, nb,
+    k_accumulate_quad<F><<<accumulate_grid<F>(dev, sms), 128, 0, st>>>(tasks, counters, acc_entries, acc_points, nb,
                                                                   buckets, partials);
   else
-    k_accumulate<F><<<accumulate_grid<F>(sms), 128, 0, st>>>(tasks, counters, acc_entries, acc_points, nb,
+    k_accumulate<F><<<accumulate_grid<F>(dev, sms), 128, 0, st>>>(tasks, counters, acc_entries, acc_points, nb,
                                                              buckets, partials);
   note_launch();
   k_combine_small<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);

@@ -68,17 +68,20 @@ def mpoly_from_entries(n_wires: int, wire: np.ndarray, cons: np.ndarray, coeff: 
     return out
 
 
-class SyntheticCircuit:
-    def __init__(self, ctx: Context, log_m: int, seed: int = 1, n_public: int = 1, n_inputs: int = 64):
-        import torch
-        self.ctx = ctx
+class CircuitPlan:
+    """The host-side draws of the benchmark circuit (no device work): sizes, layers, the
+    A and B rows' wires, their coefficients (normal form) and the random inputs, drawn from
+    one seeded PCG64 stream in a fixed order, so every builder of the circuit from the
+    same seed gets the same circuit."""
+
+    def __init__(self, log_m: int, seed: int = 1, n_public: int = 1, n_inputs: int = 64):
         self.log_m = log_m
         self.m = m = 1 << log_m
         self.n_public = n_public
         self.n_constraints = nc = m - n_public - 1
         n_inputs = max(n_inputs, n_public + 2)
         self.n_inputs = n_inputs
-        self.n_vars = nv = n_inputs + nc
+        self.n_vars = n_inputs + nc
         rng = np.random.Generator(np.random.PCG64(seed))
         # Layers of S constraints; a constraint reads wires below the first output of its
         # layer, so the witness is computed layer by layer.  One A index and one B index
@@ -107,43 +110,64 @@ class SyntheticCircuit:
         self.b_wire = rng.integers(0, hi[:, None], size=(nc, 3)).astype(np.uint32)
         self.a_wire[:, 0] = fa
         self.b_wire[:, 1] = fb
+        # coefficients uniform in Fr (normal form; the matrices hold them in Montgomery form)
+        self.coeff = synth.random_field(rng, 6 * nc)
+        self.inputs = synth.random_field(rng, n_inputs - 1)
+
+    def initial_witness(self) -> np.ndarray:
+        """(n_vars, 8): the constant one, the random inputs, zeros for the outputs."""
+        w = np.zeros((self.n_vars, 8), dtype=np.uint32)
+        w[0, 0] = 1
+        w[1:self.n_inputs] = self.inputs
+        return w
+
+    def matrices(self, a_coeff_m: np.ndarray, b_coeff_m: np.ndarray):
+        """polsA, polsB, polsC in the reference's by-wire layout from the Montgomery-form
+        coefficients (nc, 3, 8); A gets the public-input rows (extend)."""
+        nc, nv, npub = self.n_constraints, self.n_vars, self.n_public
+        one_m = synth.to_limbs(MONT % R)
+        cons = np.repeat(np.arange(nc, dtype=np.uint32), 3)
+        ext_w = np.arange(npub + 1, dtype=np.uint32)
+        polsA = mpoly_from_entries(
+            nv, np.concatenate([self.a_wire.reshape(-1), ext_w]),
+            np.concatenate([cons, nc + ext_w]),
+            np.concatenate([a_coeff_m.reshape(-1, 8), np.tile(one_m, (npub + 1, 1))]))
+        polsB = mpoly_from_entries(nv, self.b_wire.reshape(-1), cons, b_coeff_m.reshape(-1, 8))
+        out_w = (self.n_inputs + np.arange(nc)).astype(np.uint32)
+        polsC = mpoly_from_entries(nv, out_w, np.arange(nc, dtype=np.uint32), np.tile(one_m, (nc, 1)))
+        return polsA, polsB, polsC
+
+
+class SyntheticCircuit:
+    def __init__(self, ctx: Context, log_m: int, seed: int = 1, n_public: int = 1, n_inputs: int = 64):
+        plan = CircuitPlan(log_m, seed, n_public, n_inputs)
+        self.ctx = ctx
+        for k in ("log_m", "m", "n_public", "n_constraints", "n_inputs", "n_vars", "layers", "a_wire", "b_wire"):
+            setattr(self, k, getattr(plan, k))
+        nc, n_inputs = self.n_constraints, self.n_inputs
         L = lib()
-        # coefficients: uniform Fr, stored Montgomery (as the reference's mpolys are)
-        coeff = synth.random_field(rng, 6 * nc)
-        d = _t(coeff)
+        # coefficients to Montgomery form on the GPU
+        d = _t(plan.coeff)
         ctx.field_op_device("to_mont", 1, d.data_ptr(), 0, d.data_ptr(), 6 * nc)
         ctx.sync()
         coeff_m = _np(d).reshape(nc, 6, 8)
         self.a_coeff = np.ascontiguousarray(coeff_m[:, :3])
         self.b_coeff = np.ascontiguousarray(coeff_m[:, 3:])
-        one_m = synth.to_limbs(MONT % R)
         # witness: constant one, random inputs, then outputs layer by layer on the GPU
-        w = np.zeros((nv, 8), dtype=np.uint32)
-        w[0, 0] = 1
-        w[1:n_inputs] = synth.random_field(rng, n_inputs - 1)
-        dw = _t(w)
+        dw = _t(plan.initial_witness())
         da_wire, db_wire = _t(self.a_wire.reshape(-1)), _t(self.b_wire.reshape(-1))
         da_coeff, db_coeff = _t(self.a_coeff.reshape(-1)), _t(self.b_coeff.reshape(-1))
         doff = _t(np.arange(0, 3 * nc + 1, 3, dtype=np.uint32))
-        for c0, c1, *_ in bounds:
+        for c0, c1, *_ in plan.layers:
             check(L.cs_r1cs_layer_eval(ctx.handle, _vp(doff.data_ptr() + 4 * c0), _vp(da_wire.data_ptr()),
                                        _vp(da_coeff.data_ptr()), _vp(doff.data_ptr() + 4 * c0),
                                        _vp(db_wire.data_ptr()), _vp(db_coeff.data_ptr()), c1 - c0,
                                        _vp(dw.data_ptr()), _vp(dw.data_ptr() + 32 * (n_inputs + c0))),
                   ctx.handle)
         ctx.sync()
-        self.w = _np(dw).reshape(nv, 8).copy()
+        self.w = _np(dw).reshape(self.n_vars, 8).copy()
         self.d_w = dw
-        # QAP matrices in the reference layout; A gets the public-input rows (extend)
-        cons = np.repeat(np.arange(nc, dtype=np.uint32), 3)
-        ext_w = np.arange(n_public + 1, dtype=np.uint32)
-        self.polsA = mpoly_from_entries(
-            nv, np.concatenate([self.a_wire.reshape(-1), ext_w]),
-            np.concatenate([cons, nc + ext_w]),
-            np.concatenate([self.a_coeff.reshape(-1, 8), np.tile(one_m, (n_public + 1, 1))]))
-        self.polsB = mpoly_from_entries(nv, self.b_wire.reshape(-1), cons, self.b_coeff.reshape(-1, 8))
-        out_w = (n_inputs + np.arange(nc)).astype(np.uint32)
-        self.polsC = mpoly_from_entries(nv, out_w, np.arange(nc, dtype=np.uint32), np.tile(one_m, (nc, 1)))
+        self.polsA, self.polsB, self.polsC = plan.matrices(self.a_coeff, self.b_coeff)
 
     @property
     def public_inputs(self) -> np.ndarray:
@@ -154,6 +178,12 @@ def _inv(x: int) -> int:
     return pow(x, -1, R)
 
 
+def toxic_waste(seed: int):
+    """(t, alpha, beta, gamma, delta), uniform in Fr from a seeded PCG64 stream."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return tuple(synth.from_limbs(x) for x in synth.random_field(rng, 5))
+
+
 def setup_pk(ctx: Context, circ: SyntheticCircuit, seed: int = 7) -> dict:
     """Proving and verifying key from seeded toxic waste (t, alpha, beta, gamma, delta)."""
     import torch
@@ -161,8 +191,7 @@ def setup_pk(ctx: Context, circ: SyntheticCircuit, seed: int = 7) -> dict:
     # the library's kernels run asynchronously on the context stream: every temporary
     # they read stays referenced here until the final synchronisation
     keep = []
-    rng = np.random.Generator(np.random.PCG64(seed))
-    t, alpha, beta, gamma, delta = (synth.from_limbs(x) for x in synth.random_field(rng, 5))
+    t, alpha, beta, gamma, delta = toxic_waste(seed)
     m, nv, npub = circ.m, circ.n_vars, circ.n_public
     mont = lambda x: synth.to_limbs((x * MONT) % R)  # noqa: E731
     dt = _t(mont(t))

@@ -66,6 +66,17 @@ class PlainProver:
         self.roots = roots_table(self.levels)
         self.polsA = np.ascontiguousarray(pk["polsA"], dtype=np.uint32).reshape(-1)
         self.polsB = np.ascontiguousarray(pk["polsB"], dtype=np.uint32).reshape(-1)
+        # the key's point arrays of the five multi-exponentiations, contiguous host arrays
+        # made once per key (the reference loads its key once); each call still copies them
+        # to the GPU, as the reference's multi-exp does
+        nv, npub, m = pk["n_vars"], pk["n_public"], self.m
+        key = lambda a, lo, hi, pw: np.ascontiguousarray(np.asarray(a, dtype=np.uint32).reshape(-1, pw)[lo:hi])  # noqa: E731
+        self.pts_a = key(pk["A"], 0, nv + 2, 16)
+        self.pts_b2 = key(pk["B2"], 0, nv + 2, 32)
+        self.pts_b1 = key(pk["B1"], 0, nv + 2, 16)
+        self.pts_c = key(pk["C"], npub + 1, nv, 16)
+        self.pts_h = np.ascontiguousarray(np.concatenate([np.asarray(pk["hExps"], dtype=np.uint32).reshape(-1, 16)[:m - 1],
+                                                          np.asarray(pk["delta_1"], dtype=np.uint32).reshape(-1, 16)]))
 
     def _mpoly(self, w, pin):
         nv = self.pk["n_vars"]
@@ -106,13 +117,12 @@ class PlainProver:
         M = np.ctypeslib.as_array(ptr, shape=((2 * m) * 8,)).reshape(-1, 8)
         polH = M[m:2 * m - 1].copy()
         neg_rs = (-(r * s)) % R
-        pi_a = self._msm(_ext(w, [1, r]), pk["A"][:nv + 2])
-        pi_b = self._msm(_ext(w, [1, s]), pk["B2"][:nv + 2], ec2=True)
-        pi_b1 = self._msm(_ext(w, [1, s]), pk["B1"][:nv + 2])
-        pi_c = self._msm(w[npub + 1:nv], np.asarray(pk["C"]).reshape(-1, 16)[npub + 1:nv])
-        hpts = np.concatenate([np.asarray(pk["hExps"]).reshape(-1, 16)[:m - 1],
-                               np.asarray(pk["delta_1"]).reshape(-1, 16)])
-        pi_c2 = self._msm(_ext(polH, [neg_rs]), hpts)
+        ws = _ext(w, [1, s])
+        pi_a = self._msm(_ext(w, [1, r]), self.pts_a)
+        pi_b = self._msm(ws, self.pts_b2, ec2=True)
+        pi_b1 = self._msm(ws, self.pts_b1)
+        pi_c = self._msm(w[npub + 1:nv], self.pts_c)
+        pi_c2 = self._msm(_ext(polH, [neg_rs]), self.pts_h)
         fin = self._msm(np.stack([_limbs(1), _limbs(1), _limbs(s), _limbs(r)]),
                         np.stack([pi_c2, pi_c, pi_a, pi_b1]))
         return np.concatenate([pi_a, pi_b, fin]).astype(np.uint32)

@@ -267,7 +267,6 @@ int cs_msm_tuned_window(cs_ctx *ctx, int ec2, uint32_t n);
 #define CS_FOP_INV 4       /* Montgomery inverse (aR)^-1 R, 0 -> 0 */
 #define CS_FOP_TO_MONT 5   /* a -> aR */
 #define CS_FOP_FROM_MONT 6 /* aR -> a */
-#define CS_FOP_MUL_LOHI 7  /* Montgomery product, mad.lo/mad.hi variant (cross-check) */
 #define CS_FOP_FQ2_MUL 8
 #define CS_FOP_MUL_DP52 9  /* Montgomery product, radix-2^52 FP64-pipe variant (cross-check) */
 int cs_field_op_device(cs_ctx *ctx, int op, int pidx, const uint32_t *d_a, const uint32_t *d_b,
@@ -401,8 +400,10 @@ void writeWitnessFile_h(uint32_t *samples, const char *filename, unsigned long l
  * latency-critical path.  Inputs and output are the caller's device pointers (same
  * layout as cs_msm_device, automatic window); scratch is a fixed file-scope device array
  * of cs_msm_noalloc_scratch_bytes() bytes (32 MiB) that every GPU loading this library
- * keeps reserved until exit, which bounds n to cs_msm_g1_noalloc_max_terms() (2^16);
- * larger n is rejected with CS_ERR_ARG and a message in cs_msm_g1_noalloc_error().
+ * keeps reserved until exit, which bounds n to cs_msm_g1_noalloc_max_terms() (at least
+ * 2^16; query the function rather than hard-coding a figure: 69,843 with the current
+ * automatic window); larger n is rejected with CS_ERR_ARG and a message in
+ * cs_msm_g1_noalloc_error().
  * Runs asynchronously on `stream` (a cudaStream_t, NULL = legacy default stream).  The
  * first call on a device looks up the array's device address (cudaGetSymbolAddress) with
  * that device current; make that first call before any stream capture.  Every call shares
@@ -521,18 +522,9 @@ int cs_r1cs_layer_eval(cs_ctx *ctx, const uint32_t *a_off, const uint32_t *a_wir
                        const uint32_t *d_w, uint32_t *d_out);
 
 /* ------------------------------------------------------------ measurement ----------- */
-/* Sustained 32-bit integer multiply-add instruction rate of the context's device
- * (instructions per second, all SMs), the ceiling for the integer-bound kernels. */
-int cs_bench_imad_peak(cs_ctx *ctx, double *imad_per_s);
 /* Instruction-rate probes (ops per second, all SMs): mode 1 mad.lo.u32, 2 mad.hi.u32,
  * 3 mad.wide.u32, 4 fma.rn.f64, 5 carry-chained mad.lo.cc/madc.hi.cc. */
 int cs_bench_pipe(cs_ctx *ctx, int mode, double *ops_per_s);
-/* Montgomery products per second (variant 0: mad.lo/mad.hi CIOS, 1: wide-product CIOS;
- * variant 2 reports 32-bit add-with-carry instructions per second instead). */
-int cs_bench_mulmod(cs_ctx *ctx, int variant, double *rate);
-/* Single-thread latency, ns per Montgomery product, of `chains` (1 or 4) independent
- * dependent chains: variant 0 flag-carry CIOS, 1 wide-product CIOS, 2 carry-flag-free CIOS. */
-int cs_bench_mul_latency(cs_ctx *ctx, int variant, int chains, double *ns_per_mul);
 /* Number of kernels this library has launched in the process so far. */
 unsigned long long cs_kernel_launches(void);
 

@@ -744,3 +744,294 @@ void or_mpoly_eval(uint32_t *pout, const uint32_t *scalar, const uint32_t *pin,
     doff = acc * 9 + 1 + npoly;
   }
 }
+
+/* ----------------------------------------------------- batched products ----------- */
+/* z[i] = a[i] * b[i] * 2^-256 mod p for n pairs (OpenMP).  Operands may be any 256-bit
+ * values: they are reduced mod p first, so lazily reduced inputs in [p, 2^256) give the
+ * product of their residues (montmult_h, src/cuda/ff.cpp:225, on reduced operands). */
+static void reduce4(uint64_t *x, const modctx_t *m) {
+  while (geq4(x, m->p)) sub4(x, x, m->p);
+}
+void or_montmult_batch(uint32_t *z, const uint32_t *a, const uint32_t *b, uint64_t n, uint32_t pidx) {
+  init_mods();
+  const modctx_t *m = &MODS[pidx];
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < (long)n; i++) {
+    uint64_t x[4], y[4], t[4];
+    memcpy(x, a + 8 * (size_t)i, 32);
+    memcpy(y, b + 8 * (size_t)i, 32);
+    reduce4(x, m);
+    reduce4(y, m);
+    fmul(t, x, y, m);
+    memcpy(z + 8 * (size_t)i, t, 32);
+  }
+}
+
+/* ------------------------------------ benchmark circuit and proving key on the CPU --- */
+/* The benchmark's synthetic circuit and its proving key, built without a GPU (for a
+ * process that must not load the CUDA library).  The quantities are those of Groth16
+ * setup as the reference computes them (src/python/groth_setup.py: calculateValuesAtT
+ * :771, calculateEncryptedValuesAtT :488): Lagrange basis at t, wire polynomials at t,
+ * the C scalars (beta u + alpha v + w)/delta, t^j Z(t)/delta, and fixed-base scalar
+ * multiplications of the generators. */
+
+/* Witness of the synthetic circuit, constraints in order: w[first_out + c] =
+ * (sum_k a_coeff * w[a_wire]) * (sum_k b_coeff * w[b_wire]), `per_row` terms each side,
+ * coefficients Montgomery, witness normal form.  A constraint reads only wires defined
+ * before its layer, so one pass in order computes every output. */
+void or_r1cs_eval(uint32_t *w, uint64_t first_out, uint64_t nc, uint32_t per_row,
+                  const uint32_t *a_wire, const uint32_t *a_coeff,
+                  const uint32_t *b_wire, const uint32_t *b_coeff) {
+  init_mods();
+  const modctx_t *m = &MODS[1];
+  for (uint64_t c = 0; c < nc; c++) {
+    uint64_t sa[4] = {0, 0, 0, 0}, sb[4] = {0, 0, 0, 0}, t[4], v[4], x[4];
+    for (uint32_t k = 0; k < per_row; k++) {
+      const uint64_t e = c * per_row + k;
+      memcpy(v, a_coeff + 8 * e, 32);
+      memcpy(x, w + 8 * (size_t)a_wire[e], 32);
+      fmul(t, v, x, m);           /* Montgomery coefficient times normal value = normal */
+      fadd(sa, sa, t, m);
+      memcpy(v, b_coeff + 8 * e, 32);
+      memcpy(x, w + 8 * (size_t)b_wire[e], 32);
+      fmul(t, v, x, m);
+      fadd(sb, sb, t, m);
+    }
+    fmul(t, sa, sb, m);           /* sa sb / R */
+    fmul(t, t, m->r2, m);         /* sa sb */
+    memcpy(w + 8 * (first_out + c), t, 32);
+  }
+}
+
+/* out[i] = 1 / in[i] for n nonzero Montgomery elements of Fr (one inversion). */
+static void batch_inv_fr(uint64_t *out, const uint64_t *in, uint64_t n) {
+  const modctx_t *m = &MODS[1];
+  if (n == 0) return;
+  uint64_t *pre = (uint64_t *)malloc(32 * n), acc[4], inv[4], t[4];
+  memcpy(acc, m->one, 32);
+  for (uint64_t i = 0; i < n; i++) {
+    fmul(acc, acc, in + 4 * i, m);
+    memcpy(pre + 4 * i, acc, 32);
+  }
+  finv(inv, acc, m);
+  for (uint64_t i = n; i-- > 0;) {
+    if (i) fmul(t, inv, pre + 4 * (i - 1), m); else memcpy(t, inv, 32);
+    fmul(inv, inv, in + 4 * i, m);
+    memcpy(out + 4 * i, t, 32);
+  }
+  free(pre);
+}
+
+/* Lagrange basis of the domain <w> (m = 2^levels, w the reference's primitive root) at
+ * t: L_c(t) = w^c (t^m - 1) / (m (t - w^c)), Montgomery in and out. */
+void or_lagrange_at(uint32_t *out, uint32_t levels, const uint32_t *t_mont) {
+  init_mods();
+  const modctx_t *m = &MODS[1];
+  const uint64_t n = 1ull << levels;
+  uint64_t t[4], tm[4], zm[4], nn[4] = {0, 0, 0, 0}, ninv[4];
+  memcpy(t, t_mont, 32);
+  memcpy(tm, t, 32);
+  for (uint32_t k = 0; k < levels; k++) fmul(tm, tm, tm, m);
+  fsub(zm, tm, m->one, m);
+  nn[levels >> 6] = 1ull << (levels & 63);
+  fmul(ninv, nn, m->r2, m);
+  finv(ninv, ninv, m);
+  fmul(zm, zm, ninv, m);           /* (t^m - 1) / m */
+  uint64_t *wp = (uint64_t *)malloc(32 * n), *den = (uint64_t *)malloc(32 * n);
+  or_find_roots((uint32_t *)wp, levels);
+  for (uint64_t c = 0; c < n; c++) fsub(den + 4 * c, t, wp + 4 * c, m);
+  batch_inv_fr(den, den, n);
+  for (uint64_t c = 0; c < n; c++) {
+    uint64_t v[4];
+    fmul(v, zm, wp + 4 * c, m);
+    fmul(v, v, den + 4 * c, m);
+    memcpy(out + 8 * c, v, 32);
+  }
+  free(wp);
+  free(den);
+}
+
+/* Wire polynomials at t: out[i] = sum over wire i's (c, coeff) of coeff * L[c] for
+ * c < n_rows, reference mpoly layout (src/cuda/mpoly.cpp:195), Montgomery. */
+void or_wire_eval(uint32_t *out, const uint32_t *mpoly, const uint32_t *Lc, uint32_t n_rows) {
+  init_mods();
+  const modctx_t *m = &MODS[1];
+  const uint64_t nw = mpoly[0];
+  uint64_t *start = (uint64_t *)malloc(8 * (nw + 1));
+  start[0] = 0;
+  for (uint64_t i = 0; i < nw; i++) start[i + 1] = start[i] + mpoly[1 + i];
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < (long)nw; i++) {
+    const uint64_t nc = mpoly[1 + i];
+    const uint64_t blk = 1 + nw + 9 * start[i];
+    uint64_t acc[4] = {0, 0, 0, 0}, v[4], l[4], t[4];
+    for (uint64_t k = 0; k < nc; k++) {
+      const uint32_t c = mpoly[blk + k];
+      if (c >= n_rows) continue;
+      memcpy(v, mpoly + blk + nc + 8 * k, 32);
+      memcpy(l, Lc + 8 * (size_t)c, 32);
+      fmul(t, v, l, m);
+      fadd(acc, acc, t, m);
+    }
+    memcpy(out + 8 * (size_t)i, acc, 32);
+  }
+  free(start);
+}
+
+/* out[i] (normal form) = (beta u_i + alpha v_i + w_i) k, inputs Montgomery. */
+void or_c_scalars(uint32_t *out, const uint32_t *u, const uint32_t *v, const uint32_t *w,
+                  const uint32_t *alpha, const uint32_t *beta, const uint32_t *k, uint64_t n) {
+  init_mods();
+  const modctx_t *m = &MODS[1];
+  uint64_t al[4], be[4], kk[4], one[4] = {1, 0, 0, 0};
+  memcpy(al, alpha, 32); memcpy(be, beta, 32); memcpy(kk, k, 32);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < (long)n; i++) {
+    uint64_t x[4], y[4], t[4];
+    memcpy(t, u + 8 * (size_t)i, 32);
+    fmul(x, be, t, m);
+    memcpy(t, v + 8 * (size_t)i, 32);
+    fmul(y, al, t, m);
+    fadd(x, x, y, m);
+    memcpy(t, w + 8 * (size_t)i, 32);
+    fadd(x, x, t, m);
+    fmul(x, x, kk, m);
+    fmul(x, x, one, m);
+    memcpy(out + 8 * (size_t)i, x, 32);
+  }
+}
+
+/* out[j] (normal form) = t^j k for j < n, t and k Montgomery. */
+void or_pow_scalars(uint32_t *out, const uint32_t *t_mont, const uint32_t *k, uint64_t n) {
+  init_mods();
+  const modctx_t *m = &MODS[1];
+  uint64_t t[4], acc[4], one[4] = {1, 0, 0, 0}, x[4];
+  memcpy(t, t_mont, 32);
+  memcpy(acc, k, 32);
+  for (uint64_t j = 0; j < n; j++) {
+    fmul(x, acc, one, m);
+    memcpy(out + 8 * j, x, 32);
+    fmul(acc, acc, t, m);
+  }
+}
+
+/* Jacobian P plus affine A (not infinity), the formulas of ec_jacaddmixed_h
+ * (src/cuda/ec.cpp:216) with Z2 = 1; equal points double, opposite ones give infinity. */
+static void pt_madd(uint64_t *R, const uint64_t *P, const uint64_t *A, const fops_t *f) {
+  const modctx_t *m = &MODS[0];
+  const int w = f->w;
+  if (pt_isinf(P, w)) {
+    memcpy(R, A, 2 * 8 * w);
+    e_one(R + 2 * w, w);
+    return;
+  }
+  uint64_t z1s[MAXW], z1c[MAXW], U2[MAXW], S2[MAXW], H[MAXW], Rr[MAXW], HH[MAXW], HHH[MAXW];
+  uint64_t V[MAXW], X3[MAXW], Y3[MAXW], Z3[MAXW], t[MAXW];
+  f->mul(z1s, P + 2 * w, P + 2 * w, m);
+  f->mul(z1c, z1s, P + 2 * w, m);
+  f->mul(U2, A, z1s, m);
+  f->mul(S2, A + w, z1c, m);
+  if (memcmp(U2, P, 8 * w) == 0) {
+    if (memcmp(S2, P + w, 8 * w) != 0) { pt_inf(R, w); return; }
+    uint64_t tmp[3 * MAXW];
+    memcpy(tmp, P, 3 * 8 * w);
+    pt_double(R, tmp, f);
+    return;
+  }
+  f->sub(H, U2, P, m);
+  f->sub(Rr, S2, P + w, m);
+  f->mul(HH, H, H, m);
+  f->mul(HHH, H, HH, m);
+  f->mul(V, P, HH, m);
+  f->mul(X3, Rr, Rr, m);
+  f->sub(X3, X3, HHH, m);
+  f->sub(X3, X3, V, m);
+  f->sub(X3, X3, V, m);
+  f->sub(t, V, X3, m);
+  f->mul(Y3, Rr, t, m);
+  f->mul(t, P + w, HHH, m);
+  f->sub(Y3, Y3, t, m);
+  f->mul(Z3, P + 2 * w, H, m);
+  memcpy(R, X3, 8 * w); memcpy(R + w, Y3, 8 * w); memcpy(R + 2 * w, Z3, 8 * w);
+}
+
+/* Jacobian -> affine for n points with one inversion (Montgomery's simultaneous
+ * inversion over the nonzero Z); infinity -> (0, 1_mont). */
+static void jac_to_aff_batch(uint64_t *A, const uint64_t *P, uint64_t n, const fops_t *f) {
+  const modctx_t *m = &MODS[0];
+  const int w = f->w;
+  const size_t PJ = 3 * (size_t)w, PA = 2 * (size_t)w;
+  uint64_t *pre = (uint64_t *)malloc(8 * (size_t)w * (n + 1));
+  uint64_t acc[MAXW], inv[MAXW], zi[MAXW], zi2[MAXW], zi3[MAXW];
+  e_one(acc, w);
+  for (uint64_t i = 0; i < n; i++) {
+    if (!pt_isinf(P + i * PJ, w)) f->mul(acc, acc, P + i * PJ + 2 * w, m);
+    memcpy(pre + (size_t)w * i, acc, 8 * w);
+  }
+  if (w == 4) finv(inv, acc, m); else f2inv(inv, acc, m);
+  for (uint64_t i = n; i-- > 0;) {
+    const uint64_t *Q = P + i * PJ;
+    if (pt_isinf(Q, w)) {
+      memset(A + i * PA, 0, 8 * PA);
+      e_one(A + i * PA + w, w);
+      continue;
+    }
+    if (i) f->mul(zi, inv, pre + (size_t)w * (i - 1), m); else memcpy(zi, inv, 8 * w);
+    f->mul(inv, inv, Q + 2 * w, m);
+    f->mul(zi2, zi, zi, m);
+    f->mul(zi3, zi2, zi, m);
+    f->mul(A + i * PA, Q, zi2, m);
+    f->mul(A + i * PA + w, Q + w, zi3, m);
+  }
+  free(pre);
+}
+
+/* out[i] = scl[i] * G for one base G (affine Montgomery, not infinity); scalars normal
+ * form below 2^256; affine Montgomery out.  Comb over 8-bit windows: table
+ * T[j][d] = d 2^(8j) G, then 32 mixed additions per scalar, affine conversion with one
+ * inversion per run of 256 points (the fixed-base multiplication of the reference's
+ * sc1mulecjac kernel, src/cuda/ecbn128_device.cu:326, in another schedule). */
+void or_fixed_base_mul(uint32_t *out_aff, const uint32_t *scl, uint64_t n, const uint32_t *base_aff,
+                       uint32_t ec2) {
+  init_mods();
+  const fops_t *f = &FOPS[ec2 ? 1 : 0];
+  const int w = f->w;
+  const size_t PJ = 3 * (size_t)w, PA = 2 * (size_t)w;
+  uint64_t *tab = (uint64_t *)malloc(8 * PA * 32 * 256);
+  {
+    uint64_t B[3 * MAXW], A[2 * MAXW];
+    memcpy(A, base_aff, 8 * PA);
+    aff_to_jac(B, A, w);
+    uint64_t *jt = (uint64_t *)malloc(8 * PJ * 32 * 256);
+    for (int j = 0; j < 32; j++) {
+      uint64_t *row = jt + (size_t)j * 256 * PJ;
+      pt_inf(row, w);
+      for (int d = 1; d < 256; d++) pt_add(row + d * PJ, row + (d - 1) * PJ, B, f);
+      for (int k = 0; k < 8; k++) pt_double(B, B, f);
+    }
+    jac_to_aff_batch(tab, jt, 32 * 256, f);
+    free(jt);
+  }
+  const uint64_t RUN = 256;
+  const uint64_t nruns = (n + RUN - 1) / RUN;
+#pragma omp parallel
+  {
+    uint64_t *jac = (uint64_t *)malloc(8 * PJ * RUN), *aff = (uint64_t *)malloc(8 * PA * RUN);
+#pragma omp for schedule(dynamic, 4)
+    for (long r = 0; r < (long)nruns; r++) {
+      const uint64_t lo = (uint64_t)r * RUN, hi = lo + RUN < n ? lo + RUN : n;
+      for (uint64_t i = lo; i < hi; i++) {
+        uint64_t *acc = jac + (i - lo) * PJ;
+        pt_inf(acc, w);
+        const uint8_t *k = (const uint8_t *)(scl + 8 * i);
+        for (int j = 0; j < 32; j++)
+          if (k[j]) pt_madd(acc, acc, tab + ((size_t)j * 256 + k[j]) * PA, f);
+      }
+      jac_to_aff_batch(aff, jac, hi - lo, f);
+      memcpy(out_aff + 4 * (size_t)w * lo, aff, 8 * PA * (hi - lo));
+    }
+    free(jac);
+    free(aff);
+  }
+  free(tab);
+}

@@ -65,6 +65,21 @@ void or_hstep_coset(uint32_t *H, const uint32_t *A, const uint32_t *B, const uin
 void or_mpoly_eval(uint32_t *pout, const uint32_t *scalar, const uint32_t *pin,
                    uint32_t start_idx, uint32_t last_idx, uint32_t pidx);
 
+/* batched Montgomery products of any 256-bit operands (reduced mod p first) */
+void or_montmult_batch(uint32_t *z, const uint32_t *a, const uint32_t *b, uint64_t n, uint32_t pidx);
+
+/* the benchmark circuit's witness and proving key without a GPU */
+void or_r1cs_eval(uint32_t *w, uint64_t first_out, uint64_t nc, uint32_t per_row,
+                  const uint32_t *a_wire, const uint32_t *a_coeff,
+                  const uint32_t *b_wire, const uint32_t *b_coeff);
+void or_lagrange_at(uint32_t *out, uint32_t levels, const uint32_t *t_mont);
+void or_wire_eval(uint32_t *out, const uint32_t *mpoly, const uint32_t *Lc, uint32_t n_rows);
+void or_c_scalars(uint32_t *out, const uint32_t *u, const uint32_t *v, const uint32_t *w,
+                  const uint32_t *alpha, const uint32_t *beta, const uint32_t *k, uint64_t n);
+void or_pow_scalars(uint32_t *out, const uint32_t *t_mont, const uint32_t *k, uint64_t n);
+void or_fixed_base_mul(uint32_t *out_aff, const uint32_t *scl, uint64_t n, const uint32_t *base_aff,
+                       uint32_t ec2);
+
 #ifdef __cplusplus
 }
 #endif

@@ -3,7 +3,7 @@
 Run in a container that has the reference mounted (default /root/reference) and the
 reference CPU library built (``make -C oracle ref``):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref DIR]  (default: $CUSNARKS_REF, else /root/reference)
 
 Sources:
   * test/c/aux_data/test_scmul_samples.tbin, test_scmul_reduction_soln.tbin,
@@ -59,7 +59,7 @@ def make_mpoly(rng, nvars: int, ncons: int, nnz_per_var: int, oracle: Oracle):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("CUSNARKS_REF", "/root/reference"))
     args = ap.parse_args()
     aux = os.path.join(args.ref, "test", "c", "aux_data")
     src = open(os.path.join(args.ref, "test", "c", "test_utils_host.cpp")).read()

@@ -1,7 +1,7 @@
 """Regenerate tests/golden/pk_files.npz: a proving key written by the reference's own writer
 and a witness file written by the reference's own C routine.
 
-    python tests/golden/make_pkbin.py [--ref /root/reference]
+    python tests/golden/make_pkbin.py [--ref DIR]  (default: $CUSNARKS_REF, else /root/reference)
 
 * Proving key: src/python/pysnarks_utils.py pkvars_to_bin(FMT_MONT, EC_T_AFFINE, pk, ext=True)
   imported from the reference tree.  The module imports Python-2 compatibility packages
@@ -49,7 +49,7 @@ def _shim_py2_compat():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("CUSNARKS_REF", "/root/reference"))
     args = ap.parse_args()
     o = Oracle()
     rng = np.random.Generator(np.random.PCG64(2025))

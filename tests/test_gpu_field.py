@@ -40,7 +40,6 @@ def test_binary_ops(ctx, oracle, pidx):
     b = np.concatenate([random_field(rng, 4000, pidx), _edge(MOD[pidx])[::-1]])
     want_mul = oracle.montmult(a, b, pidx)
     assert np.array_equal(_run(ctx, "mul", pidx, a, b), want_mul)
-    assert np.array_equal(_run(ctx, "mul_lohi", pidx, a, b), want_mul)
     assert np.array_equal(_run(ctx, "mul_dp52", pidx, a, b), want_mul)
     z_add = np.zeros_like(a); z_sub = np.zeros_like(a)
     P = ctypes.POINTER(ctypes.c_uint32)
@@ -118,3 +117,48 @@ def test_mul_dp52_lazy_inputs(ctx, oracle, pidx):
     a2 = np.where((mix & 1)[:, None] == 1, plus_p(a), a).astype(np.uint32)
     b2 = np.where((mix & 2)[:, None] == 2, plus_p(b), b).astype(np.uint32)
     assert np.array_equal(_run(ctx, "mul_dp52", pidx, a2, b2), want)
+
+
+def _structured(p):
+    """Operands in [0, 2p) at the edges of the radix-2^52 cut and of the lazy range: 0, 1,
+    p - 1, p, p + 1, 2p - 1, 2p - 2, values at the 2^52, 2^104, 2^156, 2^208 limb boundaries
+    (and those plus p), R mod p and its double."""
+    vals = {0, 1, 2, p - 1, p, p + 1, 2 * p - 1, 2 * p - 2, (1 << 256) % p, (2 << 256) % p}
+    for b in (52, 104, 156, 208):
+        for v in ((1 << b) - 1, 1 << b, (1 << b) + 1, p - (1 << b), p + (1 << b), p + (1 << b) - 1):
+            if 0 <= v < 2 * p:
+                vals.add(v)
+    return sorted(vals)
+
+
+@pytest.mark.parametrize("pidx", [0, 1])
+def test_mul_dp52_ten_million_products(ctx, oracle, pidx):
+    """10^7 random products (half the operands lifted into [p, 2p)) plus every pair of the
+    structured edge operands, radix-2^52 FP64-pipe product against the oracle's montmult_h
+    restatement (ff.cpp:225), all words equal."""
+    from oracle.oracle import _p
+    p = MOD[pidx]
+    n = 10_000_000
+    rng = np.random.Generator(np.random.PCG64(1000 + pidx))
+    a = random_field(rng, n, pidx)
+    b = random_field(rng, n, pidx)
+    # lift every other operand by p (a lazily reduced value, still below 2p < 2^256)
+    pl = ints_to_limbs([p])[0].astype(np.uint64)
+    for x, sel in ((a, slice(0, n, 2)), (b, slice(1, n, 3))):
+        v = x[sel].astype(np.uint64)
+        carry = np.zeros(v.shape[0], dtype=np.uint64)
+        for i in range(8):
+            t = v[:, i] + pl[i] + carry
+            v[:, i] = t & 0xFFFFFFFF
+            carry = t >> 32
+        x[sel] = v.astype(np.uint32)
+    e = ints_to_limbs(_structured(p))
+    ea = np.repeat(e, e.shape[0], axis=0)
+    eb = np.tile(e, (e.shape[0], 1))
+    a = np.ascontiguousarray(np.concatenate([a, ea]))
+    b = np.ascontiguousarray(np.concatenate([b, eb]))
+    want = np.zeros_like(a)
+    oracle.lib.or_montmult_batch(_p(want), _p(a), _p(b), ctypes.c_uint64(a.shape[0]), pidx)
+    got = _run(ctx, "mul_dp52", pidx, a, b)
+    bad = np.nonzero((got != want).any(axis=1))[0]
+    assert bad.size == 0, (bad.size, bad[:5])

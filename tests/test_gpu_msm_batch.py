@@ -103,3 +103,30 @@ def test_autotune_feeds_batch(ctx):
             assert np.array_equal(got, _single(ctx, ins[q][1], ins[q][2], n, 0, False)), q
     finally:
         batch.close()
+
+
+@pytest.mark.parametrize("ec2", [False, True])
+def test_batch_config4_sizes_against_oracle(ctx, oracle, ec2):
+    """Instances of the batched configuration's size range up to 2^16 terms (log-uniform and
+    ragged), one batch, graph replay: every instance equals the oracle's multi-exp."""
+    import torch
+    if ec2:
+        sizes = [1 << 10, 1 << 16, 5000, 1 << 13]
+    else:
+        sizes = [1 << 16, 1 << 10, 1 << 11, 1 << 12, 1 << 13, 1 << 14, 1 << 15, 3000, 50000]
+    ins, jobs = _case(ctx, sizes, [0] * len(sizes), ec2, seed=90 if ec2 else 80)
+    batch = ctx.msm_batch(jobs, ec2=ec2)
+    try:
+        batch.run(graph=True)
+        ctx.sync()
+        for (_, _, _, do) in ins:
+            do.zero_()
+        torch.cuda.synchronize()
+        batch.run(graph=True)  # replay
+        ctx.sync()
+        for q, n in enumerate(sizes):
+            got = ins[q][3].cpu().numpy().view(np.uint32)
+            p = ins[q][2].cpu().numpy().view(np.uint32)[:n]
+            assert np.array_equal(got, oracle.msm(ins[q][0][:n], p, ec2=1 if ec2 else 0)), (q, n)
+    finally:
+        batch.close()

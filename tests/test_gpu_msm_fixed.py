@@ -141,3 +141,41 @@ def test_fixed_equals_generic_large(ctx):
     gen = ctx.msm(s, p)
     w = ctx.msm_fixed_window(n)
     assert np.array_equal(fixed_msm(ctx, s, p, w), gen)
+
+
+def _neg(p, ec2=False):
+    """-P of an affine Montgomery point (y -> q - y per coordinate; 0 stays 0)."""
+    out = p.copy()
+    w = 16 if ec2 else 8
+    for k in range(w // 8):
+        y = limbs_to_int(p[w + 8 * k:w + 8 * (k + 1)])
+        out[w + 8 * k:w + 8 * (k + 1)] = ints_to_limbs([(Q - y) % Q])[0]
+    return out
+
+
+@pytest.mark.parametrize("ec2,rounds", [(True, 1), (True, 2), (False, 1), (False, 2)])
+def test_fixed_affine_rounds_match_oracle(ctx, oracle, pts_g1, pts_g2, ec2, rounds):
+    """Batch-affine rounds forced on a fixed-base MSM: round one gathers table rows j*n + i
+    through the sorted entries (k_affine_round with FIRST), later rounds their outputs.
+    Many copies of P and -P under one scalar put equal points (doublings), opposite points
+    (infinity inside the rounds) and their results side by side in the same buckets; points
+    at infinity and zero scalars are among the terms."""
+    pts = pts_g2 if ec2 else pts_g1
+    inf = _inf(oracle, ec2)
+    P = pts[3].copy()
+    rest = list(pts[100:100 + 400])
+    p = np.stack([P] * 48 + [_neg(P, ec2)] * 40 + [inf] * 8 + rest)
+    rng = np.random.Generator(np.random.PCG64(700 + rounds + 10 * ec2))
+    s = np.concatenate([np.tile(ints_to_limbs([0x1f2e3d4c5b6a79881726354]), (88, 1)),
+                        random_field(rng, 8 + len(rest), 1)])
+    s[100:104] = 0
+    ctx.set_msm_affine_rounds(rounds)
+    try:
+        got = fixed_msm(ctx, s, p, 8, ec2)
+        # everything cancels: equal numbers of P and -P under one scalar
+        k = np.tile(ints_to_limbs([0xabcdef]), (80, 1))
+        none = fixed_msm(ctx, k, np.stack([P] * 40 + [_neg(P, ec2)] * 40), 8, ec2)
+    finally:
+        ctx.set_msm_affine_rounds(-1)
+    assert np.array_equal(got, oracle.msm(s, p, ec2=1 if ec2 else 0))
+    assert np.array_equal(none, inf)

@@ -8,7 +8,7 @@ outputs of the reference library itself captured in tests/golden/ref_transforms.
 import numpy as np
 import pytest
 
-from oracle.oracle import random_field, hstep_roots_table, limbs_to_int, R, Q
+from oracle.oracle import random_field, hstep_roots_table, limbs_to_int, ints_to_limbs, R, Q
 
 
 def test_field_known_answers(oracle, golden):
@@ -126,3 +126,17 @@ def test_random_against_reference_library(oracle, reflib):
     table = hstep_roots_table(oracle, L)
     assert np.array_equal(oracle.interpolandmul(A, B, oracle.find_roots(L + 1), L, 2),
                           reflib.interpolandmul(A, B, table, L, 2))
+
+
+def test_reference_msm_small_scalars(oracle, reflib):
+    """The reference library as built here (LZCNT, like the reference's own -march=native
+    build) equals the restatement on multi-exponentiations whose last scalars are small --
+    the extension scalars [1, r] of a proof -- which a build where __builtin_clz(0) is not 32
+    gets wrong (src/cuda/bigint.cpp:216 msbu256_h)."""
+    from oracle.synth_cpu import fixed_base_mul
+    rng = np.random.Generator(np.random.PCG64(77))
+    for n, tail in ((128, [1, 5]), (127, [3, 3]), (2000, [1, 0x1234567890abcdef])):
+        s = random_field(rng, n, 1)
+        s[n - len(tail):] = ints_to_limbs(tail)
+        p = fixed_base_mul(oracle, random_field(rng, n, 1))
+        assert np.array_equal(reflib.msm(s, p, 0, 6), oracle.msm(s, p)), n

@@ -84,3 +84,58 @@ def test_cpu_prover_proof_verifies(oracle):
 def test_cpu_prover_reference_library_identical(oracle, reflib):
     pk, vk, w = _tiny_groth(oracle, L=5, seed=9)
     assert np.array_equal(cpu_prove(oracle, pk, w, 777, 888), cpu_prove(oracle, pk, w, 777, 888, ref=reflib))
+
+
+def test_cpu_builder_key_matches_integer_setup(oracle):
+    """oracle/synth_cpu.py (the builder bench.py's reference arm uses) against Groth16 setup
+    restated with Python integers and the oracle's double-and-add scalar multiplication, on
+    the benchmark circuit family at m = 2^5; its witness satisfies every constraint and its
+    proof, from the staged CPU sequence, verifies."""
+    from oracle.oracle import from_mont_int
+    from oracle.prover import cpu_prove_stages
+    from oracle.synth_cpu import CpuCircuit, cpu_setup_pk
+    from cusnarks_b200.groth import toxic_waste
+    L = 5
+    c = CpuCircuit(oracle, L, seed=21, n_public=2)
+    m, nv, nc = c.m, c.n_vars, c.n_constraints
+    w = [limbs_to_int(x) for x in c.w]
+    mi = pow(1 << 256, -1, R)
+    coef = lambda x: limbs_to_int(x) * mi % R  # noqa: E731
+    for k in range(nc):
+        a = sum(coef(c.a_coeff[k, j]) * w[c.a_wire[k, j]] for j in range(3)) % R
+        b = sum(coef(c.b_coeff[k, j]) * w[c.b_wire[k, j]] for j in range(3)) % R
+        assert a * b % R == w[c.n_inputs + k]
+    pk = cpu_setup_pk(oracle, c, seed=22)
+    t, al, be, ga, de = toxic_waste(22)
+    omega = from_mont_int(limbs_to_int(oracle.find_roots(L)[1]), 1)
+    Lc = [pow(omega, i, R) * (pow(t, m, R) - 1) * pow(m * (t - pow(omega, i, R)), -1, R) % R for i in range(m)]
+
+    def wire_eval(pol):
+        out, off = [0] * nv, 1 + nv
+        for i in range(nv):
+            cnt = int(pol[1 + i])
+            for j in range(cnt):
+                row = int(pol[off + j])
+                out[i] = (out[i] + coef(pol[off + cnt + 8 * j:off + cnt + 8 * j + 8]) * Lc[row]) % R
+            off += 9 * cnt
+        return out
+
+    u, v, ww = (wire_eval(p) for p in (c.polsA, c.polsB, c.polsC))
+    g1 = g1_generator_mont().reshape(1, -1)
+    g2 = g2_generator_mont().reshape(1, -1)
+    m1 = lambda ks: oracle.scmul(ints_to_limbs(ks), g1, 0)  # noqa: E731
+    m2 = lambda ks: oracle.scmul(ints_to_limbs(ks), g2, 1)  # noqa: E731
+    dinv = pow(de, -1, R)
+    assert np.array_equal(pk["A"], np.concatenate([m1(u), m1([al, de])]))
+    assert np.array_equal(pk["B1"], np.concatenate([m1(v), m1([be, de])]))
+    assert np.array_equal(pk["B2"], np.concatenate([m2(v), m2([be, de])]))
+    assert np.array_equal(pk["C"], m1([(be * u[i] + al * v[i] + ww[i]) * dinv % R for i in range(nv)]))
+    assert np.array_equal(pk["hExps"], m1([pow(t, j, R) * (pow(t, m, R) - 1) * dinv % R for j in range(m - 1)]))
+    ginv = pow(ga, -1, R)
+    assert np.array_equal(pk["vk"]["IC"], m1([(be * u[i] + al * v[i] + ww[i]) * ginv % R for i in range(3)]))
+    stages, st = cpu_prove_stages(oracle, pk, c.w, 4242, 2424)
+    assert [n for n, _ in stages] == ["qap", "hstep", "msm_A", "msm_B2", "msm_B1", "msm_C", "msm_H+combine"]
+    for _, fn in stages:
+        fn()
+    assert np.array_equal(st["proof"], cpu_prove(oracle, pk, c.w, 4242, 2424))
+    assert verify(pk["vk"], st["proof"], c.public_inputs)

@@ -4,7 +4,8 @@ It exists for callers that may not call cudaMalloc (their device memory belongs 
 host framework's pool, or the allocation's implicit synchronisation is not acceptable on
 their path).  Its scratch is a fixed device array shared by all calls, so this test
 checks two consecutive calls against the regular entry point, word for word, and that a
-size beyond the array is refused with an error instead of running.  The file sorts last
+size beyond the array is refused with an error instead of running; the smaller call is
+also checked against the oracle's multi-exponentiation.  The file sorts last
 so that a run stopping at the first failure has already run every other test.
 """
 import ctypes
@@ -28,7 +29,7 @@ def _points(ctx, rng, n):
     return p
 
 
-def test_noalloc_matches_allocating_entry_point_twice():
+def test_noalloc_matches_allocating_entry_point_twice(oracle):
     import torch
     from cusnarks_b200 import Context, lib
     L = lib()
@@ -53,6 +54,10 @@ def test_noalloc_matches_allocating_entry_point_twice():
         torch.cuda.synchronize()
         results.append(got.cpu().numpy())
         assert np.array_equal(got.cpu().numpy(), want.cpu().numpy()), n
+        if n <= 3000:  # and the oracle's multi-exp (the reference's ec_jacreduce_server_h restated)
+            host = got.cpu().numpy().view(np.uint32)
+            assert np.array_equal(host, oracle.msm(s.cpu().numpy().view(np.uint32),
+                                                   pts.cpu().numpy().view(np.uint32))), n
     assert not np.array_equal(results[0], results[1])
     ctx.close()
 
