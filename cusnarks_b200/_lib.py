@@ -208,6 +208,13 @@ _SIGNATURES = [
     ("readWitnessFile_h", None, [_vp, ctypes.c_char_p, ctypes.c_uint32, ctypes.c_ulonglong]),
     ("writeWitnessFile_h", None, [_vp, ctypes.c_char_p, ctypes.c_ulonglong]),
     ("ec2_jacreduce_server_h", None, [ctypes.POINTER(JacaddReduced)]),
+    ("shared_new_h", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_ulonglong]),
+    ("shared_free_h", None, [_vp, ctypes.c_int]),
+    ("readR1CSFileHeader_h", None, [_vp, ctypes.c_char_p]),
+    ("readR1CSFile_h", None, [_vp, ctypes.c_char_p, _vp, ctypes.c_int]),
+    ("r1cs_to_mpoly_len_h", None, [_vp, _vp, _vp, ctypes.c_uint32]),
+    ("r1cs_to_mpoly_h", None, [_vp, _vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    ("readECTablesNElementsFile_h", None, [_vp, ctypes.c_char_p]),
 ]
 
 _lock = threading.Lock()

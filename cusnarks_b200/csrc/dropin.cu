@@ -11,6 +11,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <sys/ipc.h>
+#include <sys/shm.h>
 #include <string>
 #include <thread>
 #include <vector>
@@ -498,6 +500,43 @@ void writeWitnessFile_h(uint32_t* samples, const char* filename, unsigned long l
   std::fwrite(&wmore, 4, 1, f);
   std::fwrite(samples, 32, nwords, f);
   std::fclose(f);
+}
+
+// System V shared memory for the witness, as the reference's processes share it
+// (utils_host.cpp:156 / :180: key 123456, created if absent, mode 0666).
+int shared_new_h(void** shmem, unsigned long long size) {
+  if (!shmem) return -1;
+  const int shmid = shmget((key_t)123456, (size_t)size, IPC_CREAT | 0666);
+  if (shmid < 0) return -1;
+  void* p = shmat(shmid, nullptr, 0);
+  if (p == (void*)-1) return -1;
+  *shmem = p;
+  return shmid;
+}
+
+void shared_free_h(void* shmem, int shmid) {
+  if (shmem) shmdt(shmem);
+  shmctl(shmid, IPC_RMID, nullptr);
+}
+
+// Circuit compilation and EC table files: bound by the reference's Cython layer, not on this
+// library's path.  Outputs are zeroed; the status says why.
+void readR1CSFileHeader_h(r1csv1_t* r1cs_hdr, const char* filename) {
+  if (r1cs_hdr) memset(r1cs_hdr, 0, sizeof(*r1cs_hdr));
+  dropin_status(CS_ERR_UNSUPPORTED, "readR1CSFileHeader_h: R1CS files are compiled before proving (not on this path)");
+}
+void readR1CSFile_h(uint32_t*, const char*, r1csv1_t*, r1cs_idx_t) {
+  dropin_status(CS_ERR_UNSUPPORTED, "readR1CSFile_h: R1CS files are compiled before proving (not on this path)");
+}
+void r1cs_to_mpoly_len_h(uint32_t*, uint32_t*, cirbin_hfile_t*, uint32_t) {
+  dropin_status(CS_ERR_UNSUPPORTED, "r1cs_to_mpoly_len_h: circuit compilation is not on this path");
+}
+void r1cs_to_mpoly_h(uint32_t*, uint32_t*, cirbin_hfile_t*, uint32_t, uint32_t, uint32_t) {
+  dropin_status(CS_ERR_UNSUPPORTED, "r1cs_to_mpoly_h: circuit compilation is not on this path");
+}
+void readECTablesNElementsFile_h(ec_table_offset_t* t, const char*) {
+  if (t) memset(t, 0, sizeof(*t));
+  dropin_status(CS_ERR_UNSUPPORTED, "readECTablesNElementsFile_h: precomputed EC table files are not supported");
 }
 
 }  // extern "C"

@@ -40,6 +40,11 @@ extern "C" {
 #define CS_ERR_CANCELLED 7   /* the request was cancelled before it ran */
 
 /* ------------------------------------------- reference argument structs (layouts) --- */
+/* The structs and enums below repeat the reference's src/cuda/types.h layouts.  A
+ * translation unit that includes the reference's own types.h as well (the reference's
+ * Cython module built against this library) defines CS_REFERENCE_TYPES first, and the
+ * declarations then use the reference's definitions. */
+#ifndef CS_REFERENCE_TYPES
 /* jacadd_reduced_t, reference src/cuda/types.h:548-567 (same member order and types). */
 typedef struct {
   uint32_t *out_ep;
@@ -91,6 +96,7 @@ typedef struct {
   uint32_t thread_id;
   uint32_t pidx;
 } mpoly_eval_t;
+#endif /* CS_REFERENCE_TYPES */
 
 /* ------------------------------------------------ drop-in reference entry points --- */
 /* Replaces ec_jacreduce_server_h, reference src/cuda/ec.cpp:1536 (bound at
@@ -147,8 +153,10 @@ uint32_t *get_Mtranspose_h(void);
  * (mNrows, mNcols) = (Nrows+1, Ncols) if Nrows < Ncols else (Nrows, Ncols+1)
  * (ntt.cpp:767).  Valid until the next H-step call; NULL before the first. */
 uint32_t *get_Mmul_h(void);
+#ifndef CS_REFERENCE_TYPES
 /* fft_mode_t, reference src/cuda/types.h:235 */
 typedef enum { FFT_T_DIT = 0, FFT_T_DIF, FFT_T_MODE_N } fft_mode_t;
+#endif
 /* Replaces ntt_parallel_h, reference src/cuda/ntt.cpp:274 (_utils_host.pxd:78): the reference
  * computes the 2^(Nrows+Ncols)-point transform by four steps (column transforms, twiddles,
  * row transforms, transpose); its result is the natural-order transform of ntt_h with
@@ -357,6 +365,7 @@ void ec2_isinf(uint32_t *z, const uint32_t *x, const uint32_t n, const uint32_t 
 /* bigint.cpp:72 -- indices 0..len-1, sorted (std::sort) by the top word of v[i] if sort_en. */
 void sortu256_idx_h(uint32_t *idx, const uint32_t *v, uint32_t len, uint32_t sort_en);
 /* ntt.cpp:1116 -- transform decomposition of nsamples (types.h fft_params_t layout). */
+#ifndef CS_REFERENCE_TYPES
 typedef enum { FFT_T_1D = 0, FFT_T_2D, FFT_T_3D, FFT_T_4D, FFT_T_N } fft_t;
 typedef struct {
   fft_t fft_type;
@@ -364,6 +373,7 @@ typedef struct {
   uint32_t padding;
   uint32_t levels;
 } fft_params_t;
+#endif
 void ntt_build_h(fft_params_t *ntt_params, uint32_t nsamples);
 /* init.cpp:44 / :54 (no roots files are read: twiddles are made on the device), and
  * utils_host get_nprocs_h. */
@@ -377,6 +387,7 @@ void readU256PKFile_h(uint32_t *samples, const char *filename, unsigned long lon
 /* types.h cirbin_hfile_t / pkbin_hfile_t and file_utils.cpp:49 / :447: the leading header
  * words of a circuit file (9 x uint64) and of a proving-key file (9 x uint32, read in order,
  * so domainSize receives the file's domainBits word, as in the reference). */
+#ifndef CS_REFERENCE_TYPES
 typedef struct {
   unsigned long long nWords, nPubInputs, nOutputs, nVars, nConstraints, cirformat, R1CSA_nWords,
       R1CSB_nWords, R1CSC_nWords;
@@ -384,6 +395,7 @@ typedef struct {
 typedef struct {
   uint32_t nWords, ftype, protocol, Rbitlen, k_binformat, k_ecformat, nVars, nPublic, domainSize;
 } pkbin_hfile_t;
+#endif
 void readU256CircuitFileHeader_h(cirbin_hfile_t *hfile, const char *filename);
 void readU256PKFileHeader_h(pkbin_hfile_t *hfile, const char *filename);
 void readU256DataFile_h(uint32_t *samples, const char *filename, uint32_t insize, uint32_t outsize);
@@ -393,6 +405,39 @@ void writeU256DataFile_h(uint32_t *samples, const char *filename, unsigned long 
 void appendU256DataFile_h(uint32_t *samples, const char *filename, unsigned long long nwords);
 void readWitnessFile_h(uint32_t *samples, const char *filename, uint32_t fmt, unsigned long long inlen);
 void writeWitnessFile_h(uint32_t *samples, const char *filename, unsigned long long nwords);
+
+/* The rest of what the reference's Cython layer binds (src/cython/_utils_host.pxd), exported
+ * so that its module links against this library unchanged.
+ *   shared_new_h / shared_free_h (utils_host.cpp:156 / :180): the System V shared-memory
+ *     witness buffer (key 123456) the reference's processes exchange; same behaviour.
+ *   readR1CSFileHeader_h / readR1CSFile_h (file_utils.cpp), r1cs_to_mpoly_len_h /
+ *     r1cs_to_mpoly_h (mpoly.cpp:201): circuit compilation, before proving -- not on this
+ *     library's path (it reads compiled proving keys); they zero their outputs and report
+ *     CS_ERR_UNSUPPORTED in cs_last_status().
+ *   readECTablesNElementsFile_h: precomputed EC table files, refused like the table-file
+ *     option of ec_jacreduce_server_h (CS_ERR_UNSUPPORTED). */
+#ifndef CS_REFERENCE_TYPES
+/* r1csv1_t, r1cs_idx_t, ec_table_offset_t: reference src/cuda/types.h:581-626 */
+typedef struct {
+  uint32_t magic_number, version, nsections, word_width_bytes, nVars, nPubOutputs, nPubInputs, nPrivInputs;
+  unsigned long long nLabels;
+  uint32_t nConstraints, R1CSA_nCoeff, R1CSB_nCoeff, R1CSC_nCoeff, constraintOffset;
+  long long constraintLen;
+} r1csv1_t;
+typedef enum { R1CSA_IDX = 0, R1CSB_IDX = 1, R1CSC_IDX = 2, R1CS_N_IDX = 3 } r1cs_idx_t;
+typedef struct {
+  uint32_t table_order;
+  unsigned long long woffset_A, woffset_B2, woffset_B1, woffset_C, woffset_hExps, nwords_tdata;
+} ec_table_offset_t;
+#endif
+int shared_new_h(void **shmem, unsigned long long size);
+void shared_free_h(void *shmem, int shmid);
+void readR1CSFileHeader_h(r1csv1_t *r1cs_hdr, const char *filename);
+void readR1CSFile_h(uint32_t *samples, const char *filename, r1csv1_t *r1cs, r1cs_idx_t r1cs_idx);
+void r1cs_to_mpoly_len_h(uint32_t *plen_out, uint32_t *cin, cirbin_hfile_t *header, uint32_t extend);
+void r1cs_to_mpoly_h(uint32_t *pout, uint32_t *cin, cirbin_hfile_t *header, uint32_t to_mont, uint32_t pidx,
+                     uint32_t extend);
+void readECTablesNElementsFile_h(ec_table_offset_t *table_offset, const char *filename);
 
 /* G1 multi-exponentiation that allocates nothing (no counterpart in the reference).
  * For callers whose device memory is owned by a host framework's pool and who may not

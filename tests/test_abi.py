@@ -57,3 +57,27 @@ def test_server_refuses_without_device():
     h = ctypes.c_void_p()
     assert lib().cs_server_create(0, 2, 0, ctypes.byref(h)) == CS_ERR_NODEVICE
     assert not h.value
+
+
+def test_reference_cython_module_links_this_library():
+    """Where it was built (the reference tree present at build time), the reference's own
+    Cython module loads against this library on a machine without a GPU: every symbol it
+    binds resolves to libcusnarks_b200.so."""
+    import importlib
+    import subprocess
+    import sys
+    from cusnarks_b200 import refcython
+    path = refcython.module_path()
+    if path is None:
+        pytest.skip("pycusnarks not built here (no reference tree at build time)")
+    need = subprocess.run(["ldd", path], capture_output=True, text=True).stdout
+    assert os.path.join("cusnarks_b200", "libcusnarks_b200.so") in need
+    assert "not found" not in need
+    d = os.path.dirname(path)
+    sys.path.insert(0, d)
+    try:
+        mod = importlib.import_module("pycusnarks")
+    finally:
+        sys.path.remove(d)
+    for name in ("ec_jacreduce_h", "ntt_h", "intt_h", "ntt_interpolandmul_h", "mpoly_eval_h"):
+        assert callable(getattr(mod, name))
