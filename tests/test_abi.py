@@ -71,8 +71,11 @@ def test_reference_cython_module_links_this_library():
     if path is None:
         pytest.skip("pycusnarks not built here (no reference tree at build time)")
     need = subprocess.run(["ldd", path], capture_output=True, text=True).stdout
-    assert os.path.join("cusnarks_b200", "libcusnarks_b200.so") in need
     assert "not found" not in need
+    lines = [ln for ln in need.splitlines() if "libcusnarks_b200.so =>" in ln]
+    assert len(lines) == 1
+    resolved = lines[0].split("=>")[1].split("(")[0].strip()
+    assert os.path.realpath(resolved) == os.path.join(ROOT, "cusnarks_b200", "libcusnarks_b200.so")
     d = os.path.dirname(path)
     sys.path.insert(0, d)
     try:
