@@ -24,9 +24,9 @@ memory, proof back in host memory, K requests submitted at once, wall clock.
 that saturated rate.  ``single_proof``: one proof per call (cs_prove_device), device time.
 ``plain_per_call``: the reference's flow through the drop-in entry points (mpoly_eval_server_h,
 ntt_interpolandmul_server_h, ec_jacreduce_server_h per MSM with the key points copied per
-call), wall clock; ``served_vs_plain`` = e2e / plain.  ``served_mix``: 8 circuits of
-2^12..2^20 constraints (log-uniform, seeded), requests uniform over them, saturation and
-Poisson 50% / 90% with p50/p99.  ``batched_msm``: 64 G1 + 8 G2 MSMs of 2^floor(U(10,20))
+call), wall clock; ``served_vs_plain`` = e2e / plain.  ``served_mix``: 8 circuits spanning
+2^12..2^20 constraints (both ends and six seeded log-uniform sizes; the 2^20 one is the
+headline circuit), requests uniform over them, saturation and Poisson 50% / 90% with p50/p99.  ``batched_msm``: 64 G1 + 8 G2 MSMs of 2^floor(U(10,20))
 terms in one batch plan per group (autotuned windows, CUDA graph replay) vs one call per
 instance.  Also one BN128 G1 MSM of 2^20 terms (``g1_msm_2^20_ms``),
 whose bucket-accumulation kernel -- the dominant kernel of every proof -- carries the roofline.
@@ -371,19 +371,25 @@ def served_run(srv, jobs, rate_hz=None, seed=0, proofs=None):
     return time.perf_counter() - t0, lat
 
 
-def served_mix(ctx, slots: int, n_requests: int, seed: int = 5):
-    """Config 5: 8 circuits of 2^12..2^20 constraints (log-uniform, seeded), keys resident,
-    requests over them (uniform) at Poisson rates 50% / 90% of the measured saturation."""
+def served_mix(ctx, slots: int, n_requests: int, seed: int = 5, big=None):
+    """Config 5: 8 circuits spanning 2^12..2^20 constraints (the two ends plus six seeded
+    log-uniform draws), keys resident, requests over them (uniform) at Poisson rates 50% /
+    90% of the measured saturation.  big: (circuit, prover) of a 2^20 circuit to reuse."""
     from cusnarks_b200.groth import SyntheticCircuit, setup_pk, Prover
     from cusnarks_b200.server import ProveServer
     from cusnarks_b200.synth import to_limbs
     rng = np.random.Generator(np.random.PCG64(seed))
-    logs = sorted(int(x) for x in rng.integers(12, 21, 8))
-    circs, provers = [], []
+    logs = sorted([12, 20] + [int(x) for x in rng.integers(12, 21, 6)])
+    circs, provers, owned = [], [], []
     for i, lm in enumerate(logs):
+        if lm == 20 and big is not None and big[0] not in circs:
+            circs.append(big[0])
+            provers.append(big[1])
+            continue
         c = SyntheticCircuit(ctx, lm, seed=300 + i)
         circs.append(c)
         provers.append(Prover(ctx, setup_pk(ctx, c, seed=400 + i)))
+        owned.append(provers[-1])
     srv = ProveServer(ctx.device, slots=slots, reserve_bytes=1 << 30)
     keys = [srv.add_key(p) for p in provers]
     r, s = to_limbs(0x1234567890abcdef), to_limbs(0xfedcba0987654321)
@@ -402,7 +408,7 @@ def served_mix(ctx, slots: int, n_requests: int, seed: int = 5):
                                                 "p50_ms": round(pct(lat, 50), 2), "p99_ms": round(pct(lat, 99), 2)}
     out["max_concurrent"] = srv.stats()["max_concurrent"]
     srv.close()
-    for p in provers:
+    for p in owned:
         p.close()
     return out
 
@@ -607,7 +613,7 @@ def run_ours(args, world, rank, local):
     if rank == 0 and not args.no_batch:
         line["batched_msm"] = batched_msm(ctx, reps=3)
     if rank == 0 and not args.no_mix:
-        line["served_mix"] = served_mix(ctx, args.slots, args.mix_requests)
+        line["served_mix"] = served_mix(ctx, args.slots, args.mix_requests, big=(wl.circ, wl.prover))
     if rank == 0 and world == 1 and not args.no_cpu:
         from cusnarks_b200.groth import pk_to_host
         from oracle.prover import verify

@@ -308,6 +308,15 @@ ProvePlan plan_prove(const cs_pk* pk) {
 namespace csb {
 size_t prove_workspace_bytes(const cs_pk* pk) { return plan_prove(pk).total; }
 uint32_t pk_n_vars(const cs_pk* pk) { return pk->n_vars; }
+// Grows the context's arenas to what a proof with this key needs (cs_prove would grow them
+// on its first call): lets the server allocate a slot's scratch right after admission.
+cudaError_t prove_reserve(cs_ctx* ctx, const cs_pk* pk) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaError_t e = ctx->work.reserve(plan_prove(pk).total, ctx->stream);
+  if (e == cudaSuccess) e = ctx->in.reserve((size_t)pk->n_vars * 32 + 512, ctx->stream);
+  return e;
+}
 }  // namespace csb
 
 extern "C" {

@@ -7,8 +7,10 @@
 //     NTT twiddles stay resident in each slot's context;
 //   * requests queue FIFO; each of `slots` worker threads owns a context (its own streams
 //     and scratch arena) and takes the next request as soon as it is free AND the request
-//     is admitted by device memory: free memory (cudaMemGetInfo) minus the bytes already
-//     promised to admitted requests must cover the slot's scratch growth plus `reserve`;
+//     is admitted by device memory: free memory (cudaMemGetInfo) minus the bytes promised
+//     to admitted requests whose slots have not grown yet must cover the slot's scratch
+//     growth plus `reserve`; an admitted slot grows its arenas at once and then withdraws
+//     its promise, since cudaMemGetInfo counts the memory from then on;
 //   * admitted proofs run concurrently on the device: one proof's MSM tails, QAP and
 //     H step overlap the next one's bucket accumulation.
 // Results do not depend on the mix: every proof is computed by the same kernels on its
@@ -32,6 +34,7 @@
 namespace csb {
 size_t prove_workspace_bytes(const cs_pk* pk);
 uint32_t pk_n_vars(const cs_pk* pk);
+cudaError_t prove_reserve(cs_ctx* ctx, const cs_pk* pk);
 }  // namespace csb
 
 namespace {
@@ -152,10 +155,25 @@ void cs_server::worker(int slot) {
     const size_t wbytes = (size_t)csb::pk_n_vars(pk) * 32;
     int st = CS_OK;
     std::string msg;
-    if (stage.reserve(wbytes) != cudaSuccess) {
+    if (need) {  // grow the slot's scratch now; from here on free memory accounts for it
+      const cudaError_t ge = csb::prove_reserve(ctx, pk);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        promised = promised > need ? promised - need : 0;
+        need = 0;
+      }
+      cv_work.notify_all();
+      if (ge != cudaSuccess) {
+        cudaGetLastError();
+        st = CS_ERR_NOMEM;
+        msg = "server: slot scratch allocation failed";
+      }
+    }
+    if (st == CS_OK && stage.reserve(wbytes) != cudaSuccess) {
       st = CS_ERR_NOMEM;
       msg = "server: pinned staging buffer";
-    } else {
+    }
+    if (st == CS_OK) {
       std::memcpy(stage.ptr, rq->w, wbytes);
       st = cs_prove(ctx, pk, static_cast<const uint32_t*>(stage.ptr), rq->r, rq->s, rq->proof);
       if (st != CS_OK) msg = cs_ctx_error(ctx);
@@ -163,7 +181,6 @@ void cs_server::worker(int slot) {
     const float dev_ms = cs_ctx_last_ms(ctx);
     {
       std::lock_guard<std::mutex> lk(mu);
-      promised = promised > need ? promised - need : 0;
       busy--;
       rq->status = st;
       rq->err = msg;
