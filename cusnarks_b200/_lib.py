@@ -102,6 +102,7 @@ _SIGNATURES = [
     ("cs_msm_num_windows", ctypes.c_int, [ctypes.c_int]),
     ("cs_ctx_set_msm_affine_rounds", ctypes.c_int, [_vp, ctypes.c_int]),
     ("cs_ctx_prove_stages", ctypes.c_int, [_vp, _vp, ctypes.c_int]),
+    ("cs_ctx_set_prove_graphs", ctypes.c_int, [_vp, ctypes.c_int]),
     ("cs_msm_fixed_window", ctypes.c_int, [ctypes.c_uint32, ctypes.c_int]),
     ("cs_msm_fixed_table_points", ctypes.c_size_t, [ctypes.c_uint32, ctypes.c_int]),
     ("cs_msm_fixed_workspace_bytes", ctypes.c_size_t, [ctypes.c_uint32, ctypes.c_int, ctypes.c_int]),

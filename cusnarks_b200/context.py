@@ -54,6 +54,10 @@ class Context:
     def sync(self):
         check(self._lib.cs_ctx_sync(self.handle), self.handle)
 
+    def set_prove_graphs(self, enable: bool):
+        """Capture and replay each key's proof launch sequence as a CUDA graph (default on)."""
+        check(self._lib.cs_ctx_set_prove_graphs(self.handle, int(bool(enable))), self.handle)
+
     def set_msm_affine_rounds(self, rounds: int):
         """Batch-affine halving rounds before the XYZZ bucket accumulation (-1 auto, 0 off)."""
         check(self._lib.cs_ctx_set_msm_affine_rounds(self.handle, rounds), self.handle)

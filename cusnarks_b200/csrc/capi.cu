@@ -13,7 +13,12 @@ namespace csb {
 
 void domain_release(cs_ctx* ctx);  // hstep.cu
 static std::atomic<unsigned long long> g_launches{0};
-void note_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+thread_local unsigned long long t_launches = 0;
+void note_launch(unsigned n) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+  t_launches += n;
+}
+unsigned long long thread_launches() { return t_launches; }
 
 #ifndef CSB_PRIO_MODE
 #define CSB_PRIO_MODE 2  // G2 MSM and the QAP/H chain first (measured 32.0 -> 31.6 ms per 2^20 proof)
@@ -173,6 +178,7 @@ int cs_ctx_create(int device, cs_ctx** out) {
 void cs_ctx_destroy(cs_ctx* ctx) {
   if (!ctx) return;
   cudaStreamSynchronize(ctx->stream);
+  csb::prove_graphs_release(ctx);
   csb::domain_release(ctx);
   ctx->work.release();
   ctx->in.release();
@@ -188,6 +194,18 @@ void cs_ctx_destroy(cs_ctx* ctx) {
   for (int i = 0; i < 8; i++)
     if (ctx->aux_ev[i]) cudaEventDestroy(ctx->aux_ev[i]);
   delete ctx;
+}
+
+int cs_ctx_set_prove_graphs(cs_ctx* ctx, int enable) {
+  if (!ctx) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  ctx->use_prove_graphs = enable != 0;
+  if (!enable) {
+    cudaStreamSynchronize(ctx->stream);
+    csb::prove_graphs_release(ctx);
+  }
+  return CS_OK;
 }
 
 int cs_ctx_set_stream(cs_ctx* ctx, void* stream) {
@@ -230,6 +248,9 @@ int cs_ctx_prove_stages(cs_ctx* ctx, float* ms, int n) {
   if (!ctx || !ms || n < 1) return CS_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
   if (!ctx->aux_ready) return CS_ERR_ARG;
+  if (!ctx->stages_valid)
+    return csb::fail_msg(ctx, CS_ERR_UNSUPPORTED,
+                         "stage times: the last proof was a graph replay (cs_ctx_set_prove_graphs(ctx, 0) times stages)");
   // completion of: A, B1, B2, C MSM chains, the H step, the H MSM, the whole proof
   cudaEvent_t evs[7] = {ctx->aux_ev[1], ctx->aux_ev[2], ctx->aux_ev[3], ctx->aux_ev[4], ctx->aux_ev[6],
                         ctx->aux_ev[5], ctx->ev_stop};

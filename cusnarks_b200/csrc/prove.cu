@@ -16,6 +16,7 @@
 // of one window for C and H, the C MSM accumulates its buckets early (beside the H step) and
 // hands them to the H MSM, which adds them to its own before its reduction: pi_C + pi_C2 from
 // one bucket reduction instead of two (the same group element, so the same affine proof).
+#include <atomic>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -44,6 +45,7 @@ const uint32_t* domain_consts(const Domain* d);
 using namespace csb;
 
 struct cs_pk {
+  uint64_t id = 0;  // unique per key and per fixed-base table build: names the key in graph caches
   int device = 0;
   uint32_t n_vars = 0, n_public = 0, m = 0, log_m = 0;
   QapRows rows_a, rows_b;
@@ -84,6 +86,8 @@ struct cs_pk {
 };
 
 namespace {
+
+std::atomic<uint64_t> g_pk_ids{1};
 
 inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -303,9 +307,152 @@ ProvePlan plan_prove(const cs_pk* pk) {
   return P;
 }
 
+// The proof's launch sequence after the scalar uploads (which cs_prove_device makes): the
+// witness scalars with their extensions, the four witness MSMs on the auxiliary streams with
+// the GLV scalings, QAP -> H step -> H MSM on the H stream, the join and the final pi_C.
+// Results land in the scratch's point area.  Sets *where on failure.
+cudaError_t prove_body(cs_ctx* ctx, cs_pk* pk, const ProvePlan& P, const uint32_t* d_w, Domain* dom1,
+                       Domain* dom2, const char** where) {
+  char* base = static_cast<char*>(ctx->work.ptr);
+  auto at = [&](size_t off) { return reinterpret_cast<uint32_t*>(base + off); };
+  uint32_t *wA = at(P.wA), *wB = at(P.wB), *pA = at(P.pA), *pB = at(P.pB), *M = at(P.M), *hscr = at(P.hscr);
+  uint32_t* pts = at(P.pts);
+  uint32_t *outA = pts, *outB1 = pts + 16, *outB2 = pts + 32, *outC = pts + 64, *outH = pts + 80;
+  uint32_t *sA = pts + 96, *rB1 = pts + 128, *piC = pts + 160;
+  uint32_t* rs = at(P.rs);
+  const uint32_t nv = pk->n_vars, m = pk->m, np1 = pk->n_public + 1;
+  cudaStream_t s0 = ctx->stream;
+  cudaEvent_t ev_w = ctx->aux_ev[0];
+  MsmConfig cfg;
+  cudaError_t e;
+  // scalars: w ++ [1, r] and w ++ [1, s]; -rs
+  bool ok = (e = cudaMemcpyAsync(wA, d_w, (size_t)nv * 32, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess &&
+            (e = cudaMemcpyAsync(wB, d_w, (size_t)nv * 32, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess;
+  if (!ok) { *where = "prove inputs"; return e; }
+  k_set_tail<<<1, 32, 0, s0>>>(wA, nv, rs);
+  k_set_tail<<<1, 32, 0, s0>>>(wB, nv, rs + 8);
+  k_neg_rs<<<1, 32, 0, s0>>>(rs, rs + 8, rs + 16);
+  note_launch(3);
+  cudaEventRecord(ev_w, s0);
+  // witness MSMs on the auxiliary streams
+  cudaStream_t sa = ctx->aux[0], sb1 = ctx->aux[1], sb2 = ctx->aux[2], sc = ctx->aux[3];
+  for (int i = 0; i < 4; i++) cudaStreamWaitEvent(ctx->aux[i], ev_w, 0);
+  // resident fixed-base tables when the key has them, else the generic MSM over the points
+  auto run_msm = [&](bool ec2, const uint32_t* sc, const uint32_t* pts, const cs_pk::Fixed& f, uint32_t n,
+                     uint32_t* out, size_t off, size_t bytes, cudaStream_t st, const MsmConfig* share = nullptr) {
+    if (pk->has_fixed()) {
+      MsmConfig fcfg = share ? *share : MsmConfig{};
+      fcfg.c = f.c;
+      return ec2 ? msm_fixed_g2(sc, f.table, n, out, at(off), bytes, fcfg, st)
+                 : msm_fixed_g1(sc, f.table, n, out, at(off), bytes, fcfg, st);
+    }
+    return ec2 ? msm_g2(sc, pts, n, out, at(off), bytes, cfg, st) : msm_g1(sc, pts, n, out, at(off), bytes, cfg, st);
+  };
+  // C hands its buckets to H (outC is then the point at infinity, and outH the sum of both)
+  MsmConfig share_c, share_h;
+  if (P.share_ch) {
+    share_c.bucket_out = at(P.cbk);
+    share_h.bucket_add = at(P.cbk);
+    share_h.bucket_ready = ctx->aux_ev[7];
+  }
+  ok = (e = run_msm(false, wA, pk->a_ext, pk->fa, nv + 2, outA, P.ms_a, P.bytes_a, sa)) == cudaSuccess &&
+       (e = run_msm(false, wB, pk->b1_ext, pk->fb1, nv + 2, outB1, P.ms_b1, P.bytes_b1, sb1)) == cudaSuccess &&
+       (e = run_msm(true, wB, pk->b2_ext, pk->fb2, nv + 2, outB2, P.ms_b2, P.bytes_b2, sb2)) == cudaSuccess &&
+       (e = run_msm(false, wA + (size_t)np1 * 8, pk->c + (size_t)np1 * 16, pk->fc, nv - np1, outC, P.ms_c, P.bytes_c,
+                    sc, &share_c)) == cudaSuccess;
+  if (!ok) { *where = "prove witness MSMs"; return e; }
+  if (P.share_ch && (e = cudaEventRecord(ctx->aux_ev[7], sc)) != cudaSuccess) { *where = "prove C buckets"; return e; }
+  {
+    const GlvSplit* gsp = reinterpret_cast<const GlvSplit*>(rs + 32);
+    k_scale_point_glv<<<1, 32, 0, sa>>>(outA, gsp, sA);        // s * pi_A
+    k_scale_point_glv<<<1, 32, 0, sb1>>>(outB1, gsp + 1, rB1);  // r * pi_B1
+  }
+  note_launch(2);
+  // QAP evaluation, H step and H MSM on their own stream
+  cudaStream_t sh = ctx->aux_h;
+  cudaStreamWaitEvent(sh, ev_w, 0);
+  ok = (e = qap_eval(pk->rows_a, d_w, pA, 0, sh)) == cudaSuccess &&
+       (e = qap_eval(pk->rows_b, d_w, pB, 0, sh)) == cudaSuccess &&
+       (e = hstep_reference_core(pA, pB, pk->log_m, domain_wf(dom2), domain_wi(dom2), domain_wf(dom2),
+                                 domain_consts(dom1) + 16, domain_consts(dom2) + 24, M, hscr, sh)) == cudaSuccess &&
+       (e = cudaEventRecord(ctx->aux_ev[6], sh)) == cudaSuccess &&  // H step done (stage times)
+       // polH = M[m .. 2m-2]; M[2m-1] (always zero) becomes the -rs term for delta_1
+       (e = cudaMemcpyAsync(M + (size_t)(2 * m - 1) * 8, rs + 16, 32, cudaMemcpyDeviceToDevice, sh)) == cudaSuccess &&
+       (e = run_msm(false, M + (size_t)m * 8, pk->h_ext, pk->fh, m, outH, P.ms_h, P.bytes_h, sh, &share_h)) == cudaSuccess;
+  if (!ok) { *where = "prove QAP/H"; return e; }
+  for (int i = 0; i < 4; i++) {
+    cudaEventRecord(ctx->aux_ev[1 + i], ctx->aux[i]);
+    cudaStreamWaitEvent(s0, ctx->aux_ev[1 + i], 0);
+  }
+  cudaEventRecord(ctx->aux_ev[5], sh);
+  cudaStreamWaitEvent(s0, ctx->aux_ev[5], 0);
+  k_final_c<<<1, 32, 0, s0>>>(outH, outC, sA, rB1, piC);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// Captures prove_body on the context stream as a CUDA graph, keeps it for the key, witness
+// buffer and scratch, and launches it.  Capture is thread-local, so other threads
+// (other server slots) keep launching meanwhile.  If the capture or its instantiation fails, the
+// entry records that and the sequence runs launch by launch, now and on later calls.
+cudaError_t prove_capture(cs_ctx* ctx, cs_pk* pk, const ProvePlan& P, const uint32_t* d_w, Domain* dom1,
+                          Domain* dom2, const char** where) {
+  // a served context sees every key of its server: room for that many, the oldest goes first
+  // (a graph destroyed while a launch of it runs is freed when the launch completes)
+  constexpr size_t kMaxGraphs = 32;
+  cudaStream_t s0 = ctx->stream;
+  // entries made with an earlier scratch arena can never match again
+  for (size_t i = 0; i < ctx->prove_graphs.size();) {
+    auto& x = ctx->prove_graphs[i];
+    if (x.work != ctx->work.ptr || x.work_bytes != ctx->work.bytes) {
+      if (x.exec) cudaGraphExecDestroy(x.exec);
+      ctx->prove_graphs.erase(ctx->prove_graphs.begin() + i);
+    } else {
+      i++;
+    }
+  }
+  if (ctx->prove_graphs.size() >= kMaxGraphs) {
+    if (ctx->prove_graphs.front().exec) cudaGraphExecDestroy(ctx->prove_graphs.front().exec);
+    ctx->prove_graphs.erase(ctx->prove_graphs.begin());
+  }
+  cs_ctx::ProveGraph g;
+  g.pk_id = pk->id;
+  g.d_w = d_w;
+  g.work = ctx->work.ptr;
+  g.work_bytes = ctx->work.bytes;
+  const unsigned long long l0 = thread_launches();
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    const cudaError_t eb = prove_body(ctx, pk, P, d_w, dom1, dom2, where);
+    e = cudaStreamEndCapture(s0, &graph);
+    if (eb != cudaSuccess) e = eb;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&g.exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e == cudaSuccess) {
+    g.launches = thread_launches() - l0;
+    ctx->prove_graphs.push_back(g);
+    *where = "prove graph launch";
+    return cudaGraphLaunch(g.exec, s0);
+  }
+  // capture failed: clear the error, remember not to capture this combination again and run
+  // the launches directly
+  cudaGetLastError();
+  g.exec = nullptr;
+  ctx->prove_graphs.push_back(g);
+  *where = "prove launch";
+  return prove_body(ctx, pk, P, d_w, dom1, dom2, where);
+}
+
 }  // namespace
 
 namespace csb {
+void prove_graphs_release(cs_ctx* ctx) {
+  for (auto& g : ctx->prove_graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  ctx->prove_graphs.clear();
+}
 size_t prove_workspace_bytes(const cs_pk* pk) { return plan_prove(pk).total; }
 uint32_t pk_n_vars(const cs_pk* pk) { return pk->n_vars; }
 // Grows the context's arenas to what a proof with this key needs (cs_prove would grow them
@@ -332,6 +479,7 @@ int cs_pk_create(cs_ctx* ctx, const cs_pk_desc* d, int on_device, cs_pk** out) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
   std::unique_ptr<cs_pk> pk(new cs_pk());
+  pk->id = g_pk_ids.fetch_add(1);
   pk->device = ctx->device;
   pk->n_vars = d->n_vars;
   pk->n_public = d->n_public;
@@ -395,6 +543,7 @@ int cs_pk_fixed_base(cs_ctx* ctx, cs_pk* pk, int window) {
     if (ctx->aux[i]) e = cudaStreamSynchronize(ctx->aux[i]);
   if (e != cudaSuccess) return fail(ctx, e, "cs_pk_fixed_base: sync");
   pk->drop_fixed();
+  pk->id = g_pk_ids.fetch_add(1);  // the tables move: graphs captured with the old ones are stale
   if (window < 0) return CS_OK;
   const uint32_t nv = pk->n_vars, np1 = pk->n_public + 1;
   struct Job {
@@ -464,88 +613,49 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
   if (e != cudaSuccess) return fail(ctx, e, "prove streams");
   const ProvePlan P = plan_prove(pk);
   if ((e = ctx->work.reserve(P.total, ctx->stream)) != cudaSuccess) return fail(ctx, e, "prove workspace");
-  char* base = static_cast<char*>(ctx->work.ptr);
-  auto at = [&](size_t off) { return reinterpret_cast<uint32_t*>(base + off); };
-  uint32_t *wA = at(P.wA), *wB = at(P.wB), *pA = at(P.pA), *pB = at(P.pB), *M = at(P.M), *hscr = at(P.hscr);
-  uint32_t* pts = at(P.pts);
-  uint32_t *outA = pts, *outB1 = pts + 16, *outB2 = pts + 32, *outC = pts + 64, *outH = pts + 80;
-  uint32_t *sA = pts + 96, *rB1 = pts + 128, *piC = pts + 160;
-  uint32_t* rs = at(P.rs);
-  const uint32_t nv = pk->n_vars, m = pk->m, np1 = pk->n_public + 1;
-  cudaStream_t s0 = ctx->stream;
-  cudaEvent_t ev_w = ctx->aux_ev[0];
   Domain *dom2 = nullptr, *dom1 = nullptr;
   if ((e = domain_get(ctx, pk->log_m + 1, &dom2)) != cudaSuccess || (e = domain_get(ctx, pk->log_m, &dom1)) != cudaSuccess)
     return fail(ctx, e, "prove tables");
-  MsmConfig cfg;
+  char* base = static_cast<char*>(ctx->work.ptr);
+  uint32_t* pts = reinterpret_cast<uint32_t*>(base + P.pts);
+  uint32_t *outA = pts, *outB2 = pts + 32, *piC = pts + 160;
+  uint32_t* rs = reinterpret_cast<uint32_t*>(base + P.rs);
+  cudaStream_t s0 = ctx->stream;
   const GlvSplit glv_rs[2] = {glv::split(s), glv::split(r)};  // s * pi_A, r * pi_B1
   cudaEventRecord(ctx->ev_start, s0);
-  // scalars: w ++ [1, r] and w ++ [1, s]; r, s, -rs
+  // the call's scalars r, s and their GLV splits go to the device first; everything after
+  // them depends only on the key, the witness buffer and the scratch layout
   bool ok = (e = cudaMemcpyAsync(rs, r, 32, cudaMemcpyHostToDevice, s0)) == cudaSuccess &&
             (e = cudaMemcpyAsync(rs + 8, s, 32, cudaMemcpyHostToDevice, s0)) == cudaSuccess &&
-            (e = cudaMemcpyAsync(rs + 32, glv_rs, sizeof(glv_rs), cudaMemcpyHostToDevice, s0)) == cudaSuccess &&
-            (e = cudaMemcpyAsync(wA, d_w, (size_t)nv * 32, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess &&
-            (e = cudaMemcpyAsync(wB, d_w, (size_t)nv * 32, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess;
+            (e = cudaMemcpyAsync(rs + 32, glv_rs, sizeof(glv_rs), cudaMemcpyHostToDevice, s0)) == cudaSuccess;
   if (!ok) return fail(ctx, e, "prove inputs");
-  k_set_tail<<<1, 32, 0, s0>>>(wA, nv, rs);
-  k_set_tail<<<1, 32, 0, s0>>>(wB, nv, rs + 8);
-  k_neg_rs<<<1, 32, 0, s0>>>(rs, rs + 8, rs + 16);
-  note_launch(3);
-  cudaEventRecord(ev_w, s0);
-  // witness MSMs on the auxiliary streams
-  cudaStream_t sa = ctx->aux[0], sb1 = ctx->aux[1], sb2 = ctx->aux[2], sc = ctx->aux[3];
-  for (int i = 0; i < 4; i++) cudaStreamWaitEvent(ctx->aux[i], ev_w, 0);
-  // resident fixed-base tables when the key has them, else the generic MSM over the points
-  auto run_msm = [&](bool ec2, const uint32_t* sc, const uint32_t* pts, const cs_pk::Fixed& f, uint32_t n,
-                     uint32_t* out, size_t off, size_t bytes, cudaStream_t st, const MsmConfig* share = nullptr) {
-    if (pk->has_fixed()) {
-      MsmConfig fcfg = share ? *share : MsmConfig{};
-      fcfg.c = f.c;
-      return ec2 ? msm_fixed_g2(sc, f.table, n, out, at(off), bytes, fcfg, st)
-                 : msm_fixed_g1(sc, f.table, n, out, at(off), bytes, fcfg, st);
+  const char* where = "prove launch";
+  // Graphs pay where launching is a visible part of a proof (small domains: a 2^12 proof
+  // served ~1.45x faster); for large domains they change nothing alone and slowed a served
+  // mix of sizes, so those proofs launch directly.
+  constexpr uint32_t kGraphMaxDomain = 1u << 17;
+  if (!ctx->use_prove_graphs || pk->m > kGraphMaxDomain) {
+    e = prove_body(ctx, pk, P, d_w, dom1, dom2, &where);
+    ctx->stages_valid = true;
+  } else {
+    cs_ctx::ProveGraph* g = nullptr;
+    for (auto& x : ctx->prove_graphs)
+      if (x.pk_id == pk->id && x.d_w == d_w && x.work == ctx->work.ptr && x.work_bytes == ctx->work.bytes)
+        g = &x;
+    if (g && g->exec) {
+      e = cudaGraphLaunch(g->exec, s0);
+      note_launch((unsigned)g->launches);
+      where = "prove graph launch";
+      ctx->stages_valid = false;
+    } else if (g) {
+      e = prove_body(ctx, pk, P, d_w, dom1, dom2, &where);
+      ctx->stages_valid = true;
+    } else {
+      e = prove_capture(ctx, pk, P, d_w, dom1, dom2, &where);
+      ctx->stages_valid = false;
     }
-    return ec2 ? msm_g2(sc, pts, n, out, at(off), bytes, cfg, st) : msm_g1(sc, pts, n, out, at(off), bytes, cfg, st);
-  };
-  // C hands its buckets to H (outC is then the point at infinity, and outH the sum of both)
-  MsmConfig share_c, share_h;
-  if (P.share_ch) {
-    share_c.bucket_out = at(P.cbk);
-    share_h.bucket_add = at(P.cbk);
-    share_h.bucket_ready = ctx->aux_ev[7];
   }
-  ok = (e = run_msm(false, wA, pk->a_ext, pk->fa, nv + 2, outA, P.ms_a, P.bytes_a, sa)) == cudaSuccess &&
-       (e = run_msm(false, wB, pk->b1_ext, pk->fb1, nv + 2, outB1, P.ms_b1, P.bytes_b1, sb1)) == cudaSuccess &&
-       (e = run_msm(true, wB, pk->b2_ext, pk->fb2, nv + 2, outB2, P.ms_b2, P.bytes_b2, sb2)) == cudaSuccess &&
-       (e = run_msm(false, wA + (size_t)np1 * 8, pk->c + (size_t)np1 * 16, pk->fc, nv - np1, outC, P.ms_c, P.bytes_c,
-                    sc, &share_c)) == cudaSuccess;
-  if (!ok) return fail(ctx, e, "prove witness MSMs");
-  if (P.share_ch && (e = cudaEventRecord(ctx->aux_ev[7], sc)) != cudaSuccess) return fail(ctx, e, "prove C buckets");
-  {
-    const GlvSplit* gsp = reinterpret_cast<const GlvSplit*>(rs + 32);
-    k_scale_point_glv<<<1, 32, 0, sa>>>(outA, gsp, sA);        // s * pi_A
-    k_scale_point_glv<<<1, 32, 0, sb1>>>(outB1, gsp + 1, rB1);  // r * pi_B1
-  }
-  note_launch(2);
-  // QAP evaluation, H step and H MSM on their own stream
-  cudaStream_t sh = ctx->aux_h;
-  cudaStreamWaitEvent(sh, ev_w, 0);
-  ok = (e = qap_eval(pk->rows_a, d_w, pA, 0, sh)) == cudaSuccess &&
-       (e = qap_eval(pk->rows_b, d_w, pB, 0, sh)) == cudaSuccess &&
-       (e = hstep_reference_core(pA, pB, pk->log_m, domain_wf(dom2), domain_wi(dom2), domain_wf(dom2),
-                                 domain_consts(dom1) + 16, domain_consts(dom2) + 24, M, hscr, sh)) == cudaSuccess &&
-       (e = cudaEventRecord(ctx->aux_ev[6], sh)) == cudaSuccess &&  // H step done (stage times)
-       // polH = M[m .. 2m-2]; M[2m-1] (always zero) becomes the -rs term for delta_1
-       (e = cudaMemcpyAsync(M + (size_t)(2 * m - 1) * 8, rs + 16, 32, cudaMemcpyDeviceToDevice, sh)) == cudaSuccess &&
-       (e = run_msm(false, M + (size_t)m * 8, pk->h_ext, pk->fh, m, outH, P.ms_h, P.bytes_h, sh, &share_h)) == cudaSuccess;
-  if (!ok) return fail(ctx, e, "prove QAP/H");
-  for (int i = 0; i < 4; i++) {
-    cudaEventRecord(ctx->aux_ev[1 + i], ctx->aux[i]);
-    cudaStreamWaitEvent(s0, ctx->aux_ev[1 + i], 0);
-  }
-  cudaEventRecord(ctx->aux_ev[5], sh);
-  cudaStreamWaitEvent(s0, ctx->aux_ev[5], 0);
-  k_final_c<<<1, 32, 0, s0>>>(outH, outC, sA, rB1, piC);
-  note_launch();
+  if (e != cudaSuccess) return fail(ctx, e, where);
   // proof = pi_A (16) | pi_B (32) | pi_C (16), affine Montgomery
   ok = (e = cudaMemcpyAsync(d_proof, outA, 64, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess &&
        (e = cudaMemcpyAsync(d_proof + 16, outB2, 128, cudaMemcpyDeviceToDevice, s0)) == cudaSuccess &&

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include <nvtx3/nvToolsExt.h>  // header-only; ranges cost nothing unless a profiler is attached
 
@@ -95,6 +96,19 @@ struct cs_ctx {
   cudaStream_t aux_h = nullptr;  // QAP -> H step -> H MSM chain of a proof
   cudaEvent_t aux_ev[8] = {nullptr};
   bool aux_ready = false;
+  // Proof launch sequences captured as CUDA graphs (prove.cu): one per key, witness buffer
+  // and scratch arena, replayed while all three are those of the capture.
+  struct ProveGraph {
+    uint64_t pk_id = 0;
+    const void* d_w = nullptr;
+    void* work = nullptr;
+    size_t work_bytes = 0;
+    cudaGraphExec_t exec = nullptr;  // null: the capture failed, the sequence runs launch by launch
+    unsigned long long launches = 0; // kernels in the graph
+  };
+  std::vector<ProveGraph> prove_graphs;
+  bool use_prove_graphs = true;
+  bool stages_valid = false;  // the stage events hold the last proof's times (not a graph replay)
 };
 
 namespace csb {
@@ -102,6 +116,10 @@ namespace csb {
 cudaError_t ctx_aux_init(cs_ctx* ctx);
 // Counts kernel launches made by this library (cs_kernel_launches()).
 void note_launch(unsigned n = 1);
+// Kernel launches counted by the calling thread so far.
+unsigned long long thread_launches();
+// Destroys the context's captured proof graphs.
+void prove_graphs_release(cs_ctx* ctx);
 // Records a CUDA error on the context and maps it to the C ABI status code.
 int fail(cs_ctx* ctx, cudaError_t e, const char* where);
 int fail_msg(cs_ctx* ctx, int code, const std::string& msg);

@@ -126,10 +126,11 @@ void cs_server::worker(int slot) {
         }
         if (!queue.empty()) {
           need = growth(ctx, queue.front()->pk, stage.bytes);
+          if (need == 0) break;  // the slot already holds the scratch: nothing to admit
           size_t free_b = 0, total_b = 0;
           cudaMemGetInfo(&free_b, &total_b);
           const size_t avail = free_b > promised ? free_b - promised : 0;
-          if (need == 0 || avail >= need + reserve) break;
+          if (avail >= need + reserve) break;
           if (busy == 0) {  // nothing will free memory: refuse the head request
             auto bad = queue.front();
             queue.pop_front();

@@ -61,6 +61,8 @@ def _prove(args, ctx):
     circ = SyntheticCircuit(ctx, args.log_m, seed=args.seed)
     pk = setup_pk(ctx, circ, seed=args.seed + 1)
     prover = Prover(ctx, pk, fixed_base=-1 if args.no_fixed else 0)
+    if not args.graphs:  # stage times need the launches themselves (graph replays carry none)
+        ctx.set_prove_graphs(False)
     r, s = to_limbs(0x1234567890abcdef), to_limbs(0xfedcba0987654321)
     d_proof = torch.zeros(64, dtype=torch.int32, device=torch.device("cuda", ctx.device))
     torch.cuda.synchronize()
@@ -109,6 +111,7 @@ def main(argv=None):
     p = sub.add_parser("prove")
     p.add_argument("--log-m", type=int, default=20)
     p.add_argument("--no-fixed", action="store_true", help="generic MSMs instead of fixed-base tables")
+    p.add_argument("--graphs", action="store_true", help="replay the proof as a CUDA graph (no stage times)")
     t = sub.add_parser("ntt")
     t.add_argument("--log-n", type=int, default=20)
     t.add_argument("--hstep", choices=["reference", "coset"], default=None)
@@ -131,7 +134,7 @@ def main(argv=None):
         rec = dict(info, rep=i, ms=round(ctx.last_ms, 4))
         if args.what == "msm":
             rec["accumulate_ms"] = round(ctx.last_phase_ms, 4)
-        if args.what == "prove":
+        if args.what == "prove" and not args.graphs:
             rec["stages_ms"] = call.keep[2].stages()
         print(json.dumps(rec), flush=True)
     torch.cuda.profiler.stop()

@@ -493,15 +493,21 @@ int cs_pk_fixed_window(const cs_pk *pk, int which);
  * Montgomery, the reference prover's pi_a_eccf1 / pi_b_eccf2 / pi_c_eccf1
  * (groth_prover.py:1245 gen_proof; CPU sequence :575-790 and :1414-1453).
  * cs_prove: host witness and proof, synchronous.  cs_prove_device: device witness and
- * proof buffers, asynchronous on the context stream (r and s are read at call time). */
+ * proof buffers, asynchronous on the context stream (r and s are read at call time).
+ * The launch sequence after the scalar uploads is captured as a CUDA graph on the first
+ * proof with a given key, witness buffer and scratch arena on a context, and replayed by
+ * later proofs with the same three (one graph launch instead of ~150 API calls per proof). */
 int cs_prove(cs_ctx *ctx, cs_pk *pk, const uint32_t *w, const uint32_t *r, const uint32_t *s,
              uint32_t *proof);
 int cs_prove_device(cs_ctx *ctx, cs_pk *pk, const uint32_t *d_w, const uint32_t *r, const uint32_t *s,
                     uint32_t *d_proof);
 /* Stage completion times (ms after the start) of the context's last finished proof: A, B1,
  * B2 (G2), C MSM chains, H step, H MSM, whole proof (up to n of them; the reference prover's
- * t_GP phase dict).  Call after the proof has completed (cs_prove, or cs_ctx_sync). */
+ * t_GP phase dict).  Call after the proof has completed (cs_prove, or cs_ctx_sync).  Graph
+ * replays carry no stage events: CS_ERR_UNSUPPORTED after one (turn graphs off to time stages). */
 int cs_ctx_prove_stages(cs_ctx *ctx, float *ms, int n);
+/* Proof graphs on this context on (default) or off (off also frees the captured graphs). */
+int cs_ctx_set_prove_graphs(cs_ctx *ctx, int enable);
 
 /* ----------------------------------------------- served proving (continuous batching) */
 /* Replaces the reference's one-proof-at-a-time server loop (groth_prover.py:808-891

@@ -112,3 +112,37 @@ def test_dropin_mpoly_eval_fixture(golden):
         L.mpoly_eval_server_h(ctypes.byref(a))
         assert L.cs_qap_last_status() == 0
         assert np.array_equal(out, f[f"mpoly_out_{nv}"])
+
+
+def test_prove_graph_replays_match_cpu(ctx, oracle):
+    """The proof's launch sequence is captured as a CUDA graph on the first proof with a key,
+    witness buffer and scratch, then replayed: replays with new r, s and a new witness in the
+    same buffer give the CPU sequence's bytes; rebuilt tables and graphs turned off too."""
+    import pytest as _pt
+    from cusnarks_b200._lib import CsError
+    from cusnarks_b200.groth import SyntheticCircuit, setup_pk, pk_to_host, Prover
+    from oracle.oracle import random_field
+    circ = SyntheticCircuit(ctx, 9, seed=91)
+    pk = setup_pk(ctx, circ, seed=92)
+    host = pk_to_host(pk)
+    prover = Prover(ctx, pk)
+    lim = lambda x: ints_to_limbs([x])[0]  # noqa: E731
+    try:
+        cases = [(circ.w, 11, 22), (circ.w, 11, 22), (circ.w, 333333, 4444)]
+        w2 = random_field(np.random.Generator(np.random.PCG64(93)), circ.n_vars, 1)
+        w2[0] = ints_to_limbs([1])[0]
+        cases.append((w2, 55, 66))
+        for w, r, s in cases:  # capture, replay, replay with new scalars, new witness
+            got = prover.prove(w, lim(r), lim(s))
+            assert np.array_equal(got, cpu_prove(oracle, host, w, r, s)), (r, s)
+        with _pt.raises(CsError):
+            prover.stages()  # the last proof was a replay: no stage events
+        prover.set_fixed_base(7)  # tables move: the old graph must not be replayed
+        assert np.array_equal(prover.prove(w2, lim(55), lim(66)), cpu_prove(oracle, host, w2, 55, 66))
+        assert np.array_equal(prover.prove(circ.w, lim(11), lim(22)), cpu_prove(oracle, host, circ.w, 11, 22))
+        ctx.set_prove_graphs(False)
+        assert np.array_equal(prover.prove(circ.w, lim(11), lim(22)), cpu_prove(oracle, host, circ.w, 11, 22))
+        assert prover.stages()["total"] > 0
+    finally:
+        ctx.set_prove_graphs(True)
+        prover.close()
