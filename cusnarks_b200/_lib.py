@@ -45,7 +45,8 @@ class ServerStats(ctypes.Structure):
                 ("cancelled", ctypes.c_uint64), ("queued", ctypes.c_uint64), ("running", ctypes.c_uint32),
                 ("max_concurrent", ctypes.c_uint32), ("promised_bytes", ctypes.c_size_t),
                 ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
-                ("hbm_free_bytes", ctypes.c_size_t), ("hbm_total_bytes", ctypes.c_size_t)]
+                ("hbm_free_bytes", ctypes.c_size_t), ("hbm_total_bytes", ctypes.c_size_t),
+                ("batched", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("max_batch_seen", ctypes.c_uint32)]
 
 
 class MpolyEval(ctypes.Structure):
@@ -156,6 +157,7 @@ _SIGNATURES = [
     ("cs_pk_fixed_window", ctypes.c_int, [_vp, ctypes.c_int]),
     ("cs_prove", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     ("cs_prove_device", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    ("cs_prove_batch_device", ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, _vp, _vp, _vp]),
     ("cs_server_create", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(_vp)]),
     ("cs_server_destroy", None, [_vp]),
     ("cs_server_add_key", ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_int)]),
@@ -164,6 +166,7 @@ _SIGNATURES = [
     ("cs_server_stats", ctypes.c_int, [_vp, ctypes.POINTER(ServerStats)]),
     ("cs_server_error", ctypes.c_char_p, [_vp]),
     ("cs_server_cancel", ctypes.c_int, [_vp, ctypes.c_uint64]),
+    ("cs_server_set_max_batch", ctypes.c_int, [_vp, ctypes.c_int]),
     ("cs_debug_fail_allocs", None, [ctypes.c_int]),
     ("cs_setup_lagrange", ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp]),
     ("cs_setup_wire_eval", ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32, _vp]),

@@ -78,23 +78,24 @@ struct cs_msm_batch {
   }
 };
 
-extern "C" {
+namespace csb {
 
-int cs_msm_batch_create(cs_ctx* ctx, int ec2, const cs_msm_job* jobs, uint32_t njobs, int task,
-                        cs_msm_batch** out) {
-  if (!ctx || !out || (njobs && !jobs)) return CS_ERR_ARG;
+// Builds a batch plan from instance descriptions (the caller holds ctx->mu): windows (given, or
+// tuned / by the cost model for generic instances; a fixed-base instance must give the window
+// its table was built with), instances ordered by window, the device job table and the scratch.
+int batch_build(cs_ctx* ctx, int ec2, const BatchSpec* jobs, uint32_t njobs, int task, cs_msm_batch** out) {
   *out = nullptr;
-  std::lock_guard<std::mutex> lk(ctx->mu);
-  cudaSetDevice(ctx->device);
   std::unique_ptr<cs_msm_batch> b(new cs_msm_batch());
   b->device = ctx->device;
   b->ec2 = ec2 ? 1 : 0;
   std::vector<int> win(njobs);
   for (uint32_t i = 0; i < njobs; i++) {
     if (!jobs[i].out || (jobs[i].n && (!jobs[i].scalars || !jobs[i].points)))
-      return csb::fail_msg(ctx, CS_ERR_ARG, "cs_msm_batch_create: job " + std::to_string(i) + " has a null pointer");
-    if (jobs[i].window && (jobs[i].window < 4 || jobs[i].window > 22))
-      return csb::fail_msg(ctx, CS_ERR_ARG, "cs_msm_batch_create: window must be 0 or 4..22");
+      return fail_msg(ctx, CS_ERR_ARG, "cs_msm_batch_create: job " + std::to_string(i) + " has a null pointer");
+    if (jobs[i].fixed && !jobs[i].window)
+      return fail_msg(ctx, CS_ERR_ARG, "batch: a fixed-base instance needs its table's window");
+    if (jobs[i].window && (jobs[i].window < 4 || jobs[i].window > (jobs[i].fixed ? 24 : 22)))
+      return fail_msg(ctx, CS_ERR_ARG, "cs_msm_batch_create: window must be 0 or 4..22");
     win[i] = jobs[i].window ? jobs[i].window : pick_window(ctx->device, ec2, jobs[i].n);
   }
   b->order.resize(njobs);
@@ -103,26 +104,29 @@ int cs_msm_batch_create(cs_ctx* ctx, int ec2, const cs_msm_job* jobs, uint32_t n
   uint64_t terms = 0, buckets = 0, entries = 0, windows = 0;
   uint64_t lv = 0, lv2 = 0;
   for (uint32_t k = 0; k < njobs; k++) {
-    const cs_msm_job& j = jobs[b->order[k]];
+    const BatchSpec& j = jobs[b->order[k]];
     const int c = win[b->order[k]];
     const uint32_t W = 254 / c + 1;
-    csb::BatchJob bj{};
+    const uint32_t sets = j.fixed ? 1u : W;
+    BatchJob bj{};
     bj.scalars = j.scalars;
     bj.points = j.points;
     bj.out = j.out;
     bj.n = j.n;
     bj.c = (uint32_t)c;
     bj.W = W;
+    bj.fixed = j.fixed ? 1u : 0u;
+    bj.sets = sets;
     bj.term0 = (uint32_t)terms;
     bj.bucket0 = (uint32_t)buckets;
     bj.window0 = (uint32_t)windows;
     if (b->groups.empty() || b->groups.back().c != c)
-      b->groups.push_back(csb::BatchGroup{c, (uint32_t)buckets, 0u, (uint32_t)windows});
-    b->groups.back().windows += W;
+      b->groups.push_back(BatchGroup{c, (uint32_t)buckets, 0u, (uint32_t)windows});
+    b->groups.back().windows += sets;
     terms += j.n;
-    buckets += (uint64_t)W << (c - 1);
+    buckets += (uint64_t)sets << (c - 1);
     entries += (uint64_t)j.n * W;
-    windows += W;
+    windows += sets;
     b->jobs.push_back(bj);
   }
   for (const auto& g : b->groups) {
@@ -131,8 +135,8 @@ int cs_msm_batch_create(cs_ctx* ctx, int ec2, const cs_msm_job* jobs, uint32_t n
     lv2 = std::max(lv2, (uint64_t)g.windows * (n1 / 8 + 1));
   }
   if (terms >= 0xffffffffull || buckets >= 0xffffffffull || entries >= 0x7fffffffull)
-    return csb::fail_msg(ctx, CS_ERR_ARG, "cs_msm_batch_create: batch too large (terms x windows must stay below 2^31)");
-  csb::MsmBatch& P = b->plan;
+    return fail_msg(ctx, CS_ERR_ARG, "cs_msm_batch_create: batch too large (terms x windows must stay below 2^31)");
+  MsmBatch& P = b->plan;
   P.njobs = njobs;
   P.terms = (uint32_t)terms;
   P.nbuckets = (uint32_t)buckets;
@@ -145,16 +149,38 @@ int cs_msm_batch_create(cs_ctx* ctx, int ec2, const cs_msm_job* jobs, uint32_t n
   P.task = task > 0 ? task : 64;
   cudaError_t e = cudaSuccess;
   if (njobs) {
-    e = cudaMalloc(&b->d_jobs, sizeof(csb::BatchJob) * njobs);
+    e = cudaMalloc(&b->d_jobs, sizeof(BatchJob) * njobs);
     if (e == cudaSuccess)
-      e = cudaMemcpy(b->d_jobs, b->jobs.data(), sizeof(csb::BatchJob) * njobs, cudaMemcpyHostToDevice);
+      e = cudaMemcpy(b->d_jobs, b->jobs.data(), sizeof(BatchJob) * njobs, cudaMemcpyHostToDevice);
     P.d_jobs = b->d_jobs;
-    b->work_bytes = csb::msm_batch_workspace_bytes(P, ec2 != 0);
+    b->work_bytes = msm_batch_workspace_bytes(P, ec2 != 0);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_work, b->work_bytes);
   }
-  if (e != cudaSuccess) return csb::fail(ctx, e, "cs_msm_batch_create: device buffers");
+  if (e != cudaSuccess) return fail(ctx, e, "cs_msm_batch_create: device buffers");
   *out = b.release();
   return CS_OK;
+}
+
+// Enqueues a batch plan's launches on a stream (no graph of its own).
+cudaError_t batch_enqueue(cs_msm_batch* b, cudaStream_t st) {
+  if (b->plan.njobs == 0) return cudaSuccess;
+  return b->ec2 ? msm_batch_g2(b->plan, b->d_work, b->work_bytes, st)
+                : msm_batch_g1(b->plan, b->d_work, b->work_bytes, st);
+}
+
+}  // namespace csb
+
+extern "C" {
+
+int cs_msm_batch_create(cs_ctx* ctx, int ec2, const cs_msm_job* jobs, uint32_t njobs, int task,
+                        cs_msm_batch** out) {
+  if (!ctx || !out || (njobs && !jobs)) return CS_ERR_ARG;
+  std::vector<csb::BatchSpec> specs(njobs);
+  for (uint32_t i = 0; i < njobs; i++)
+    specs[i] = csb::BatchSpec{jobs[i].scalars, jobs[i].points, jobs[i].out, jobs[i].n, jobs[i].window, false};
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  return csb::batch_build(ctx, ec2, specs.data(), njobs, task, out);
 }
 
 void cs_msm_batch_destroy(cs_msm_batch* b) { delete b; }

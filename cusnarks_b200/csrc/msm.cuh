@@ -39,11 +39,14 @@ namespace csb {
 // Instance of a batch of MSMs: device pointers, size, window, and its first term, bucket
 // and window in the batch (instances are ordered by window so each window group occupies a
 // contiguous bucket range).
+// A batch instance.  fixed = 0: points holds n points, W bucket sets (one per window).
+// fixed = 1: points is a fixed-base table T[j n + i] = 2^(c j) P_i of W windows, one bucket set
+// (entries are table indices), no window Horner.  sets: bucket sets (W or 1).
 struct BatchJob {
   const uint32_t* scalars;
   const uint32_t* points;
   uint32_t* out;
-  uint32_t n, c, W, bucket0, window0, term0, pad0, pad1;
+  uint32_t n, c, W, bucket0, window0, term0, fixed, sets;
 };
 
 // A group of batch instances sharing one window c: buckets [bucket0, bucket0 + windows * B),
@@ -68,6 +71,16 @@ struct MsmBatch {
   int task = 64;
 };
 size_t msm_batch_workspace_bytes(const MsmBatch& b, bool ec2);
+// An instance as a caller describes it (batch.cu builds the plan): fixed = a fixed-base table
+// built with `window`, which is then required.
+struct BatchSpec {
+  const uint32_t* scalars;
+  const uint32_t* points;
+  uint32_t* out;
+  uint32_t n;
+  int window;
+  bool fixed;
+};
 cudaError_t msm_batch_g1(const MsmBatch& b, void* d_work, size_t work_bytes, cudaStream_t stream);
 cudaError_t msm_batch_g2(const MsmBatch& b, void* d_work, size_t work_bytes, cudaStream_t stream);
 

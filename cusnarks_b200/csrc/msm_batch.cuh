@@ -14,6 +14,8 @@
 //   * reduction per window group (instances with equal c are contiguous: one level chain and
 //     one k_window_sum launch per distinct c), and k_bfinish: one warp per instance for the
 //     window Horner and the affine result.
+// Fixed-base instances (resident tables T[j n + i] = 2^(c j) P_i, the proof's MSMs) put every
+// digit into one bucket set and need no window Horner.
 // The sequence contains no allocation and no host synchronisation, so it can be captured in a
 // CUDA graph once and replayed (cs_msm_batch_run).
 #pragma once
@@ -44,7 +46,7 @@ __global__ void k_bcount(const BatchJob* __restrict__ jobs, uint32_t njobs, uint
   if (!load_scalar<F>(jb.scalars, jb.points, i, k)) return;
   const uint32_t B = 1u << (jb.c - 1);
   for_each_digit(k, (int)jb.c, (int)jb.W, [&](int j, uint32_t mag, bool) {
-    atomicAdd(&counts[jb.bucket0 + (size_t)j * B + (mag - 1)], 1u);
+    atomicAdd(&counts[jb.bucket0 + (jb.fixed ? 0 : (size_t)j * B) + (mag - 1)], 1u);
   });
 }
 
@@ -59,13 +61,13 @@ __global__ void k_bscatter(const BatchJob* __restrict__ jobs, uint32_t njobs, ui
   if (!load_scalar<F>(jb.scalars, jb.points, i, k)) return;
   const uint32_t B = 1u << (jb.c - 1);
   for_each_digit(k, (int)jb.c, (int)jb.W, [&](int j, uint32_t mag, bool neg) {
-    const uint32_t pos = atomicAdd(&cursor[jb.bucket0 + (size_t)j * B + (mag - 1)], 1u);
-    entries[pos] = i | (neg ? NEG_BIT : 0u);
+    const uint32_t pos = atomicAdd(&cursor[jb.bucket0 + (jb.fixed ? 0 : (size_t)j * B) + (mag - 1)], 1u);
+    entries[pos] = (jb.fixed ? (uint32_t)j * jb.n + i : i) | (neg ? NEG_BIT : 0u);
   });
 }
 
 // One warp per instance (quad point operations; the warp's 8 quads compute the same):
-// sum_j 2^(c j) S_j over its windows, affine result.
+// sum_j 2^(c j) S_j over its bucket sets (a fixed-base instance has one), affine result.
 template <class F>
 __global__ void k_bfinish(const BatchJob* __restrict__ jobs, uint32_t njobs, const uint32_t* __restrict__ wsum) {
   constexpr int XW = 4 * FieldWords<F>::value;
@@ -73,9 +75,9 @@ __global__ void k_bfinish(const BatchJob* __restrict__ jobs, uint32_t njobs, con
   if (q >= njobs) return;  // whole warps leave together
   const BatchJob jb = jobs[q];
   const uint32_t* w = wsum + (size_t)jb.window0 * XW;
-  XYZZ<F> r = ld_xyzz<F>(w + (size_t)(jb.W - 1) * XW);
+  XYZZ<F> r = ld_xyzz<F>(w + (size_t)(jb.sets - 1) * XW);
 #pragma unroll 1
-  for (int j = (int)jb.W - 2; j >= 0; j--) {
+  for (int j = (int)jb.sets - 2; j >= 0; j--) {
 #pragma unroll 1
     for (uint32_t d = 0; d < jb.c; d++) r = xyzz_dbl_quad(r);
     r = xyzz_add_quad(r, ld_xyzz<F>(w + (size_t)j * XW));

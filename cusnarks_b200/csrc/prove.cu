@@ -32,6 +32,8 @@
 
 namespace csb {
 struct Domain;
+int batch_build(cs_ctx* ctx, int ec2, const BatchSpec* jobs, uint32_t njobs, int task, cs_msm_batch** out);
+cudaError_t batch_enqueue(cs_msm_batch* b, cudaStream_t st);
 cudaError_t domain_get(cs_ctx* ctx, uint32_t L, Domain** out);
 cudaError_t hstep_reference_core(const uint32_t* A, const uint32_t* B, uint32_t L, const uint32_t* Wf2,
                                  const uint32_t* Wi2, const uint32_t* shift, const uint32_t* minv_R,
@@ -212,8 +214,8 @@ inline GlvSplit split(const uint32_t* k32) {
 // out (XYZZ) = k * P for P affine (G1), k given as its GLV split.
 // One warp (launched with 32 threads; its 8 quads compute the same): the independent
 // products of each doubling and addition run on the lanes of a quad; lane 0 stores.
-__global__ void k_scale_point_glv(const uint32_t* __restrict__ P, const GlvSplit* __restrict__ gs,
-                                  uint32_t* __restrict__ out) {
+__device__ void scale_point_glv(const uint32_t* __restrict__ P, const GlvSplit* __restrict__ gs,
+                                uint32_t* __restrict__ out) {
   const Fq beta{{0xd782e155u, 0x71930c11u, 0xffbe3323u, 0xa6bb947cu, 0xd4741444u, 0xaa303344u, 0x26594943u,
                  0x2c3b3f0du}};
   const GlvSplit g = *gs;
@@ -234,12 +236,15 @@ __global__ void k_scale_point_glv(const uint32_t* __restrict__ P, const GlvSplit
   }
   if (threadIdx.x == 0) st_xyzz<Fq>(out, acc);
 }
+__global__ void k_scale_point_glv(const uint32_t* __restrict__ P, const GlvSplit* __restrict__ gs,
+                                  uint32_t* __restrict__ out) {
+  scale_point_glv(P, gs, out);
+}
 
 // pi_C = C2 + C + sA + rB1 (C2, C affine; sA, rB1 XYZZ) -> affine
-__global__ void k_final_c(const uint32_t* __restrict__ c2, const uint32_t* __restrict__ c,
-                          const uint32_t* __restrict__ sa, const uint32_t* __restrict__ rb1,
-                          uint32_t* __restrict__ out) {
-  if (threadIdx.x != 0) return;
+__device__ void final_c(const uint32_t* __restrict__ c2, const uint32_t* __restrict__ c,
+                        const uint32_t* __restrict__ sa, const uint32_t* __restrict__ rb1,
+                        uint32_t* __restrict__ out) {
   XYZZ<Fq> acc = XYZZ<Fq>::inf();
   const Affine<Fq> a = ld_affine<Fq>(c2), b = ld_affine<Fq>(c);
   if (!affine_is_inf(a)) acc = xyzz_madd(acc, a);
@@ -247,6 +252,11 @@ __global__ void k_final_c(const uint32_t* __restrict__ c2, const uint32_t* __res
   acc = xyzz_add(acc, ld_xyzz<Fq>(sa));
   acc = xyzz_add(acc, ld_xyzz<Fq>(rb1));
   st_affine<Fq>(out, xyzz_to_affine(acc));
+}
+__global__ void k_final_c(const uint32_t* __restrict__ c2, const uint32_t* __restrict__ c,
+                          const uint32_t* __restrict__ sa, const uint32_t* __restrict__ rb1,
+                          uint32_t* __restrict__ out) {
+  if (threadIdx.x == 0) final_c(c2, c, sa, rb1, out);
 }
 
 cudaError_t copy_in(void* dst, const void* src, size_t bytes, int on_device, cudaStream_t st) {
@@ -445,6 +455,193 @@ cudaError_t prove_capture(cs_ctx* ctx, cs_pk* pk, const ProvePlan& P, const uint
   return prove_body(ctx, pk, P, d_w, dom1, dom2, where);
 }
 
+// ------------------------------------------------------------------ proof batches ----
+// Several proofs with one key in one pass: their MSMs run as three batched launch sequences
+// (the A, B1 and C MSMs of every proof in one G1 batch, the B2 MSMs in one G2 batch, the H
+// MSMs in one G1 batch after the H steps), each a single sort and a single accumulation over
+// all instances' buckets with the resident fixed-base tables; the QAP and H steps, the GLV
+// scalings and the final combinations run per proof inside the same captured sequence.
+
+// One proof's call inputs, uploaded in one copy per batch.
+struct BatchCall {
+  uint32_t r[8], s[8];
+  GlvSplit glv[2];  // s (for s pi_A), r (for r pi_B1)
+  const uint32_t* d_w;
+  uint32_t* d_proof;
+  uint32_t pad[12];
+};
+static_assert(sizeof(BatchCall) == 256, "BatchCall layout");
+
+struct ProveBatch {
+  uint64_t pk_id = 0;
+  uint32_t k = 0;
+  void* buf = nullptr;
+  size_t per = 0, calls_off = 0, bytes = 0;
+  size_t o_wA = 0, o_wB = 0, o_pA = 0, o_pB = 0, o_M = 0, o_hscr = 0, o_pts = 0, o_rs = 0;
+  PinnedBuffer host;
+  cudaEvent_t uploaded = nullptr;
+  cs_msm_batch *g1abc = nullptr, *g2 = nullptr, *g1h = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long launches = 0;
+  bool no_graph = false;
+  ~ProveBatch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (g1abc) cs_msm_batch_destroy(g1abc);
+    if (g2) cs_msm_batch_destroy(g2);
+    if (g1h) cs_msm_batch_destroy(g1h);
+    if (uploaded) cudaEventDestroy(uploaded);
+    host.release();
+    if (buf) cudaFree(buf);
+  }
+  uint32_t* at(uint32_t i, size_t off) const {
+    return reinterpret_cast<uint32_t*>(static_cast<char*>(buf) + (size_t)i * per + off);
+  }
+  BatchCall* calls() const { return reinterpret_cast<BatchCall*>(static_cast<char*>(buf) + calls_off); }
+};
+
+// wA = w ++ [1, r], wB = w ++ [1, s] per proof (grid.y = proof); thread 0 of each proof also
+// writes r, s, -r s and the GLV splits into the proof's rs area.
+__global__ void k_batch_prep(const BatchCall* __restrict__ calls, uint32_t nv, char* __restrict__ base, size_t per,
+                             size_t o_wA, size_t o_wB, size_t o_rs) {
+  const uint32_t k = blockIdx.y;
+  const BatchCall* c = calls + k;
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t* wA = reinterpret_cast<uint32_t*>(base + (size_t)k * per + o_wA);
+  uint32_t* wB = reinterpret_cast<uint32_t*>(base + (size_t)k * per + o_wB);
+  if (e < nv) {
+    uint32_t v[8];
+    ld_limbs8(v, c->d_w + (size_t)e * 8);
+    st_limbs8(wA + (size_t)e * 8, v);
+    st_limbs8(wB + (size_t)e * 8, v);
+  } else if (e < nv + 2) {
+    for (int t = 0; t < 8; t++) {
+      const uint32_t one = t == 0 ? 1u : 0u;
+      wA[(size_t)e * 8 + t] = e == nv ? one : c->r[t];
+      wB[(size_t)e * 8 + t] = e == nv ? one : c->s[t];
+    }
+  }
+  if (e == 0) {
+    uint32_t* rs = reinterpret_cast<uint32_t*>(base + (size_t)k * per + o_rs);
+    for (int t = 0; t < 8; t++) { rs[t] = c->r[t]; rs[8 + t] = c->s[t]; }
+    Fr rr, ss;
+    for (int t = 0; t < 8; t++) { rr.v[t] = c->r[t]; ss.v[t] = c->s[t]; }
+    const Fr neg = Fr::zero() - rr.to_mont() * ss;  // -(r s), normal form
+    for (int t = 0; t < 8; t++) rs[16 + t] = neg.v[t];
+    const uint32_t* g = reinterpret_cast<const uint32_t*>(c->glv);
+    for (int t = 0; t < 32; t++) rs[32 + t] = g[t];
+  }
+}
+
+// s pi_A and r pi_B1 of every proof: block 2k + which, one warp each.
+__global__ void k_batch_scale(char* __restrict__ base, size_t per, size_t o_pts, size_t o_rs) {
+  const uint32_t k = blockIdx.x >> 1, which = blockIdx.x & 1;
+  uint32_t* pts = reinterpret_cast<uint32_t*>(base + (size_t)k * per + o_pts);
+  const GlvSplit* gs = reinterpret_cast<const GlvSplit*>(base + (size_t)k * per + o_rs + 32 * 4) + which;
+  scale_point_glv(which ? pts + 16 : pts, gs, which ? pts + 128 : pts + 96);
+}
+
+// pi_C of every proof (block k) and the proof words to the caller's buffer.
+__global__ void k_batch_final(const BatchCall* __restrict__ calls, char* __restrict__ base, size_t per,
+                              size_t o_pts) {
+  const uint32_t k = blockIdx.x;
+  uint32_t* pts = reinterpret_cast<uint32_t*>(base + (size_t)k * per + o_pts);
+  if (threadIdx.x == 0) final_c(pts + 80, pts + 64, pts + 96, pts + 128, pts + 160);
+  __syncthreads();
+  const uint32_t t = threadIdx.x;  // 64 threads: pi_A (16) | pi_B (32) | pi_C (16)
+  if (t < 64) {
+    const uint32_t v = t < 16 ? pts[t] : t < 48 ? pts[32 + (t - 16)] : pts[160 + (t - 48)];
+    calls[k].d_proof[t] = v;
+  }
+}
+
+// The batch's launch sequence after the call upload.
+cudaError_t prove_batch_body(cs_ctx* ctx, cs_pk* pk, ProveBatch& B, Domain* dom1, Domain* dom2, const char** where) {
+  const uint32_t nv = pk->n_vars, m = pk->m, K = B.k;
+  char* base = static_cast<char*>(B.buf);
+  cudaStream_t s0 = ctx->stream, sa = ctx->aux[0], sb = ctx->aux[1], sh = ctx->aux_h;
+  cudaError_t e;
+  k_batch_prep<<<dim3((nv + 2 + 127) / 128, K), 128, 0, s0>>>(B.calls(), nv, base, B.per, B.o_wA, B.o_wB, B.o_rs);
+  note_launch();
+  cudaEventRecord(ctx->aux_ev[0], s0);
+  for (cudaStream_t st : {sa, sb, sh}) cudaStreamWaitEvent(st, ctx->aux_ev[0], 0);
+  // A, B1, C of every proof; then the GLV scalings (they read pi_A, pi_B1)
+  if ((e = batch_enqueue(B.g1abc, sa)) != cudaSuccess) { *where = "prove batch G1 MSMs"; return e; }
+  k_batch_scale<<<2 * K, 32, 0, sa>>>(base, B.per, B.o_pts, B.o_rs);
+  note_launch();
+  if ((e = batch_enqueue(B.g2, sb)) != cudaSuccess) { *where = "prove batch G2 MSMs"; return e; }
+  for (uint32_t i = 0; i < K; i++) {
+    uint32_t* M = B.at(i, B.o_M);
+    const bool ok = (e = qap_eval(pk->rows_a, B.at(i, B.o_wA), B.at(i, B.o_pA), 0, sh)) == cudaSuccess &&
+                    (e = qap_eval(pk->rows_b, B.at(i, B.o_wA), B.at(i, B.o_pB), 0, sh)) == cudaSuccess &&
+                    (e = hstep_reference_core(B.at(i, B.o_pA), B.at(i, B.o_pB), pk->log_m, domain_wf(dom2),
+                                              domain_wi(dom2), domain_wf(dom2), domain_consts(dom1) + 16,
+                                              domain_consts(dom2) + 24, M, B.at(i, B.o_hscr), sh)) == cudaSuccess &&
+                    (e = cudaMemcpyAsync(M + (size_t)(2 * m - 1) * 8, B.at(i, B.o_rs) + 16, 32,
+                                         cudaMemcpyDeviceToDevice, sh)) == cudaSuccess;
+    if (!ok) { *where = "prove batch QAP/H"; return e; }
+  }
+  if ((e = batch_enqueue(B.g1h, sh)) != cudaSuccess) { *where = "prove batch H MSMs"; return e; }
+  cudaEventRecord(ctx->aux_ev[1], sa);
+  cudaEventRecord(ctx->aux_ev[2], sb);
+  cudaEventRecord(ctx->aux_ev[5], sh);
+  for (int i : {1, 2, 5}) cudaStreamWaitEvent(s0, ctx->aux_ev[i], 0);
+  k_batch_final<<<K, 64, 0, s0>>>(B.calls(), base, B.per, B.o_pts);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// The context's plan for (key, batch size), made on first use: per-proof scratch, the three
+// MSM batch plans over it, the pinned call staging.  At most four plans per context.
+int prove_batch_plan(cs_ctx* ctx, cs_pk* pk, uint32_t K, ProveBatch** out) {
+  for (auto& p : ctx->prove_batches) {
+    ProveBatch* b = static_cast<ProveBatch*>(p.get());
+    if (b->pk_id == pk->id && b->k == K) { *out = b; return CS_OK; }
+  }
+  constexpr size_t kMaxPlans = 4;
+  if (ctx->prove_batches.size() >= kMaxPlans) {  // the oldest goes, once nothing of it runs
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, e, "prove batch plan cache");
+    ctx->prove_batches.erase(ctx->prove_batches.begin());
+  }
+  std::shared_ptr<ProveBatch> B(new ProveBatch());
+  B->pk_id = pk->id;
+  B->k = K;
+  const size_t nv = pk->n_vars, m = pk->m;
+  size_t o = 0;
+  B->o_wA = o; o += al256((nv + 2) * 32);
+  B->o_wB = o; o += al256((nv + 2) * 32);
+  B->o_pA = o; o += al256(m * 32);
+  B->o_pB = o; o += al256(m * 32);
+  B->o_M = o; o += al256(2 * m * 32);
+  B->o_hscr = o; o += al256(4 * m * 32);
+  B->o_pts = o; o += 2048;
+  B->o_rs = o; o += 256;
+  B->per = al256(o);
+  B->calls_off = B->per * K;
+  B->bytes = B->calls_off + sizeof(BatchCall) * K;
+  cudaError_t e = cudaMalloc(&B->buf, B->bytes);
+  if (e == cudaSuccess) e = B->host.reserve(sizeof(BatchCall) * K);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B->uploaded, cudaEventDisableTiming);
+  if (e != cudaSuccess) return fail(ctx, e, "prove batch buffers");
+  const uint32_t np1 = pk->n_public + 1;
+  std::vector<BatchSpec> abc, b2, h;
+  for (uint32_t i = 0; i < K; i++) {
+    uint32_t* pts = B->at(i, B->o_pts);
+    abc.push_back(BatchSpec{B->at(i, B->o_wA), pk->fa.table, pts, pk->fa.n, pk->fa.c, true});
+    abc.push_back(BatchSpec{B->at(i, B->o_wB), pk->fb1.table, pts + 16, pk->fb1.n, pk->fb1.c, true});
+    abc.push_back(BatchSpec{B->at(i, B->o_wA) + (size_t)np1 * 8, pk->fc.table, pts + 64, pk->fc.n, pk->fc.c, true});
+    b2.push_back(BatchSpec{B->at(i, B->o_wB), pk->fb2.table, pts + 32, pk->fb2.n, pk->fb2.c, true});
+    h.push_back(BatchSpec{B->at(i, B->o_M) + (size_t)m * 8, pk->fh.table, pts + 80, pk->fh.n, pk->fh.c, true});
+  }
+  int st = batch_build(ctx, 0, abc.data(), (uint32_t)abc.size(), 0, &B->g1abc);
+  if (st == CS_OK) st = batch_build(ctx, 1, b2.data(), (uint32_t)b2.size(), 0, &B->g2);
+  if (st == CS_OK) st = batch_build(ctx, 0, h.data(), (uint32_t)h.size(), 0, &B->g1h);
+  if (st != CS_OK) return st;
+  ctx->prove_batches.push_back(B);
+  *out = B.get();
+  return CS_OK;
+}
+
 }  // namespace
 
 namespace csb {
@@ -452,8 +649,20 @@ void prove_graphs_release(cs_ctx* ctx) {
   for (auto& g : ctx->prove_graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   ctx->prove_graphs.clear();
+  ctx->prove_batches.clear();
 }
 size_t prove_workspace_bytes(const cs_pk* pk) { return plan_prove(pk).total; }
+uint32_t pk_domain(const cs_pk* pk) { return pk->m; }
+bool pk_has_fixed(const cs_pk* pk) { return pk->has_fixed(); }
+// Whether the context already holds the batch plan for (key, k): a batch then allocates nothing.
+bool prove_batch_ready(cs_ctx* ctx, const cs_pk* pk, uint32_t k) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  for (auto& p : ctx->prove_batches) {
+    const ProveBatch* b = static_cast<const ProveBatch*>(p.get());
+    if (b->pk_id == pk->id && b->k == k) return true;
+  }
+  return false;
+}
 uint32_t pk_n_vars(const cs_pk* pk) { return pk->n_vars; }
 // Grows the context's arenas to what a proof with this key needs (cs_prove would grow them
 // on its first call): lets the server allocate a slot's scratch right after admission.
@@ -663,6 +872,81 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
   cudaEventRecord(ctx->ev_stop, s0);
   if (!ok) return fail(ctx, e, "prove output");
   if ((e = cudaGetLastError()) != cudaSuccess) return fail(ctx, e, "prove launch");
+  return CS_OK;
+}
+
+int cs_prove_batch_device(cs_ctx* ctx, cs_pk* pk, uint32_t k, const uint32_t* const* d_w, const uint32_t* r,
+                          const uint32_t* s, uint32_t* const* d_proof) {
+  if (!ctx || !pk || !d_w || !r || !s || !d_proof || k == 0 || k > 64) return CS_ERR_ARG;
+  for (uint32_t i = 0; i < k; i++)
+    if (!d_w[i] || !d_proof[i]) return CS_ERR_ARG;
+  if (k == 1 || !pk->has_fixed()) {  // nothing to merge: the single-proof path, one by one
+    for (uint32_t i = 0; i < k; i++) {
+      const int st = cs_prove_device(ctx, pk, d_w[i], r + 8 * (size_t)i, s + 8 * (size_t)i, d_proof[i]);
+      if (st != CS_OK) return st;
+    }
+    return CS_OK;
+  }
+  NvtxRange nvtx("cs_prove_batch");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaError_t e = ctx_aux_init(ctx);
+  if (e != cudaSuccess) return fail(ctx, e, "prove streams");
+  Domain *dom2 = nullptr, *dom1 = nullptr;
+  if ((e = domain_get(ctx, pk->log_m + 1, &dom2)) != cudaSuccess || (e = domain_get(ctx, pk->log_m, &dom1)) != cudaSuccess)
+    return fail(ctx, e, "prove tables");
+  ProveBatch* B = nullptr;
+  int st = prove_batch_plan(ctx, pk, k, &B);
+  if (st != CS_OK) return st;
+  // the staging area may still feed the previous batch's upload
+  if ((e = cudaEventSynchronize(B->uploaded)) != cudaSuccess) return fail(ctx, e, "prove batch staging");
+  BatchCall* hc = static_cast<BatchCall*>(B->host.ptr);
+  for (uint32_t i = 0; i < k; i++) {
+    BatchCall c{};
+    std::memcpy(c.r, r + 8 * (size_t)i, 32);
+    std::memcpy(c.s, s + 8 * (size_t)i, 32);
+    c.glv[0] = glv::split(c.s);
+    c.glv[1] = glv::split(c.r);
+    c.d_w = d_w[i];
+    c.d_proof = d_proof[i];
+    hc[i] = c;
+  }
+  cudaStream_t s0 = ctx->stream;
+  cudaEventRecord(ctx->ev_start, s0);
+  if ((e = cudaMemcpyAsync(B->calls(), hc, sizeof(BatchCall) * k, cudaMemcpyHostToDevice, s0)) != cudaSuccess)
+    return fail(ctx, e, "prove batch inputs");
+  cudaEventRecord(B->uploaded, s0);
+  const char* where = "prove batch launch";
+  if (B->exec) {
+    e = cudaGraphLaunch(B->exec, s0);
+    note_launch((unsigned)B->launches);
+  } else if (B->no_graph || !ctx->use_prove_graphs) {
+    e = prove_batch_body(ctx, pk, *B, dom1, dom2, &where);
+  } else {  // capture the sequence once for this plan and launch it
+    const unsigned long long l0 = thread_launches();
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      const cudaError_t eb = prove_batch_body(ctx, pk, *B, dom1, dom2, &where);
+      e = cudaStreamEndCapture(s0, &graph);
+      if (eb != cudaSuccess) e = eb;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&B->exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e == cudaSuccess) {
+      B->launches = thread_launches() - l0;
+      e = cudaGraphLaunch(B->exec, s0);
+    } else {
+      cudaGetLastError();
+      B->exec = nullptr;
+      B->no_graph = true;
+      e = prove_batch_body(ctx, pk, *B, dom1, dom2, &where);
+    }
+  }
+  ctx->stages_valid = false;
+  cudaEventRecord(ctx->ev_stop, s0);
+  if (e != cudaSuccess) return fail(ctx, e, where);
+  if ((e = cudaGetLastError()) != cudaSuccess) return fail(ctx, e, "prove batch launch");
   return CS_OK;
 }
 

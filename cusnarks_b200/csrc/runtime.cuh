@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstddef>
 #include <cstdio>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -108,6 +109,7 @@ struct cs_ctx {
   };
   std::vector<ProveGraph> prove_graphs;
   bool use_prove_graphs = true;
+  std::vector<std::shared_ptr<void>> prove_batches;  // plans of cs_prove_batch_device (prove.cu)
   bool stages_valid = false;  // the stage events hold the last proof's times (not a graph replay)
 };
 
@@ -118,7 +120,7 @@ cudaError_t ctx_aux_init(cs_ctx* ctx);
 void note_launch(unsigned n = 1);
 // Kernel launches counted by the calling thread so far.
 unsigned long long thread_launches();
-// Destroys the context's captured proof graphs.
+// Destroys the context's captured proof graphs and proof-batch plans (the stream must be idle).
 void prove_graphs_release(cs_ctx* ctx);
 // Records a CUDA error on the context and maps it to the C ABI status code.
 int fail(cs_ctx* ctx, cudaError_t e, const char* where);

@@ -12,7 +12,11 @@
 //     growth plus `reserve`; an admitted slot grows its arenas at once and then withdraws
 //     its promise, since cudaMemGetInfo counts the memory from then on;
 //   * admitted proofs run concurrently on the device: one proof's MSM tails, QAP and
-//     H step overlap the next one's bucket accumulation.
+//     H step overlap the next one's bucket accumulation;
+//   * a slot that takes a request of a small circuit (up to 2^16 constraints) takes the
+//     queued requests with the same key along (up to max_batch, a power of two) and proves
+//     them in one cs_prove_batch_device pass: their MSMs share one digit sort and one
+//     bucket accumulation, and the pass replays as one CUDA graph.
 // Results do not depend on the mix: every proof is computed by the same kernels on its
 // own slot scratch (a test compares proofs made alone and in a mix, byte for byte).
 #include <algorithm>
@@ -35,6 +39,9 @@ namespace csb {
 size_t prove_workspace_bytes(const cs_pk* pk);
 uint32_t pk_n_vars(const cs_pk* pk);
 cudaError_t prove_reserve(cs_ctx* ctx, const cs_pk* pk);
+uint32_t pk_domain(const cs_pk* pk);
+bool pk_has_fixed(const cs_pk* pk);
+bool prove_batch_ready(cs_ctx* ctx, const cs_pk* pk, uint32_t k);
 }  // namespace csb
 
 namespace {
@@ -65,6 +72,7 @@ struct Request {
 struct cs_server {
   int device = 0;
   int nslots = 0;
+  int max_batch = 16;  // same-key requests a slot proves in one pass (cs_prove_batch_device)
   size_t reserve = 0;
   std::vector<cs_pk*> keys;
   std::deque<std::shared_ptr<Request>> queue;
@@ -77,7 +85,8 @@ struct cs_server {
   int busy = 0;
   size_t promised = 0;  // scratch growth admitted but not yet allocated
   // statistics
-  uint64_t completed = 0, failed = 0, rejected = 0, cancelled = 0;
+  uint64_t completed = 0, failed = 0, rejected = 0, cancelled = 0, batched = 0, batches = 0;
+  uint32_t max_batch_seen = 0;
   std::vector<double> lat_ring;  // latencies (ms) of the last kLatRing completed proofs
   size_t lat_next = 0;
   int max_concurrent = 0;
@@ -85,6 +94,10 @@ struct cs_server {
   std::string err;
 
   void worker(int slot);
+  // Proves rq and the same-key requests in batch in one cs_prove_batch_device pass.
+  int prove_group(cs_ctx* ctx, cs_pk* pk, const std::shared_ptr<Request>& rq,
+                  const std::vector<std::shared_ptr<Request>>& batch, csb::PinnedBuffer& stage,
+                  csb::DeviceBuffer& din, std::string& msg);
 };
 
 namespace {
@@ -112,15 +125,18 @@ void cs_server::worker(int slot) {
     return;
   }
   csb::PinnedBuffer stage;
+  csb::DeviceBuffer batch_in;  // witnesses and proofs of a batch
   for (;;) {
     std::shared_ptr<Request> rq;
-    size_t need = 0;
+    std::vector<std::shared_ptr<Request>> batch;  // requests proved together with rq
+    size_t need = 0, batch_need = 0;
     {
       std::unique_lock<std::mutex> lk(mu);
       for (;;) {
         if (stop) {
           lk.unlock();
           stage.release();
+          batch_in.release();
           cs_ctx_destroy(ctx);
           return;
         }
@@ -151,6 +167,38 @@ void cs_server::worker(int slot) {
       if (busy > max_concurrent) max_concurrent = busy;
       rq->t_start = now_ms();
       if (first_start < 0) first_start = rq->t_start;
+      // Same-key requests waiting behind it join it in one batched pass: small circuits only
+      // (up to 2^16 constraints; larger proofs already fill the GPU and would only wait longer),
+      // a power-of-two count so a slot keeps few batch plans; plans not made yet must fit in
+      // free memory (k single-proof scratches bound one).
+      if (max_batch > 1 && csb::pk_domain(rq->pk) <= (1u << 16) && csb::pk_has_fixed(rq->pk)) {
+        uint32_t avail_k = 1;
+        for (auto& q : queue)
+          if (q->pk == rq->pk && avail_k < (uint32_t)max_batch) avail_k++;
+        uint32_t k = 1;
+        while (k * 2 <= avail_k) k *= 2;
+        if (k > 1 && !csb::prove_batch_ready(ctx, rq->pk, k)) {
+          const size_t est = (size_t)k * (csb::prove_workspace_bytes(rq->pk) + (size_t)csb::pk_n_vars(rq->pk) * 32 + 512);
+          size_t free_b = 0, total_b = 0;
+          cudaMemGetInfo(&free_b, &total_b);
+          const size_t fr = free_b > promised ? free_b - promised : 0;
+          if (fr < est + reserve) {
+            k = 1;
+          } else {
+            batch_need = est;  // promised until the plan exists
+            promised += est;
+          }
+        }
+        for (auto it = queue.begin(); it != queue.end() && batch.size() + 1 < k;) {
+          if ((*it)->pk == rq->pk) {
+            (*it)->t_start = rq->t_start;
+            batch.push_back(*it);
+            it = queue.erase(it);
+          } else {
+            ++it;
+          }
+        }
+      }
     }
     cs_pk* pk = rq->pk;
     const size_t wbytes = (size_t)csb::pk_n_vars(pk) * 32;
@@ -170,41 +218,116 @@ void cs_server::worker(int slot) {
         msg = "server: slot scratch allocation failed";
       }
     }
-    if (st == CS_OK && stage.reserve(wbytes) != cudaSuccess) {
+    const size_t k = 1 + batch.size();
+    if (st == CS_OK && stage.reserve(wbytes * k) != cudaSuccess) {
       st = CS_ERR_NOMEM;
       msg = "server: pinned staging buffer";
     }
-    if (st == CS_OK) {
+    if (st == CS_OK && k == 1) {
       std::memcpy(stage.ptr, rq->w, wbytes);
       st = cs_prove(ctx, pk, static_cast<const uint32_t*>(stage.ptr), rq->r, rq->s, rq->proof);
       if (st != CS_OK) msg = cs_ctx_error(ctx);
+    } else if (st == CS_OK) {
+      st = prove_group(ctx, pk, rq, batch, stage, batch_in, msg);
+    }
+    if (batch_need) {
+      std::lock_guard<std::mutex> lk(mu);
+      promised = promised > batch_need ? promised - batch_need : 0;
     }
     const float dev_ms = cs_ctx_last_ms(ctx);
     {
       std::lock_guard<std::mutex> lk(mu);
       busy--;
-      rq->status = st;
-      rq->err = msg;
-      rq->device_ms = dev_ms;
-      rq->t_end = now_ms();
-      rq->done = true;
-      last_end = rq->t_end;
-      if (st == CS_OK) {
-        completed++;
-        const double lat = rq->t_end - rq->t_submit;
-        if (lat_ring.size() < kLatRing) lat_ring.push_back(lat);
-        else lat_ring[lat_next] = lat;
-        lat_next = (lat_next + 1) % kLatRing;
-      } else {
-        failed++;
+      batch.insert(batch.begin(), rq);
+      if (batch.size() > 1 && st == CS_OK) {
+        batched += batch.size();
+        batches++;
+        max_batch_seen = std::max(max_batch_seen, (uint32_t)batch.size());
       }
+      const double t_end = now_ms();
+      for (auto& q : batch) {
+        q->status = st;
+        q->err = msg;
+        q->device_ms = dev_ms;
+        q->t_end = t_end;
+        q->done = true;
+        if (st == CS_OK) {
+          completed++;
+          const double lat = q->t_end - q->t_submit;
+          if (lat_ring.size() < kLatRing) lat_ring.push_back(lat);
+          else lat_ring[lat_next] = lat;
+          lat_next = (lat_next + 1) % kLatRing;
+        } else {
+          failed++;
+        }
+      }
+      last_end = t_end;
     }
     cv_done.notify_all();
     cv_work.notify_all();
   }
 }
 
+int cs_server::prove_group(cs_ctx* ctx, cs_pk* pk, const std::shared_ptr<Request>& rq,
+                           const std::vector<std::shared_ptr<Request>>& batch, csb::PinnedBuffer& stage,
+                           csb::DeviceBuffer& din, std::string& msg) {
+  const size_t k = 1 + batch.size();
+  const size_t wbytes = (size_t)csb::pk_n_vars(pk) * 32;
+  const size_t wstride = (wbytes + 255) & ~size_t(255);
+  cudaStream_t st = static_cast<cudaStream_t>(cs_ctx_stream(ctx));
+  cudaError_t e = din.reserve(k * wstride + k * 256, st);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    msg = "server: batch witness buffer";
+    return CS_ERR_NOMEM;
+  }
+  std::vector<const uint32_t*> dw(k);
+  std::vector<uint32_t*> dp(k);
+  std::vector<uint32_t> r(8 * k), s(8 * k);
+  char* dbase = static_cast<char*>(din.ptr);
+  for (size_t i = 0; i < k; i++) {
+    const Request& q = i == 0 ? *rq : *batch[i - 1];
+    std::memcpy(static_cast<char*>(stage.ptr) + i * wbytes, q.w, wbytes);
+    std::memcpy(&r[8 * i], q.r, 32);
+    std::memcpy(&s[8 * i], q.s, 32);
+    dw[i] = reinterpret_cast<const uint32_t*>(dbase + i * wstride);
+    dp[i] = reinterpret_cast<uint32_t*>(dbase + k * wstride + i * 256);
+    e = cudaMemcpyAsync(const_cast<uint32_t*>(dw[i]), static_cast<char*>(stage.ptr) + i * wbytes, wbytes,
+                        cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) {
+      msg = "server: batch witness upload";
+      cudaStreamSynchronize(st);
+      cudaGetLastError();
+      return CS_ERR_CUDA;
+    }
+  }
+  int rc = cs_prove_batch_device(ctx, pk, (uint32_t)k, dw.data(), r.data(), s.data(), dp.data());
+  if (rc != CS_OK) {
+    msg = cs_ctx_error(ctx);
+    cudaStreamSynchronize(st);  // the staged witnesses may still be in flight
+    cudaGetLastError();
+    return rc;
+  }
+  for (size_t i = 0; i < k && e == cudaSuccess; i++) {
+    Request& q = i == 0 ? *rq : *batch[i - 1];
+    e = cudaMemcpyAsync(q.proof, dp[i], 256, cudaMemcpyDeviceToHost, st);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    msg = "server: batch proof download";
+    return CS_ERR_CUDA;
+  }
+  return CS_OK;
+}
+
 extern "C" {
+
+int cs_server_set_max_batch(cs_server* s, int k) {
+  if (!s || k < 1 || k > 64) return CS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->max_batch = k;
+  return CS_OK;
+}
 
 int cs_server_create(int device, int slots, size_t reserve_bytes, cs_server** out) {
   if (!out || slots < 1 || slots > 64) return CS_ERR_ARG;
@@ -313,6 +436,9 @@ int cs_server_stats(cs_server* s, cs_server_counters* st) {
     st->running = (uint32_t)s->busy;
     st->max_concurrent = (uint32_t)s->max_concurrent;
     st->promised_bytes = s->promised;
+    st->batched = s->batched;
+    st->batches = s->batches;
+    st->max_batch_seen = s->max_batch_seen;
     lat = s->lat_ring;
   }
   st->p50_ms = st->p99_ms = 0.0;

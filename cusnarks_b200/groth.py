@@ -365,6 +365,18 @@ class Prover:
                              out.ctypes.data), self.ctx.handle)
         return out
 
+    def prove_batch_device(self, d_ws, rs, ss, d_proofs):
+        """Several proofs in one pass (cs_prove_batch_device): d_ws, d_proofs device pointers,
+        rs, ss 8-word normal-form scalars, one per proof."""
+        k = len(d_ws)
+        w_arr = (ctypes.c_void_p * k)(*d_ws)
+        p_arr = (ctypes.c_void_p * k)(*d_proofs)
+        r = np.ascontiguousarray(np.stack([np.asarray(x, dtype=np.uint32).reshape(8) for x in rs]))
+        s = np.ascontiguousarray(np.stack([np.asarray(x, dtype=np.uint32).reshape(8) for x in ss]))
+        check(lib().cs_prove_batch_device(self.ctx.handle, self.handle, k, ctypes.cast(w_arr, ctypes.c_void_p),
+                                          r.ctypes.data, s.ctypes.data, ctypes.cast(p_arr, ctypes.c_void_p)),
+              self.ctx.handle)
+
     def prove_device(self, d_w: int, r, s, d_proof: int):
         r = np.ascontiguousarray(r, dtype=np.uint32).reshape(8)
         s = np.ascontiguousarray(s, dtype=np.uint32).reshape(8)

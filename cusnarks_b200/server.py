@@ -16,12 +16,19 @@ from ._lib import lib, ServerResult, ServerStats, CS_OK, CS_ERR_TIMEOUT, CsError
 
 
 class ProveServer:
-    def __init__(self, device: int = 0, slots: int = 3, reserve_bytes: int = 1 << 30):
+    def __init__(self, device: int = 0, slots: int = 3, reserve_bytes: int = 1 << 30, max_batch: int = 16):
+        """max_batch: same-key requests of a small key (at most 2^16 constraints) that one slot
+        proves in one batched pass (cs_server_set_max_batch); 1 proves one at a time."""
         h = ctypes.c_void_p()
         st = lib().cs_server_create(device, slots, reserve_bytes, ctypes.byref(h))
         if st != CS_OK:
             raise CsError(st, "cs_server_create failed")
         self.handle = h
+        st = lib().cs_server_set_max_batch(h, max_batch)
+        if st != CS_OK:
+            lib().cs_server_destroy(h)
+            self.handle = None
+            raise CsError(st, "cs_server_set_max_batch failed")
         self._keys = []
         self._pending = {}
 

@@ -501,6 +501,16 @@ int cs_prove(cs_ctx *ctx, cs_pk *pk, const uint32_t *w, const uint32_t *r, const
              uint32_t *proof);
 int cs_prove_device(cs_ctx *ctx, cs_pk *pk, const uint32_t *d_w, const uint32_t *r, const uint32_t *s,
                     uint32_t *d_proof);
+/* k proofs with one key in one pass (no counterpart in the reference, which proves one at a
+ * time): the A, B1 and C MSMs of all k proofs run as one batched G1 multi-exponentiation (one
+ * sort, one accumulation over every instance's buckets, the key's fixed-base tables), the B2
+ * MSMs as one G2 batch and the H MSMs as one G1 batch after the per-proof QAP and H steps;
+ * the sequence is captured as a CUDA graph per context, key and k.  d_w, d_proof: host arrays
+ * of k device pointers (witnesses, 64-word proofs); r, s: k x 8 words each, host.  Same proof
+ * bytes as k calls of cs_prove_device.  1 <= k <= 64; a key without fixed-base tables, or
+ * k = 1, proves one by one.  Asynchronous on the context stream. */
+int cs_prove_batch_device(cs_ctx *ctx, cs_pk *pk, uint32_t k, const uint32_t *const *d_w, const uint32_t *r,
+                          const uint32_t *s, uint32_t *const *d_proof);
 /* Stage completion times (ms after the start) of the context's last finished proof: A, B1,
  * B2 (G2), C MSM chains, H step, H MSM, whole proof (up to n of them; the reference prover's
  * t_GP phase dict).  Call after the proof has completed (cs_prove, or cs_ctx_sync).  Graph
@@ -535,6 +545,9 @@ typedef struct {
   size_t promised_bytes;
   double p50_ms, p99_ms;            /* latency (submit -> done) over the last 1024 proofs */
   size_t hbm_free_bytes, hbm_total_bytes;
+  uint64_t batched;         /* proofs that ran in a same-key batch of two or more */
+  uint64_t batches;         /* such batches */
+  uint32_t max_batch_seen;  /* largest batch so far */
 } cs_server_counters;
 int cs_server_create(int device, int slots, size_t reserve_bytes, cs_server **out);
 void cs_server_destroy(cs_server *srv);
@@ -543,6 +556,12 @@ int cs_server_submit(cs_server *srv, int key_id, const uint32_t *w, const uint32
                      uint32_t *proof, uint64_t *ticket);
 int cs_server_wait(cs_server *srv, uint64_t ticket, double timeout_s, cs_server_result *res);
 int cs_server_stats(cs_server *srv, cs_server_counters *st);
+/* Same-key batching: a slot that takes a request whose key has at most 2^16 constraints (and
+ * fixed-base tables) takes up to k - 1 more queued requests with that key along and proves
+ * them in one cs_prove_batch_device pass (k the largest power of two <= max_batch that the
+ * queue fills).  Proof bytes are those of lone proofs.  Default 16; 1 turns batching off;
+ * 1 <= max_batch <= 64. */
+int cs_server_set_max_batch(cs_server *srv, int max_batch);
 /* Removes a request that is still queued (its wait returns CS_ERR_CANCELLED); CS_ERR_ARG when
  * the request is unknown, already running or finished. */
 int cs_server_cancel(cs_server *srv, uint64_t ticket);

@@ -146,3 +146,47 @@ def test_prove_graph_replays_match_cpu(ctx, oracle):
     finally:
         ctx.set_prove_graphs(True)
         prover.close()
+
+
+def test_prove_batch_matches_cpu(ctx, oracle):
+    """cs_prove_batch_device: k proofs with one key in one pass (batched G1 / G2 / H MSMs over
+    the fixed-base tables) give, proof by proof, the CPU sequence's bytes: a first call
+    (captured), a replay with new witnesses and scalars, a different k, and a key without
+    tables (proved one by one)."""
+    import torch
+    from cusnarks_b200.groth import SyntheticCircuit, setup_pk, pk_to_host, Prover
+    from oracle.oracle import random_field
+    circ = SyntheticCircuit(ctx, 8, seed=95)
+    pk = setup_pk(ctx, circ, seed=96)
+    host = pk_to_host(pk)
+    rng = np.random.Generator(np.random.PCG64(97))
+
+    def batch(prover, k):
+        ws = [circ.w] + [random_field(rng, circ.n_vars, 1) for _ in range(k - 1)]
+        for w in ws[1:]:
+            w[0] = ints_to_limbs([1])[0]
+        rs = [int(rng.integers(1, 1 << 62)) for _ in range(k)]
+        ss = [int(rng.integers(1, 1 << 62)) * 3 % R for _ in range(k)]
+        dws = [torch.from_numpy(np.ascontiguousarray(w).view(np.int32)).cuda() for w in ws]
+        dp = torch.zeros((k, 64), dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        prover.prove_batch_device([t.data_ptr() for t in dws], [ints_to_limbs([x])[0] for x in rs],
+                                  [ints_to_limbs([x])[0] for x in ss], [dp[i].data_ptr() for i in range(k)])
+        ctx.sync()
+        got = dp.cpu().numpy().view(np.uint32)
+        for i in range(k):
+            assert np.array_equal(got[i], cpu_prove(oracle, host, ws[i], rs[i], ss[i])), (k, i)
+
+    prover = Prover(ctx, pk)
+    try:
+        batch(prover, 5)   # plan, capture, launch
+        batch(prover, 5)   # replay with new inputs
+        batch(prover, 3)
+        batch(prover, 1)
+    finally:
+        prover.close()
+    plain = Prover(ctx, pk, fixed_base=-1)
+    try:
+        batch(plain, 2)
+    finally:
+        plain.close()

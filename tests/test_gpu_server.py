@@ -77,3 +77,36 @@ def test_admission_refuses_what_cannot_fit(keys):
         assert srv.stats()["rejected"] == 1
     finally:
         srv.close()
+
+
+def test_same_key_batches_equal_alone(keys):
+    """One slot, a request of the 2^11 key first (it grows the slot's scratch while the rest
+    queue), then 13 requests of the 2^7 key with distinct witnesses and (r, s): the slot
+    proves the queued ones in same-key batches (8, then 4, then 1) and every proof equals
+    the lone proof of its own witness and (r, s)."""
+    from cusnarks_b200.server import ProveServer
+    rng = np.random.Generator(np.random.PCG64(77))
+    circ0, _, prover0 = keys[0]
+    circ2, _, prover2 = keys[2]
+    ws = []
+    for i in range(13):
+        w = circ0.w.copy()
+        lo = circ0.n_public + 1
+        w[lo:lo + 4] = ints_to_limbs([int(x) % R for x in rng.integers(1, 1 << 62, 4)])
+        ws.append(w)
+    alone = [prover0.prove(ws[i], *_rs(i)) for i in range(13)]
+    first = prover2.prove(circ2.w, *_rs(99))
+    srv = ProveServer(0, slots=1, reserve_bytes=64 << 20, max_batch=8)
+    try:
+        k0, k2 = srv.add_key(prover0), srv.add_key(prover2)
+        t_first = srv.submit(k2, circ2.w, *_rs(99))
+        tickets = [srv.submit(k0, ws[i], *_rs(i)) for i in range(13)]
+        assert np.array_equal(srv.wait(t_first, timeout=120.0)[0], first)
+        for i, t in enumerate(tickets):
+            proof, _ = srv.wait(t, timeout=120.0)
+            assert np.array_equal(proof, alone[i]), i
+        st = srv.stats()
+        assert st["completed"] == 14 and st["failed"] == 0
+        assert st["batches"] >= 1 and 2 <= st["max_batch_seen"] <= 8, st
+    finally:
+        srv.close()
