@@ -395,7 +395,7 @@ def served_mix(ctx, slots: int, n_requests: int, seed: int = 5, big=None):
     r, s = to_limbs(0x1234567890abcdef), to_limbs(0xfedcba0987654321)
     pick = rng.integers(0, 8, n_requests)
     jobs = [(keys[k], circs[k].w, r, s) for k in pick]
-    served_run(srv, jobs[:16])                    # warm every slot's scratch and twiddles
+    served_run(srv, jobs)                         # warm every slot's scratch, twiddles and batch plans
     wall, lat = served_run(srv, jobs)
     sat = len(jobs) / wall
     out = {"circuits_log2": logs, "slots": slots, "requests": len(jobs),

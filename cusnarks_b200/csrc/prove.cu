@@ -21,6 +21,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include "../../include/cusnarks_b200.h"
@@ -591,14 +592,20 @@ cudaError_t prove_batch_body(cs_ctx* ctx, cs_pk* pk, ProveBatch& B, Domain* dom1
 }
 
 // The context's plan for (key, batch size), made on first use: per-proof scratch, the three
-// MSM batch plans over it, the pinned call staging.  At most four plans per context.
+// MSM batch plans over it, the pinned call staging.  At most 16 plans per context (a server
+// slot meets a few small keys at a few batch sizes); the least recently used one goes.
 int prove_batch_plan(cs_ctx* ctx, cs_pk* pk, uint32_t K, ProveBatch** out) {
-  for (auto& p : ctx->prove_batches) {
-    ProveBatch* b = static_cast<ProveBatch*>(p.get());
-    if (b->pk_id == pk->id && b->k == K) { *out = b; return CS_OK; }
+  auto& plans = ctx->prove_batches;
+  for (size_t i = 0; i < plans.size(); i++) {
+    ProveBatch* b = static_cast<ProveBatch*>(plans[i].get());
+    if (b->pk_id == pk->id && b->k == K) {
+      std::rotate(plans.begin() + i, plans.begin() + i + 1, plans.end());  // most recent last
+      *out = b;
+      return CS_OK;
+    }
   }
-  constexpr size_t kMaxPlans = 4;
-  if (ctx->prove_batches.size() >= kMaxPlans) {  // the oldest goes, once nothing of it runs
+  constexpr size_t kMaxPlans = 16;
+  if (ctx->prove_batches.size() >= kMaxPlans) {  // the least recent goes, once nothing of it runs
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return fail(ctx, e, "prove batch plan cache");
     ctx->prove_batches.erase(ctx->prove_batches.begin());

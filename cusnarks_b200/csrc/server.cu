@@ -47,6 +47,7 @@ bool prove_batch_ready(cs_ctx* ctx, const cs_pk* pk, uint32_t k);
 namespace {
 
 constexpr size_t kLatRing = 1024;
+constexpr uint32_t kMinBatch = 4;  // fewer same-key requests are proved one by one
 
 double now_ms() {
   using namespace std::chrono;
@@ -169,14 +170,16 @@ void cs_server::worker(int slot) {
       if (first_start < 0) first_start = rq->t_start;
       // Same-key requests waiting behind it join it in one batched pass: small circuits only
       // (up to 2^16 constraints; larger proofs already fill the GPU and would only wait longer),
-      // a power-of-two count so a slot keeps few batch plans; plans not made yet must fit in
-      // free memory (k single-proof scratches bound one).
+      // 4, 8 or 16 of them (powers of two from 4: a slot keeps few batch plans, and two or three
+      // requests run as well on the other slots); plans not made yet must fit in free memory
+      // (k single-proof scratches bound one).
       if (max_batch > 1 && csb::pk_domain(rq->pk) <= (1u << 16) && csb::pk_has_fixed(rq->pk)) {
         uint32_t avail_k = 1;
         for (auto& q : queue)
           if (q->pk == rq->pk && avail_k < (uint32_t)max_batch) avail_k++;
         uint32_t k = 1;
         while (k * 2 <= avail_k) k *= 2;
+        if (k < kMinBatch) k = 1;
         if (k > 1 && !csb::prove_batch_ready(ctx, rq->pk, k)) {
           const size_t est = (size_t)k * (csb::prove_workspace_bytes(rq->pk) + (size_t)csb::pk_n_vars(rq->pk) * 32 + 512);
           size_t free_b = 0, total_b = 0;

@@ -18,7 +18,8 @@ from ._lib import lib, ServerResult, ServerStats, CS_OK, CS_ERR_TIMEOUT, CsError
 class ProveServer:
     def __init__(self, device: int = 0, slots: int = 3, reserve_bytes: int = 1 << 30, max_batch: int = 16):
         """max_batch: same-key requests of a small key (at most 2^16 constraints) that one slot
-        proves in one batched pass (cs_server_set_max_batch); 1 proves one at a time."""
+        proves in one batched pass (cs_server_set_max_batch; batches of 4, 8 or 16); below 4 proves
+        one at a time."""
         h = ctypes.c_void_p()
         st = lib().cs_server_create(device, slots, reserve_bytes, ctypes.byref(h))
         if st != CS_OK:

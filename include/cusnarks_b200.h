@@ -559,8 +559,8 @@ int cs_server_stats(cs_server *srv, cs_server_counters *st);
 /* Same-key batching: a slot that takes a request whose key has at most 2^16 constraints (and
  * fixed-base tables) takes up to k - 1 more queued requests with that key along and proves
  * them in one cs_prove_batch_device pass (k the largest power of two <= max_batch that the
- * queue fills).  Proof bytes are those of lone proofs.  Default 16; 1 turns batching off;
- * 1 <= max_batch <= 64. */
+ * queue fills, at least 4; fewer run one by one).  Proof bytes are those of lone proofs.
+ * Default 16; below 4 turns batching off; 1 <= max_batch <= 64. */
 int cs_server_set_max_batch(cs_server *srv, int max_batch);
 /* Removes a request that is still queued (its wait returns CS_ERR_CANCELLED); CS_ERR_ARG when
  * the request is unknown, already running or finished. */
