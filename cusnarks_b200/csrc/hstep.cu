@@ -141,18 +141,21 @@ const uint32_t* domain_consts(const Domain* d) { return d->consts; }
 // m-th roots (Montgomery) -> the 2m coefficients of A(x)B(x) in normal form.
 //   tabs: Wf2/Wi2 twiddles of the 2m-point domain, shift[i] (i < m) the odd-coset shift,
 //   minv_R = m^-1 (Montgomery), m2inv = (2m)^-1 (normal form).
-// Scratch: 4 m elements.  A and B are not modified.
+// Scratch: 4 m elements.  A and B are not modified.  batch instances: instance y's A, B,
+// out and scratch lie y * stride words after instance 0's (the tables are shared).
 cudaError_t hstep_reference_core(const uint32_t* A, const uint32_t* B, uint32_t L, const uint32_t* Wf2,
                                  const uint32_t* Wi2, const uint32_t* shift, const uint32_t* minv_R,
-                                 const uint32_t* m2inv, uint32_t* out, uint32_t* scratch, cudaStream_t st) {
+                                 const uint32_t* m2inv, uint32_t* out, uint32_t* scratch, cudaStream_t st,
+                                 uint32_t batch = 1, size_t stride = 0) {
   const size_t m = (size_t)1 << L;
   uint32_t* E = scratch;
   uint32_t* O = scratch + m * 8;
   uint32_t* a = scratch + 2 * m * 8;
   uint32_t* b = scratch + 3 * m * 8;
   cudaError_t e;
-  if ((e = fr_mul(A, B, E, (uint32_t)m, st)) != cudaSuccess) return e;
+  if ((e = fr_mul_batch(A, B, E, (uint32_t)m, batch, stride, st)) != cudaSuccess) return e;
   NttArgs t;
+  t.batch = batch; t.stride = stride;
   t.log_n = L; t.log_tab = L + 1;
   // a = shift * INTT_m(A), b likewise
   t.in = A; t.out = a; t.W = Wi2; t.post_scalar = minv_R; t.post_tab = shift;
@@ -165,9 +168,10 @@ cudaError_t hstep_reference_core(const uint32_t* A, const uint32_t* B, uint32_t 
   if ((e = ntt_run(t, st)) != cudaSuccess) return e;
   t.in = b; t.out = b; t.tmp = O;
   if ((e = ntt_run(t, st)) != cudaSuccess) return e;
-  if ((e = fr_mul(a, b, O, (uint32_t)m, st)) != cudaSuccess) return e;
+  if ((e = fr_mul_batch(a, b, O, (uint32_t)m, batch, stride, st)) != cudaSuccess) return e;
   // 2m coefficients, normal form
   NttArgs u;
+  u.batch = batch; u.stride = stride;
   u.log_n = L + 1; u.log_tab = L + 1;
   u.in = E; u.in_odd = O; u.out = out; u.W = Wi2; u.post_scalar = m2inv;
   return ntt_run(u, st);

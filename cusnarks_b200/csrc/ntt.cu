@@ -22,11 +22,17 @@ CSB_DEV void sts_fr(uint4* s, uint32_t i, const Fr& x) {
 
 // One pass: stages s0 .. s0+S-1 of a radix-2 DIT transform of 2^L points.  Block q owns
 // the 2^S elements base + (i << s0), base = ((q >> s0) << (s0 + S)) + (q & (2^s0 - 1)).
+// blockIdx.y: the instance of a batch, its arrays `stride` words after the previous one's.
 __global__ void __launch_bounds__(kThreads) k_ntt_pass(
     const uint32_t* __restrict__ in, const uint32_t* __restrict__ in_odd, uint32_t* out,
     uint32_t L, uint32_t s0, uint32_t S, int bitrev, const uint32_t* __restrict__ W,
-    uint32_t wshift, const uint32_t* __restrict__ post_tab, const uint32_t* __restrict__ post_scalar) {
+    uint32_t wshift, const uint32_t* __restrict__ post_tab, const uint32_t* __restrict__ post_scalar,
+    size_t stride) {
   extern __shared__ uint4 sm[];
+  const size_t inst = (size_t)blockIdx.y * stride;
+  in += inst;
+  if (in_odd) in_odd += inst;
+  out += inst;
   const uint32_t q = blockIdx.x;
   const uint32_t rmask = (1u << s0) - 1u;
   const uint64_t base = ((uint64_t)(q >> s0) << (s0 + S)) + (q & rmask);
@@ -103,10 +109,11 @@ __global__ void k_gather_roots(uint32_t* __restrict__ out, const uint32_t* __res
 }
 
 __global__ void k_fr_mul(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
-                         uint32_t* __restrict__ out, uint32_t n) {
+                         uint32_t* __restrict__ out, uint32_t n, size_t stride) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  st_fp<ModR>(out + (size_t)i * 8, ld_fp<ModR>(a + (size_t)i * 8) * ld_fp<ModR>(b + (size_t)i * 8));
+  const size_t o = (size_t)blockIdx.y * stride + (size_t)i * 8;
+  st_fp<ModR>(out + o, ld_fp<ModR>(a + o) * ld_fp<ModR>(b + o));
 }
 
 __global__ void k_fr_mul_sub_scale(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
@@ -134,7 +141,8 @@ void plan_passes(uint32_t L, uint32_t* sizes, int* np) {
 
 cudaError_t ntt_run(const NttArgs& a, cudaStream_t st) {
   const uint32_t L = a.log_n;
-  if (L == 0 || L > 28 || a.log_tab < L || !a.W || !a.in || !a.out) return cudaErrorInvalidValue;
+  if (L == 0 || L > 28 || a.log_tab < L || !a.W || !a.in || !a.out || a.batch == 0 || a.batch > 65535)
+    return cudaErrorInvalidValue;
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(k_ntt_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (1 << kMaxStages) * 32);
@@ -158,9 +166,9 @@ cudaError_t ntt_run(const NttArgs& a, cudaStream_t st) {
     uint32_t* dst = last ? a.out : work;
     const unsigned blocks = 1u << (L - S);
     const unsigned threads = (1u << (S - 1)) < (unsigned)kThreads ? (1u << (S - 1)) : (unsigned)kThreads;
-    k_ntt_pass<<<blocks, threads > 0 ? threads : 1, (1u << S) * 32, st>>>(
+    k_ntt_pass<<<dim3(blocks, a.batch), threads > 0 ? threads : 1, (1u << S) * 32, st>>>(
         src, src_odd, dst, L, s0, S, first ? 1 : 0, a.W, a.log_tab - L,
-        last ? a.post_tab : nullptr, last ? a.post_scalar : nullptr);
+        last ? a.post_tab : nullptr, last ? a.post_scalar : nullptr, a.stride);
     note_launch();
     s0 += S;
   }
@@ -185,8 +193,14 @@ cudaError_t ntt_gather_roots(uint32_t* d_out, const uint32_t* d_table, uint64_t 
 }
 
 cudaError_t fr_mul(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n, cudaStream_t st) {
-  if (n == 0) return cudaSuccess;
-  k_fr_mul<<<(n + 255) / 256, 256, 0, st>>>(a, b, out, n);
+  return fr_mul_batch(a, b, out, n, 1, 0, st);
+}
+
+cudaError_t fr_mul_batch(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n, uint32_t batch,
+                         size_t stride, cudaStream_t st) {
+  if (n == 0 || batch == 0) return cudaSuccess;
+  if (batch > 65535) return cudaErrorInvalidValue;
+  k_fr_mul<<<dim3((n + 255) / 256, batch), 256, 0, st>>>(a, b, out, n, stride);
   note_launch();
   return cudaGetLastError();
 }

@@ -25,6 +25,10 @@ struct NttArgs {
   uint32_t log_tab = 0;             // W is a table for 2^log_tab points
   const uint32_t* post_tab = nullptr;     // out[i] *= post_tab[i] (Montgomery product)
   const uint32_t* post_scalar = nullptr;  // out[i] *= *post_scalar (Montgomery product)
+  // batch instances of the transform: instance y reads and writes in, in_odd, out and tmp
+  // offset by y * stride words (W, post_tab and post_scalar are shared)
+  uint32_t batch = 1;
+  size_t stride = 0;
 };
 
 cudaError_t ntt_run(const NttArgs& a, cudaStream_t st);
@@ -38,6 +42,9 @@ cudaError_t ntt_gather_roots(uint32_t* d_out, const uint32_t* d_table, uint64_t 
 
 // Elementwise helpers on Fr arrays (Montgomery products)
 cudaError_t fr_mul(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n, cudaStream_t st);
+// batch instances of fr_mul, instance y at a, b and out offset by y * stride words
+cudaError_t fr_mul_batch(const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t n, uint32_t batch,
+                         size_t stride, cudaStream_t st);
 // out = (a*b - c) * s  (s one element)
 cudaError_t fr_mul_sub_scale(const uint32_t* a, const uint32_t* b, const uint32_t* c,
                              const uint32_t* s, uint32_t* out, uint32_t n, cudaStream_t st);

@@ -38,7 +38,8 @@ cudaError_t batch_enqueue(cs_msm_batch* b, cudaStream_t st);
 cudaError_t domain_get(cs_ctx* ctx, uint32_t L, Domain** out);
 cudaError_t hstep_reference_core(const uint32_t* A, const uint32_t* B, uint32_t L, const uint32_t* Wf2,
                                  const uint32_t* Wi2, const uint32_t* shift, const uint32_t* minv_R,
-                                 const uint32_t* m2inv, uint32_t* out, uint32_t* scratch, cudaStream_t st);
+                                 const uint32_t* m2inv, uint32_t* out, uint32_t* scratch, cudaStream_t st,
+                                 uint32_t batch = 1, size_t stride = 0);
 // accessors into the opaque Domain (hstep.cu)
 const uint32_t* domain_wf(const Domain* d);
 const uint32_t* domain_wi(const Domain* d);
@@ -541,6 +542,14 @@ __global__ void k_batch_scale(char* __restrict__ base, size_t per, size_t o_pts,
   scale_point_glv(which ? pts + 16 : pts, gs, which ? pts + 128 : pts + 96);
 }
 
+// Proof k's H coefficient 2m-1 (always zero) becomes its -r s (block k), the scalar of the
+// delta_1 point that ends the H MSM's bases, as in the single-proof path.
+__global__ void k_batch_rs(char* __restrict__ base, size_t per, size_t o_rs, size_t o_M, size_t m) {
+  const uint32_t* rs = reinterpret_cast<const uint32_t*>(base + blockIdx.x * per + o_rs) + 16;
+  uint32_t* M = reinterpret_cast<uint32_t*>(base + blockIdx.x * per + o_M) + (2 * m - 1) * 8;
+  M[threadIdx.x] = rs[threadIdx.x];
+}
+
 // pi_C of every proof (block k) and the proof words to the caller's buffer.
 __global__ void k_batch_final(const BatchCall* __restrict__ calls, char* __restrict__ base, size_t per,
                               size_t o_pts) {
@@ -570,16 +579,17 @@ cudaError_t prove_batch_body(cs_ctx* ctx, cs_pk* pk, ProveBatch& B, Domain* dom1
   k_batch_scale<<<2 * K, 32, 0, sa>>>(base, B.per, B.o_pts, B.o_rs);
   note_launch();
   if ((e = batch_enqueue(B.g2, sb)) != cudaSuccess) { *where = "prove batch G2 MSMs"; return e; }
-  for (uint32_t i = 0; i < K; i++) {
-    uint32_t* M = B.at(i, B.o_M);
-    const bool ok = (e = qap_eval(pk->rows_a, B.at(i, B.o_wA), B.at(i, B.o_pA), 0, sh)) == cudaSuccess &&
-                    (e = qap_eval(pk->rows_b, B.at(i, B.o_wA), B.at(i, B.o_pB), 0, sh)) == cudaSuccess &&
-                    (e = hstep_reference_core(B.at(i, B.o_pA), B.at(i, B.o_pB), pk->log_m, domain_wf(dom2),
-                                              domain_wi(dom2), domain_wf(dom2), domain_consts(dom1) + 16,
-                                              domain_consts(dom2) + 24, M, B.at(i, B.o_hscr), sh)) == cudaSuccess &&
-                    (e = cudaMemcpyAsync(M + (size_t)(2 * m - 1) * 8, B.at(i, B.o_rs) + 16, 32,
-                                         cudaMemcpyDeviceToDevice, sh)) == cudaSuccess;
+  {  // the K QAP evaluations and H steps as batched launches (per-proof arrays B.per bytes apart)
+    const size_t stride = B.per / sizeof(uint32_t);
+    const bool ok =
+        (e = qap_eval(pk->rows_a, B.at(0, B.o_wA), B.at(0, B.o_pA), 0, sh, K, stride)) == cudaSuccess &&
+        (e = qap_eval(pk->rows_b, B.at(0, B.o_wA), B.at(0, B.o_pB), 0, sh, K, stride)) == cudaSuccess &&
+        (e = hstep_reference_core(B.at(0, B.o_pA), B.at(0, B.o_pB), pk->log_m, domain_wf(dom2), domain_wi(dom2),
+                                  domain_wf(dom2), domain_consts(dom1) + 16, domain_consts(dom2) + 24,
+                                  B.at(0, B.o_M), B.at(0, B.o_hscr), sh, K, stride)) == cudaSuccess;
     if (!ok) { *where = "prove batch QAP/H"; return e; }
+    k_batch_rs<<<K, 8, 0, sh>>>(base, B.per, B.o_rs, B.o_M, m);
+    note_launch();
   }
   if ((e = batch_enqueue(B.g1h, sh)) != cudaSuccess) { *where = "prove batch H MSMs"; return e; }
   cudaEventRecord(ctx->aux_ev[1], sa);

@@ -71,9 +71,11 @@ __global__ void k_row_scatter(const uint32_t* __restrict__ mpoly, uint32_t n_wir
 
 __global__ void k_qap_eval(const uint32_t* __restrict__ row_off, const uint32_t* __restrict__ wire,
                            const uint32_t* __restrict__ coeff, const uint32_t* __restrict__ w, uint32_t n_rows,
-                           int accumulate, uint32_t* __restrict__ out) {
+                           int accumulate, uint32_t* __restrict__ out, size_t stride) {
   const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n_rows) return;
+  w += (size_t)blockIdx.y * stride;  // instance y of a batch
+  out += (size_t)blockIdx.y * stride;
   Fr acc = accumulate ? ld_fp<ModR>(out + (size_t)c * 8) : Fr::zero();
   const uint32_t b = row_off[c], e = row_off[c + 1];
   for (uint32_t k = b; k < e; k++) acc = acc + ld_fp<ModR>(coeff + (size_t)k * 8) * ld_fp<ModR>(w + (size_t)wire[k] * 8);
@@ -118,10 +120,12 @@ cudaError_t qap_transpose(const uint32_t* d_mpoly, uint32_t n_wires, uint32_t n_
   return cudaGetLastError();
 }
 
-cudaError_t qap_eval(const QapRows& rows, const uint32_t* d_w, uint32_t* d_out, int accumulate, cudaStream_t st) {
-  if (rows.n_rows == 0) return cudaSuccess;
-  k_qap_eval<<<(rows.n_rows + 255) / 256, 256, 0, st>>>(rows.row_off, rows.wire, rows.coeff, d_w, rows.n_rows,
-                                                          accumulate, d_out);
+cudaError_t qap_eval(const QapRows& rows, const uint32_t* d_w, uint32_t* d_out, int accumulate, cudaStream_t st,
+                     uint32_t batch, size_t stride) {
+  if (rows.n_rows == 0 || batch == 0) return cudaSuccess;
+  if (batch > 65535) return cudaErrorInvalidValue;
+  k_qap_eval<<<dim3((rows.n_rows + 255) / 256, batch), 256, 0, st>>>(rows.row_off, rows.wire, rows.coeff, d_w,
+                                                                      rows.n_rows, accumulate, d_out, stride);
   note_launch();
   return cudaGetLastError();
 }

@@ -34,8 +34,9 @@ cudaError_t qap_transpose(const uint32_t* d_mpoly, uint32_t n_wires, uint32_t n_
                           uint32_t wire_lo, uint32_t wire_hi, uint32_t n_rows, QapRows& rows,
                           void* scratch, cudaStream_t st);
 
-// out[c] (+)= sum over row c of coeff * w[wire]; accumulate != 0 adds into out.
+// out[c] (+)= sum over row c of coeff * w[wire]; accumulate != 0 adds into out.  batch
+// instances: instance y reads w and writes out y * stride words further on.
 cudaError_t qap_eval(const QapRows& rows, const uint32_t* d_w, uint32_t* d_out, int accumulate,
-                     cudaStream_t st);
+                     cudaStream_t st, uint32_t batch = 1, size_t stride = 0);
 
 }  // namespace csb

@@ -1,7 +1,7 @@
 """Run one synthetic workload of the prover path and print its device times.
 
     python -m cusnarks_b200.run msm   --log-n 20 [--g2] [--fixed] [--window C] [--reps K]
-    python -m cusnarks_b200.run prove --log-m 20 [--no-fixed] [--reps K]
+    python -m cusnarks_b200.run prove --log-m 20 [--no-fixed] [--batch B] [--reps K]
     python -m cusnarks_b200.run ntt   --log-n 20 [--hstep reference|coset] [--reps K]
 
 Inputs are seeded: MSM scalars uniform in Fr, bases k_i * G (k_i seeded, built on the GPU);
@@ -64,13 +64,27 @@ def _prove(args, ctx):
     if not args.graphs:  # stage times need the launches themselves (graph replays carry none)
         ctx.set_prove_graphs(False)
     r, s = to_limbs(0x1234567890abcdef), to_limbs(0xfedcba0987654321)
-    d_proof = torch.zeros(64, dtype=torch.int32, device=torch.device("cuda", ctx.device))
+    dev = torch.device("cuda", ctx.device)
+    info = {"workload": "prove", "log_m": args.log_m, "fixed_windows": prover.fixed_windows()}
+    if args.batch > 1:  # B proofs of the same witness buffer with distinct r, s in one pass
+        d_proofs = torch.zeros((args.batch, 64), dtype=torch.int32, device=dev)
+        rs = [to_limbs(0x1234567890abcdef + i) for i in range(args.batch)]
+        ss = [to_limbs(0xfedcba0987654321 + i) for i in range(args.batch)]
+        torch.cuda.synchronize()
+
+        def call():
+            prover.prove_batch_device([circ.d_w.data_ptr()] * args.batch, rs, ss,
+                                      [d_proofs[i].data_ptr() for i in range(args.batch)])
+
+        info["batch"] = args.batch
+        call.keep = (circ, pk, prover, d_proofs)
+        return call, info
+    d_proof = torch.zeros(64, dtype=torch.int32, device=dev)
     torch.cuda.synchronize()
 
     def call():
         prover.prove_device(circ.d_w.data_ptr(), r, s, d_proof.data_ptr())
 
-    info = {"workload": "prove", "log_m": args.log_m, "fixed_windows": prover.fixed_windows()}
     call.keep = (circ, pk, prover, d_proof)
     return call, info
 
@@ -112,6 +126,8 @@ def main(argv=None):
     p.add_argument("--log-m", type=int, default=20)
     p.add_argument("--no-fixed", action="store_true", help="generic MSMs instead of fixed-base tables")
     p.add_argument("--graphs", action="store_true", help="replay the proof as a CUDA graph (no stage times)")
+    p.add_argument("--batch", type=int, default=1,
+                   help="B proofs with the key in one pass (cs_prove_batch_device, a CUDA graph); ms per pass")
     t = sub.add_parser("ntt")
     t.add_argument("--log-n", type=int, default=20)
     t.add_argument("--hstep", choices=["reference", "coset"], default=None)
@@ -134,7 +150,7 @@ def main(argv=None):
         rec = dict(info, rep=i, ms=round(ctx.last_ms, 4))
         if args.what == "msm":
             rec["accumulate_ms"] = round(ctx.last_phase_ms, 4)
-        if args.what == "prove" and not args.graphs:
+        if args.what == "prove" and not args.graphs and args.batch <= 1:
             rec["stages_ms"] = call.keep[2].stages()
         print(json.dumps(rec), flush=True)
     torch.cuda.profiler.stop()
