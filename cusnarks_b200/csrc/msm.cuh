@@ -68,8 +68,9 @@ struct MsmBatch {
   uint64_t lv_points = 0, lv2_points = 0;  // max over groups of W*(2^(c-1)/8+1), W*(.../64+1)
   const BatchGroup* groups = nullptr;  // host array
   uint32_t ngroups = 0;
-  int task = 64;
+  int task = 64;           // entries per accumulation task, kBatchMinTask..64 (set by the builder)
 };
+constexpr int kBatchMinTask = 8;
 size_t msm_batch_workspace_bytes(const MsmBatch& b, bool ec2);
 // An instance as a caller describes it (batch.cu builds the plan): fixed = a fixed-base table
 // built with `window`, which is then required.

@@ -92,7 +92,7 @@ struct BatchLayout {
 
 inline BatchLayout batch_layout(const MsmBatch& b, int xyzz_bytes) {
   const size_t nb = b.nbuckets, ne = b.nentries;
-  const size_t tl = kMinTask;
+  const size_t tl = (size_t)std::max(kBatchMinTask, std::min(b.task, kMaxTask));
   const size_t lv = b.lv_points, lv2 = b.lv2_points;
   BatchLayout L{};
   size_t o = 0;
@@ -129,9 +129,7 @@ cudaError_t batch_impl(const MsmBatch& b, void* d_work, size_t work_bytes, cudaS
   Task* tasks = reinterpret_cast<Task*>(base + L.tasks);
   Multi* multi = reinterpret_cast<Multi*>(base + L.multi);
   const uint32_t nb = b.nbuckets;
-  uint32_t task_len = (uint32_t)(b.task > 0 ? b.task : 64);
-  if (task_len < kMinTask) task_len = kMinTask;
-  if (task_len > (uint32_t)kMaxTask) task_len = kMaxTask;
+  const uint32_t task_len = (uint32_t)std::max(kBatchMinTask, std::min(b.task, kMaxTask));  // as the layout
   cudaError_t e;
   if ((e = cudaMemsetAsync(counters, 0, kCtrWords * sizeof(uint32_t), st)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(counts, 0, ((size_t)nb + 1) * sizeof(uint32_t), st)) != cudaSuccess) return e;
@@ -156,8 +154,17 @@ cudaError_t batch_impl(const MsmBatch& b, void* d_work, size_t work_bytes, cudaS
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_accumulate<F><<<accumulate_grid<F>(dev, sms), 128, 0, st>>>(tasks, counters, entries, nullptr, nb, buckets, partials,
-                                                           b.d_jobs);
+  // Latency form (one quad per task) when the tasks fill the quads at most four times over:
+  // four proofs of 2^12 constraints 2.96 -> 2.62 ms a batch; at eight or sixteen times over the
+  // thread form wins (sixteen proofs of 2^12: 4.03 vs 4.76 ms).
+  const uint64_t resident_threads = (uint64_t)accumulate_grid<F>(dev, sms) * 128;
+  const bool latency_mode = ((uint64_t)nb + b.nentries / task_len + 1) * 4 <= resident_threads * 4;
+  if (latency_mode)
+    k_accumulate_quad<F><<<accumulate_grid<F>(dev, sms), 128, 0, st>>>(tasks, counters, entries, nullptr, nb, buckets,
+                                                                  partials, b.d_jobs);
+  else
+    k_accumulate<F><<<accumulate_grid<F>(dev, sms), 128, 0, st>>>(tasks, counters, entries, nullptr, nb, buckets,
+                                                             partials, b.d_jobs);
   k_combine_small<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);
   k_combine<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);
   note_launch(3);

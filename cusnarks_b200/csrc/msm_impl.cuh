@@ -283,7 +283,7 @@ template <class F>
 __global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate_quad(
     const Task* __restrict__ tasks, const uint32_t* __restrict__ counters, const uint32_t* __restrict__ entries,
     const uint32_t* __restrict__ points, uint32_t nb, uint32_t* __restrict__ buckets,
-    uint32_t* __restrict__ partials) {
+    uint32_t* __restrict__ partials, const BatchJob* __restrict__ jobs = nullptr) {
   constexpr int PW = 2 * FieldWords<F>::value;
   constexpr int XW = 4 * FieldWords<F>::value;
   const uint32_t ntasks = counters[0];
@@ -294,18 +294,21 @@ __global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate_quad
     const uint32_t t = base + qw;
     const bool valid = t < ntasks;
     const Task tk = valid ? tasks[t] : Task{0, 0, 0, 0};
+    const uint32_t* pts = jobs && valid ? jobs[tk.job].points : points;  // read only where live
     const uint32_t steps = __reduce_max_sync(0xffffffffu, tk.len);
     XYZZ<F> acc = XYZZ<F>::inf();
 #pragma unroll 1
     for (uint32_t e = 0; e < steps; e++) {
       const bool live = e < tk.len;
-      Affine<F> p;
-      if (entries) {
-        const uint32_t ent = live ? entries[tk.start + e] : 0u;
-        p = ld_affine<F>(points + (size_t)(ent & ~NEG_BIT) * PW);
-        if (ent & NEG_BIT) p.y = p.y.neg();
-      } else {
-        p = ld_affine<F>(points + (size_t)(live ? tk.start + e : 0u) * PW);
+      Affine<F> p{F::zero(), F::zero()};  // past the task's end: not taken
+      if (live) {
+        if (entries) {
+          const uint32_t ent = entries[tk.start + e];
+          p = ld_affine<F>(pts + (size_t)(ent & ~NEG_BIT) * PW);
+          if (ent & NEG_BIT) p.y = p.y.neg();
+        } else {
+          p = ld_affine<F>(pts + (size_t)(tk.start + e) * PW);
+        }
       }
       const XYZZ<F> nxt = xyzz_madd_quad(acc, p);
       const bool take = live && (entries || !(p.x.is_zero() && p.y.is_zero()));

@@ -245,7 +245,8 @@ int cs_msm_fixed_device(cs_ctx *ctx, int ec2, const uint32_t *d_scalars, const u
  * cost-model default.  cs_msm_batch_run is asynchronous on the context stream; use_graph != 0
  * captures the sequence into a CUDA graph on the first run and replays it afterwards (the
  * plan's pointers are baked in: change inputs in place).  task = bucket tile (max entries
- * per accumulation task, 32..64; 0 = 64).  Each result equals cs_msm_device's. */
+ * per accumulation task, 8..64; 0 = by the batch's size: about one task per resident
+ * accumulation thread, 8..64).  Each result equals cs_msm_device's. */
 typedef struct {
   const uint32_t *scalars, *points;
   uint32_t *out;

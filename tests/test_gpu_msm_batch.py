@@ -56,12 +56,15 @@ def _single(ctx, ds, dp, n, w, ec2):
     return out.cpu().numpy().view(np.uint32).copy()
 
 
+@pytest.mark.parametrize("task", [0, 8, 64])
 @pytest.mark.parametrize("ec2", [False, True])
-def test_batch_equals_single_and_oracle(ctx, oracle, ec2):
+def test_batch_equals_single_and_oracle(ctx, oracle, ec2, task):
+    """task 0: the tile the batch's size picks (8 here: small instances); 8: buckets split
+    into many partial sums; 64: few splits."""
     sizes = [0, 1, 3, 100, 1000, 2048, 1 << 13, 1 << 15] if not ec2 else [5, 0, 300, 2048, 1 << 12]
     windows = [0, 0, 5, 0, 9, 0, 12, 0] if not ec2 else [0, 7, 0, 11, 0]
     ins, jobs = _case(ctx, sizes, windows, ec2, seed=7 if ec2 else 3)
-    batch = ctx.msm_batch(jobs, ec2=ec2)
+    batch = ctx.msm_batch(jobs, ec2=ec2, task=task)
     try:
         got = []
         for mode in (False, True, True):          # direct, capture + launch, replay
