@@ -70,8 +70,8 @@ UNIT = "proofs/s (2^20 constraints)"
 PRODUCTS_PER_MONT = 136
 MONT_PER_MADD = 11     # mixed addition, 7M + 4S (the canonical count of the MSM cost model)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_accumulate launch of
-# the 2^20 G1 MSM (window 16), from an ncu capture of that launch
-ACC_TRAFFIC_BYTES = 439_780_864 + 60_918_784
+# the 2^20 G1 MSM (GLV split, window 16), from an ncu capture of that launch
+ACC_TRAFFIC_BYTES = 847_947_264 + 39_934_976
 L2_BYTES = 126 * 1024 * 1024
 LOG_M = 20
 R_INT, S_INT = 0x1234567890abcdef, 0xfedcba0987654321
@@ -265,9 +265,11 @@ class MsmWorkload:
         return self.ctx.last_ms, self.ctx.last_phase_ms
 
     def dominant_units(self):
+        """Bucket entries of one launch: the G1 MSM splits each scalar by GLV into two
+        half-scalars below 2^127, so 2n terms of ceil(128 / c) windows."""
         from cusnarks_b200._lib import lib
         c = lib().cs_msm_default_window(self.n, 0)
-        return self.n * lib().cs_msm_num_windows(c), c
+        return 2 * self.n * (-(-128 // c)), c
 
 
 def sharded_msm_leg(ctx, world, rank, reps: int, log_n: int = 20, seed: int = 7):
@@ -591,7 +593,7 @@ def run_ours(args, world, rank, local):
                      "unit": "T wide products/s", "frac": round(achieved / peak_wide, 4),
                      "traffic": ACC_TRAFFIC_BYTES, "kernel_ms": round(acc, 4), "units_per_launch": units,
                      "window": window,
-                     "basis": "2^20 G1 MSM: N*W bucket entries x 11 Montgomery products x 136 32x32->64 "
+                     "basis": "2^20 G1 MSM: 2N*ceil(128/c) bucket entries (GLV half-scalars) x 11 Montgomery products x 136 32x32->64 "
                               "products / kernel ms (CUDA events around the kernels); peak = live "
                               "mad.wide.u32 rate (cs_bench_pipe mode 3), the ceiling of a 32-bit CIOS "
                               "product (this kernel computes products in radix 2^52 on the FP64 pipe); "

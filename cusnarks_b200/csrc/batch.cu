@@ -34,7 +34,7 @@ int pick_window(int dev, int ec2, uint32_t n) {
     const int w = g_tuned[dev][ec2 ? 1 : 0][ceil_log2(n < 1 ? 1 : n)];
     if (w) return w;
   }
-  return csb::msm_default_window(n ? n : 1, ec2 != 0);
+  return csb::msm_window_model(n ? n : 1, false);  // batch instances sort full scalars
 }
 
 // Pseudo-random limbs for timing runs (splitmix-style hash); top limb masked below 2^253 so
@@ -269,14 +269,17 @@ int cs_msm_autotune(cs_ctx* ctx, int ec2, uint32_t log_min, uint32_t log_max, in
     if (e == cudaSuccess) e = cudaEventCreate(&z);
     for (uint32_t L = log_min; L <= log_max && e == cudaSuccess; L++) {
       const uint32_t n = 1u << L;
-      const int c0 = csb::msm_default_window(n, ec2 != 0);
+      // the form a batch instance runs: full scalars (single G1 MSMs split them by GLV and
+      // keep the cost model's window)
+      const int c0 = csb::msm_window_model(n, false);
       float best = 1e30f;
       int bw = c0;
       for (int c = std::max(4, c0 - 2); c <= std::min(22, c0 + 2) && e == cudaSuccess; c++) {
-        e = ctx->work.reserve(csb::msm_workspace_bytes(n, c, ec2 != 0), ctx->stream);
+        e = ctx->work.reserve(csb::msm_workspace_bytes(n, c, ec2 != 0, -1, 0), ctx->stream);
         if (e != cudaSuccess) break;
         csb::MsmConfig cfg;
         cfg.c = c;
+        cfg.glv = 0;
         float t_best = 1e30f;
         for (int rep = 0; rep < 3 && e == cudaSuccess; rep++) {
           cudaEventRecord(a, ctx->stream);

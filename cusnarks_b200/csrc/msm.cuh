@@ -87,8 +87,9 @@ cudaError_t msm_batch_g2(const MsmBatch& b, void* d_work, size_t work_bytes, cud
 
 struct MsmConfig {
   int c = 0;          // window bits; 0 = pick from N
-  int task = 64;      // max points per accumulation task
+  int task = 0;       // max points per accumulation task, 32..96 (0: 64, or 96 for buckets of 48+)
   int affine = -1;    // batch-affine halving rounds before the XYZZ accumulation: -1 auto, 0 off
+  int glv = -1;       // generic G1 MSMs: split the scalars by the GLV endomorphism (-1 auto = on, 0 off)
   // optional events recorded around the bucket-accumulation kernels (phase timing)
   cudaEvent_t acc_start = nullptr, acc_stop = nullptr;
   // Two fixed-base MSMs with the same window whose sums are added (a proof's C and H terms)
@@ -103,8 +104,12 @@ struct MsmConfig {
 
 // Bytes of device scratch one MSM of n terms needs (G2 when ec2).
 // affine_mode: batch-affine rounds the MSM will run (-1 automatic, 0 none, > 0 that many).
-size_t msm_workspace_bytes(uint32_t n, int c, bool ec2, int affine_mode = -1);
+// glv_mode: as MsmConfig::glv (G1 only).
+size_t msm_workspace_bytes(uint32_t n, int c, bool ec2, int affine_mode = -1, int glv_mode = -1);
+// Window for n terms: G1 for the GLV split (2n terms of 128 bits), G2 for n of 254 bits.
 int msm_default_window(uint32_t n, bool ec2);
+// The cost model's window for n terms with (glv) or without the GLV split.
+int msm_window_model(uint32_t n, bool glv);
 
 // d_scalars: n x 8 words (normal form), d_points: n affine points (16 or 32 words),
 // d_out: one affine point (16 or 32 words), d_work: msm_workspace_bytes() bytes,

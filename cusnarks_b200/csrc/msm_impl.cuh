@@ -5,6 +5,7 @@
 #include <atomic>
 #include "msm.cuh"
 #include "curve.cuh"
+#include "glv.cuh"
 #include "scan.cuh"
 #include "runtime.cuh"
 
@@ -13,9 +14,17 @@ namespace msm_detail {
 
 constexpr int SCALAR_BITS = 254;  // scalars are reduced below r < 2^254 first
 constexpr uint32_t NEG_BIT = 0x80000000u;
+// Generic G1 MSMs with the GLV split: an entry of the k2 half reads phi(P_i) = (beta x_i, y_i)
+// (terms below 2^30).
+constexpr uint32_t PHI_BIT = 0x40000000u;
 constexpr uint32_t kMinTask = 32;  // workspace bounds assume tasks of at least this size
 
 __host__ __device__ inline int num_windows(int c) { return SCALAR_BITS / c + 1; }
+// Windows of a GLV half-scalar (|k1|, |k2| < 2^127): c W >= 128 leaves the top digit at most
+// 2^(c-1) after the signed recoding's carry, so no further window is needed.
+__host__ __device__ inline int glv_windows(int c) { return (128 + c - 1) / c; }
+// Window count of an MSM: generic G1 MSMs split their scalars by the endomorphism (glv).
+__host__ __device__ inline int msm_windows(int c, bool glv) { return glv ? glv_windows(c) : num_windows(c); }
 
 // k <- k mod r for any 256-bit k (at most 5 subtractions since 2^256 / r < 6)
 CSB_DEV void scalar_reduce(uint32_t (&k)[8]) {
@@ -114,6 +123,95 @@ __global__ void k_scatter(const uint32_t* __restrict__ scalars, const uint32_t* 
   });
 }
 
+// GLV split of a generic G1 MSM: k_i P_i = k1 P_i + k2 phi(P_i) with k_i = k1 + k2 lambda
+// (mod r), |k1|, |k2| < 2^127, so the pipeline sorts 2n half-size scalars: half the windows,
+// half the bucket sets to reduce and half the window Horner.  k_glv_prep writes, per term,
+// s2[i] = |k1| (words 0-3) and |k2| (words 4-7) with each half's sign in bit 31 of its top
+// word (zero halves for a zero scalar or a point at infinity), and phix[i] = beta x_i.  The
+// points themselves are not copied: an entry of the k2 half carries PHI_BIT and reads x from
+// phix and y from P_i, so the gathered set stays the n input points plus n x-coordinates.
+template <class F>
+__global__ void k_glv_prep(const uint32_t* __restrict__ scalars, const uint32_t* __restrict__ points, uint32_t n,
+                           uint32_t* __restrict__ s2, uint32_t* __restrict__ phix) {
+  constexpr int PW = 2 * FieldWords<F>::value;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t k[8];
+  ld_limbs8(k, scalars + (size_t)i * 8);
+  scalar_reduce(k);
+  const uint32_t* P = points + (size_t)i * PW;
+  uint32_t k1[4] = {0, 0, 0, 0}, k2[4] = {0, 0, 0, 0}, neg1 = 0, neg2 = 0;
+  const bool zero = (k[0] | k[1] | k[2] | k[3] | k[4] | k[5] | k[6] | k[7]) == 0;
+  if (!zero && !point_is_inf<F>(P)) {
+    const uint64_t kk[4] = {k[0] | (uint64_t)k[1] << 32, k[2] | (uint64_t)k[3] << 32, k[4] | (uint64_t)k[5] << 32,
+                            k[6] | (uint64_t)k[7] << 32};
+    glv::split_reduced(kk, k1, &neg1, k2, &neg2);
+  }
+  uint4* o = reinterpret_cast<uint4*>(s2 + (size_t)i * 8);
+  o[0] = make_uint4(k1[0], k1[1], k1[2], k1[3] | (neg1 << 31));
+  o[1] = make_uint4(k2[0], k2[1], k2[2], k2[3] | (neg2 << 31));
+  F x, beta;
+  ld_field(x, P);
+  glv::beta_mont(beta.v);
+  st_field(phix + (size_t)i * 8, x * beta);
+}
+
+// Digits of both halves of a split term: f(half, window, |d|, negative), the half's sign
+// folded into the digit's.
+template <class Fn>
+CSB_DEV void for_each_glv_digit(const uint32_t (&t)[8], int c, int W, Fn f) {
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const uint32_t k[8] = {t[4 * h], t[4 * h + 1], t[4 * h + 2], t[4 * h + 3] & 0x7fffffffu, 0u, 0u, 0u, 0u};
+    const bool sgn = (t[4 * h + 3] >> 31) != 0;
+    for_each_digit(k, c, W, [&](int j, uint32_t mag, bool neg) { f(h, j, mag, neg != sgn); });
+  }
+}
+
+template <class F>
+__global__ void k_count_glv(const uint32_t* __restrict__ s2, uint32_t n, int c, int W, uint32_t* __restrict__ counts) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t t[8];
+  ld_limbs8(t, s2 + (size_t)i * 8);
+  const uint32_t B = 1u << (c - 1);
+  for_each_glv_digit(t, c, W, [&](int, int j, uint32_t mag, bool) { atomicAdd(&counts[(size_t)j * B + (mag - 1)], 1u); });
+}
+
+template <class F>
+__global__ void k_scatter_glv(const uint32_t* __restrict__ s2, uint32_t n, int c, int W, uint32_t* __restrict__ cursor,
+                              uint32_t* __restrict__ entries) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t t[8];
+  ld_limbs8(t, s2 + (size_t)i * 8);
+  const uint32_t B = 1u << (c - 1);
+  for_each_glv_digit(t, c, W, [&](int h, int j, uint32_t mag, bool neg) {
+    const uint32_t pos = atomicAdd(&cursor[(size_t)j * B + (mag - 1)], 1u);
+    entries[pos] = i | (h ? PHI_BIT : 0u) | (neg ? NEG_BIT : 0u);
+  });
+}
+
+// The base of an entry: P_i, or phi(P_i) = (phix[i], y_i) for a GLV k2 entry (phix given).
+// One load path either way (the x address is selected), so lanes of a warp that read P and
+// phi(P) do not diverge.
+template <class F>
+CSB_DEV Affine<F> ld_entry_point(const uint32_t* base, const uint32_t* phix, uint32_t ent) {
+  constexpr int FW = FieldWords<F>::value;
+  constexpr int PW = 2 * FW;
+  if constexpr (FW == 8) {
+    const bool phi = phix != nullptr && (ent & PHI_BIT) != 0;
+    const uint32_t i = ent & ~(NEG_BIT | (phix ? PHI_BIT : 0u));
+    const uint32_t* xp = phi ? phix + (size_t)i * 8 : base + (size_t)i * PW;
+    Affine<F> p;
+    ld_field(p.x, xp);
+    ld_field(p.y, base + (size_t)i * PW + FW);
+    return p;
+  } else {
+    return ld_affine<F>(base + (size_t)(ent & ~NEG_BIT) * PW);
+  }
+}
+
 // Task record: entries [start, start+len) summed into dst.  dst < nb: bucket index;
 // dst >= nb: partial slot (dst - nb).  job: the instance whose bases the entries index (a
 // batch of MSMs shares one task list; 0 for a single MSM).
@@ -136,7 +234,7 @@ struct Multi {
 
 // Task lengths are in [1, TASK]; tasks are emitted in descending length (a counting sort
 // over TASK+1 bins) so the 32 lanes of a warp walk buckets of nearly equal size.
-constexpr int kMaxTask = 64;
+constexpr int kMaxTask = 96;
 
 // Pass 1: per bucket, histogram of its task lengths; empty buckets become infinity.
 template <class F>
@@ -245,7 +343,8 @@ __global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate(cons
                                                     const uint32_t* __restrict__ points, uint32_t nb,
                                                     uint32_t* __restrict__ buckets,
                                                     uint32_t* __restrict__ partials,
-                                                    const BatchJob* __restrict__ jobs = nullptr) {
+                                                    const BatchJob* __restrict__ jobs = nullptr,
+                                                    const uint32_t* __restrict__ phix = nullptr) {
   constexpr int PW = 2 * FieldWords<F>::value;
   constexpr int XW = 4 * FieldWords<F>::value;
   const uint32_t ntasks = counters[0];
@@ -257,7 +356,7 @@ __global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate(cons
 #pragma unroll 1
       for (uint32_t e = 0; e < tk.len; e++) {
         const uint32_t ent = entries[tk.start + e];
-        Affine<F> p = ld_affine<F>(base + (size_t)(ent & ~NEG_BIT) * PW);
+        Affine<F> p = ld_entry_point<F>(base, phix, ent);
         if (ent & NEG_BIT) p.y = p.y.neg();
         acc = madd_acc(acc, p);
       }
@@ -283,7 +382,8 @@ template <class F>
 __global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate_quad(
     const Task* __restrict__ tasks, const uint32_t* __restrict__ counters, const uint32_t* __restrict__ entries,
     const uint32_t* __restrict__ points, uint32_t nb, uint32_t* __restrict__ buckets,
-    uint32_t* __restrict__ partials, const BatchJob* __restrict__ jobs = nullptr) {
+    uint32_t* __restrict__ partials, const BatchJob* __restrict__ jobs = nullptr,
+    const uint32_t* __restrict__ phix = nullptr) {
   constexpr int PW = 2 * FieldWords<F>::value;
   constexpr int XW = 4 * FieldWords<F>::value;
   const uint32_t ntasks = counters[0];
@@ -304,7 +404,7 @@ __global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate_quad
       if (live) {
         if (entries) {
           const uint32_t ent = entries[tk.start + e];
-          p = ld_affine<F>(pts + (size_t)(ent & ~NEG_BIT) * PW);
+          p = ld_entry_point<F>(pts, phix, ent);
           if (ent & NEG_BIT) p.y = p.y.neg();
         } else {
           p = ld_affine<F>(pts + (size_t)(tk.start + e) * PW);
@@ -865,25 +965,28 @@ static __global__ void k_half_counts(const uint32_t* __restrict__ off, uint32_t 
 
 // --------------------------------------------------------------- workspace layout ----
 // counters block: [0] tasks, [1] partial slots, [2] split buckets; hist at +16 and
-// bin cursors at +96 (kMaxTask + 1 words each).
-constexpr int kCtrHist = 16, kCtrCursor = 96, kCtrWords = 192;
+// bin cursors at +128 (kMaxTask + 1 words each).
+constexpr int kCtrHist = 16, kCtrCursor = 128, kCtrWords = 256;
+static_assert(kCtrHist + kMaxTask + 1 <= kCtrCursor && kCtrCursor + kMaxTask + 1 <= kCtrWords,
+              "task-length bins must not overlap");
 // the reduction adds levels until a window has at most this many segments
 constexpr uint32_t kTopSegments = 256;
 
 struct Layout {
   size_t counts, offsets, entries, tasks, multi, partials, buckets, lv_y, lv_z, lv_y2, lv_z2, wsum,
-      counters, off2, pa, pb, pref, total;
-  bool affine;
+      counters, off2, pa, pb, pref, glv_s, glv_p, total;
+  bool affine, glv;
 };
 
 static inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 inline Layout make_layout(uint32_t n, int c, int xyzz_bytes, uint32_t task_len, bool fixed = false,
-                          bool affine = true) {
-  const int W = num_windows(c);
+                          bool affine = true, bool glv = false) {
+  const int W = msm_windows(c, glv);
+  const size_t nt = glv ? 2 * (size_t)n : n;  // terms the pipeline sorts (GLV: k1 P_i and k2 phi(P_i))
   const size_t nb = fixed ? ((size_t)1 << (c - 1)) : (size_t)W << (c - 1);
   const int WR = fixed ? 1 : W;  // bucket sets reduced
-  const size_t ne = (size_t)n * W;
+  const size_t ne = nt * W;
   const size_t max_tasks = nb + ne / task_len + 1;
   const size_t max_partials = 2 * (ne / task_len) + 1;
   const size_t n1 = ((size_t)1 << (c - 1)) / 8 + 1;
@@ -903,6 +1006,11 @@ inline Layout make_layout(uint32_t n, int c, int xyzz_bytes, uint32_t task_len, 
   L.lv_y2 = o;    o = align256(o + n2 * xyzz_bytes);
   L.lv_z2 = o;    o = align256(o + n2 * xyzz_bytes);
   L.wsum = o;     o = align256(o + (size_t)WR * xyzz_bytes);
+  L.glv = glv;
+  if (glv) {  // per term: both split halves (8 words) and beta x_i (8 words)
+    L.glv_s = o;  o = align256(o + (size_t)n * 32);
+    L.glv_p = o;  o = align256(o + (size_t)n * 32);
+  }
   L.affine = affine;
   if (affine) {  // batch-affine rounds: offsets ping-pong, two point arrays, prefix products
     const size_t pb = (size_t)xyzz_bytes / 2, fb = (size_t)xyzz_bytes / 4;
@@ -941,11 +1049,17 @@ inline int auto_affine_rounds(uint32_t n, int W, size_t nb) {
   return auto_affine_rounds_rt(FieldWords<F>::value == 16, n, W, nb);
 }
 // Whether an MSM reserves the round buffers: affine_mode -1 auto, 0 never, > 0 that many rounds.
-inline bool layout_affine(bool ec2, int affine_mode, uint32_t n, int c, bool fixed) {
+inline bool layout_affine(bool ec2, int affine_mode, uint32_t n, int c, bool fixed, bool glv = false) {
   if (affine_mode >= 0) return affine_mode > 0;
-  const int W = num_windows(c);
+  const int W = msm_windows(c, glv);
   const size_t nb = fixed ? ((size_t)1 << (c - 1)) : (size_t)W << (c - 1);
-  return auto_affine_rounds_rt(ec2, n, W, nb) > 0;
+  return auto_affine_rounds_rt(ec2, glv ? 2 * n : n, W, nb) > 0;
+}
+// Whether an MSM splits its scalars by the GLV endomorphism: generic G1 MSMs unless turned off.
+// Batch-affine rounds (asked for explicitly; G1 runs none by default) read plain point indices,
+// so they turn the split off.
+inline bool use_glv(bool ec2, bool fixed, int glv_mode, int affine_mode, uint32_t n) {
+  return !ec2 && !fixed && glv_mode != 0 && affine_mode <= 0 && n < PHI_BIT;
 }
 
 // Resident blocks of k_accumulate per SM, cached per device (callers on several threads and
@@ -983,29 +1097,29 @@ void reduce_level(const uint32_t* y, const uint32_t* z, uint32_t n, uint32_t nou
 // One MSM.  Generic: d_points holds n points.  FIXED: d_points is a table of W*n points,
 // T[j*n + i] = 2^(c j) P_i, built with the same c (fixed_table_impl).
 template <class F, bool FIXED>
-cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32_t n,
+cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32_t n_in,
                      uint32_t* d_out, void* d_work, size_t work_bytes, const MsmConfig& cfg,
                      cudaStream_t st) {
   constexpr bool EC2 = FieldWords<F>::value == 16;
   constexpr int XB = 4 * FieldWords<F>::value * 4;  // bytes per XYZZ point
   // shared buckets: fixed-base MSMs (one bucket set) with terms (the accumulation is what
   // writes every bucket of the array)
-  if ((cfg.bucket_out || cfg.bucket_add) && (!FIXED || n == 0)) return cudaErrorInvalidValue;
+  if ((cfg.bucket_out || cfg.bucket_add) && (!FIXED || n_in == 0)) return cudaErrorInvalidValue;
   if (cfg.bucket_out && cfg.bucket_add) return cudaErrorInvalidValue;
-  if (n == 0) {
+  if (n_in == 0) {
     k_store_inf<F><<<1, 32, 0, st>>>(d_out);
     note_launch();
     return cudaGetLastError();
   }
   if (FIXED && cfg.c <= 0) return cudaErrorInvalidValue;  // the table fixes the window
-  const int c = cfg.c > 0 ? cfg.c : msm_default_window(n, EC2);
+  const int c = cfg.c > 0 ? cfg.c : msm_default_window(n_in, EC2);
   if (c < 4 || c > 24) return cudaErrorInvalidValue;
-  uint32_t task_len = cfg.task > 0 ? (uint32_t)cfg.task : 64u;
-  if (task_len < kMinTask) task_len = kMinTask;
-  if (task_len > (uint32_t)kMaxTask) task_len = kMaxTask;
-  const int W = num_windows(c);
+  uint32_t task_len = cfg.task > 0 ? (uint32_t)cfg.task : 64u;  // automatic: 64, or 96 below
+  const bool glv = use_glv(EC2, FIXED, cfg.glv, cfg.affine, n_in);
+  const int W = msm_windows(c, glv);
   // entry positions are uint32 and fixed-base entries carry a table index below the sign bit
-  if ((uint64_t)W * n >= (uint64_t)NEG_BIT) return cudaErrorInvalidValue;
+  if ((uint64_t)W * n_in * (glv ? 2 : 1) >= (uint64_t)NEG_BIT) return cudaErrorInvalidValue;
+  const uint32_t n = glv ? 2 * n_in : n_in;  // terms sorted into buckets
   const uint32_t nb = FIXED ? (1u << (c - 1)) : (uint32_t)W << (c - 1);
   const int rounds_req = cfg.affine < 0 ? auto_affine_rounds<F>(n, W, nb) : cfg.affine;
   int dev = 0, sms = 148;
@@ -1015,8 +1129,14 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   // four times over runs in latency form (one quad per task, shortest tasks)
   const uint64_t resident = (uint64_t)accumulate_grid<F>(dev, sms) * 128;
   const bool latency_mode = rounds_req == 0 && ((uint64_t)nb + (uint64_t)n * W / kMinTask + 1) * 4 <= resident;
+  // Automatic tile: 96 entries where buckets average 48 or more (a GLV-split 2^20 MSM averages
+  // 64: tiles of 64 split half its buckets and the partial sums cost a combine pass; 2^20
+  // 5.16 -> 5.07 ms, 2^22 17.8 -> 17.3 ms), else 64; the latency form the shortest.
+  if (cfg.task <= 0 && (uint64_t)n * W >= 48ull * nb) task_len = 96;
+  if (task_len < kMinTask) task_len = kMinTask;
+  if (task_len > (uint32_t)kMaxTask) task_len = kMaxTask;
   if (latency_mode) task_len = kMinTask;
-  const Layout L = make_layout(n, c, XB, kMinTask, FIXED, layout_affine(EC2, cfg.affine, n, c, FIXED));
+  const Layout L = make_layout(n_in, c, XB, kMinTask, FIXED, layout_affine(EC2, cfg.affine, n_in, c, FIXED, glv), glv);
   if (work_bytes < L.total || d_work == nullptr) return cudaErrorInvalidValue;
   char* base = static_cast<char*>(d_work);
   uint32_t* counters = reinterpret_cast<uint32_t*>(base + L.counters);
@@ -1035,16 +1155,30 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   void* scan_tmp = base + (L.total - scan_workspace_bytes(nb + 1));
 
   cudaError_t e;
+  const int T = 256;
+  uint32_t* glv_s = glv ? reinterpret_cast<uint32_t*>(base + L.glv_s) : nullptr;
+  const uint32_t* phix = glv ? reinterpret_cast<uint32_t*>(base + L.glv_p) : nullptr;
+  if constexpr (!EC2 && !FIXED) {
+    if (glv) {
+      k_glv_prep<F><<<(n_in + T - 1) / T, T, 0, st>>>(d_scalars, d_points, n_in, glv_s, const_cast<uint32_t*>(phix));
+      note_launch();
+    }
+  }
   if ((e = cudaMemsetAsync(counters, 0, kCtrWords * sizeof(uint32_t), st)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(counts, 0, (nb + 1) * sizeof(uint32_t), st)) != cudaSuccess) return e;
-  const int T = 256;
-  k_count<F, FIXED><<<(n + T - 1) / T, T, 0, st>>>(d_scalars, d_points, n, c, W, counts);
+  if (glv)
+    k_count_glv<F><<<(n_in + T - 1) / T, T, 0, st>>>(glv_s, n_in, c, W, counts);
+  else
+    k_count<F, FIXED><<<(n + T - 1) / T, T, 0, st>>>(d_scalars, d_points, n, c, W, counts);
   note_launch();
   if ((e = scan_exclusive_u32(counts, offsets, nb + 1, scan_tmp, st)) != cudaSuccess) return e;
   // counts is reused as the scatter cursor
   if ((e = cudaMemcpyAsync(counts, offsets, nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
     return e;
-  k_scatter<F, FIXED><<<(n + T - 1) / T, T, 0, st>>>(d_scalars, d_points, n, c, W, counts, entries);
+  if (glv)
+    k_scatter_glv<F><<<(n_in + T - 1) / T, T, 0, st>>>(glv_s, n_in, c, W, counts, entries);
+  else
+    k_scatter<F, FIXED><<<(n + T - 1) / T, T, 0, st>>>(d_scalars, d_points, n, c, W, counts, entries);
   note_launch();
   // batch-affine halving rounds (counts is free again and holds the halved counts)
   const uint32_t* acc_entries = entries;
@@ -1089,10 +1223,10 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   if (cfg.acc_start) cudaEventRecord(cfg.acc_start, st);
   if (latency_mode)
     k_accumulate_quad<F><<<accumulate_grid<F>(dev, sms), 128, 0, st>>>(tasks, counters, acc_entries, acc_points, nb,
-                                                                  buckets, partials);
+                                                                  buckets, partials, nullptr, phix);
   else
     k_accumulate<F><<<accumulate_grid<F>(dev, sms), 128, 0, st>>>(tasks, counters, acc_entries, acc_points, nb,
-                                                             buckets, partials);
+                                                             buckets, partials, nullptr, phix);
   note_launch();
   k_combine_small<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);
   k_combine<F><<<sms * 4, 128, 0, st>>>(multi, counters, partials, buckets);

@@ -28,6 +28,7 @@
 #include "curve.cuh"
 #include "msm.cuh"
 #include "ntt.cuh"
+#include "glv.cuh"
 #include "qap.cuh"
 #include "runtime.cuh"
 
@@ -111,67 +112,15 @@ __global__ void k_neg_rs(const uint32_t* __restrict__ r, const uint32_t* __restr
   st_fp<ModR>(dst, Fr::zero() - rm * ld_fp<ModR>(s));
 }
 
-// ---- k * P through the GLV endomorphism of BN254 G1: phi(x, y) = (beta x, y) = lambda P
-// with beta^3 = 1 in Fq and lambda^2 + lambda + 1 = 0 in Fr.  k = k1 + k2 lambda (mod r) with
-// |k1|, |k2| < 2^127 from the short lattice basis (a1, b1), (a2, b2) of
-// {(x, y) : x + y lambda = 0 mod r} (extended Euclid on (r, lambda); b2 = a1, b1 < 0):
-//   c1 = round(b2 k / r), c2 = round(-b1 k / r) (as (k g1) >> 256, (k g2) >> 256),
-//   k1 = k - c1 a1 - c2 a2,  k2 = c1 |b1| - c2 b2.
-// Then k P = k1 P + k2 phi(P): 127 joint doublings instead of 254.
+// ---- k * P through the GLV endomorphism of BN254 G1 (glv.cuh): k = k1 + k2 lambda (mod r),
+// |k1|, |k2| < 2^127, and k P = k1 P + k2 phi(P): 127 joint doublings instead of 254.
 struct GlvSplit {
   uint32_t k1[4], k2[4];  // magnitudes, little-endian
   uint32_t neg1, neg2, pad[6];
 };
 
-namespace glv {
-constexpr uint64_t G1C[2] = {0xd91d232ec7e0b3d7ull, 0x2ull};
-constexpr uint64_t G2C[3] = {0x7a7bd9d4391eb18eull, 0x4ccef014a773d2cfull, 0x2ull};
-constexpr uint64_t A1 = 0x89d3256894d213e3ull;                                  // = b2
-constexpr uint64_t A2[2] = {0x0be4e1541221250bull, 0x6f4d8248eeb859fdull};
-constexpr uint64_t B1ABS[2] = {0x8211bbeb7d4f1128ull, 0x6f4d8248eeb859fcull};
-
-typedef unsigned __int128 u128;
-
-// r = a * b for little-endian 64-bit limb vectors, into an na + nb limb result
-inline void mul(const uint64_t* a, int na, const uint64_t* b, int nb, uint64_t* r) {
-  for (int i = 0; i < na + nb; i++) r[i] = 0;
-  for (int i = 0; i < na; i++) {
-    u128 c = 0;
-    for (int j = 0; j < nb; j++) {
-      c += (u128)a[i] * b[j] + r[i + j];
-      r[i + j] = (uint64_t)c;
-      c >>= 64;
-    }
-    r[i + nb] = (uint64_t)c;
-  }
-}
-// acc (4 limbs, mod 2^256) += sign * v (up to 4 limbs)
-inline void addsub(uint64_t* acc, const uint64_t* v, int nv, bool sub) {
-  u128 c = sub ? 1 : 0;  // two's complement: acc + ~v + 1
-  for (int i = 0; i < 4; i++) {
-    const uint64_t w = i < nv ? v[i] : 0;
-    c += (u128)acc[i] + (sub ? ~w : w);
-    acc[i] = (uint64_t)c;
-    c >>= 64;
-  }
-}
-inline void to_mag(const uint64_t* v, uint32_t* mag, uint32_t* neg) {
-  uint64_t t[4] = {v[0], v[1], v[2], v[3]};
-  *neg = (t[3] >> 63) ? 1u : 0u;
-  if (*neg) {  // negate
-    u128 c = 1;
-    for (int i = 0; i < 4; i++) {
-      c += (u128)(~t[i]);
-      t[i] = (uint64_t)c;
-      c >>= 64;
-    }
-  }
-  for (int i = 0; i < 2; i++) {  // |k1|, |k2| < 2^127
-    mag[2 * i] = (uint32_t)t[i];
-    mag[2 * i + 1] = (uint32_t)(t[i] >> 32);
-  }
-}
-
+namespace glv_host {
+using namespace csb::glv;
 // k mod r for any 256-bit k (at most 5 subtractions)
 inline void reduce_r(uint64_t* k) {
   static constexpr uint64_t R[4] = {0x43e1f593f0000001ull, 0x2833e84879b97091ull, 0xb85045b68181585dull,
@@ -190,36 +139,19 @@ inline GlvSplit split(const uint32_t* k32) {
   uint64_t k[4];
   for (int i = 0; i < 4; i++) k[i] = (uint64_t)k32[2 * i] | ((uint64_t)k32[2 * i + 1] << 32);
   reduce_r(k);
-  uint64_t p1[6], p2[7];
-  mul(k, 4, G1C, 2, p1);
-  mul(k, 4, G2C, 3, p2);
-  const uint64_t c1[1] = {p1[4]};            // < 2^64
-  const uint64_t c2[2] = {p2[4], p2[5]};     // < 2^128
-  uint64_t t[4];
-  uint64_t k1[4] = {k[0], k[1], k[2], k[3]}, k2[4] = {0, 0, 0, 0};
-  mul(c1, 1, &A1, 1, t);                     // c1 a1 (2 limbs)
-  addsub(k1, t, 2, true);
-  uint64_t t4[4];
-  mul(c2, 2, A2, 2, t4);                     // c2 a2
-  addsub(k1, t4, 4, true);
-  mul(c1, 1, B1ABS, 2, t);                   // c1 |b1| (3 limbs)
-  addsub(k2, t, 3, false);
-  mul(c2, 2, &A1, 1, t);                     // c2 b2, b2 = a1 (3 limbs)
-  addsub(k2, t, 3, true);
   GlvSplit g{};
-  to_mag(k1, g.k1, &g.neg1);
-  to_mag(k2, g.k2, &g.neg2);
+  split_reduced(k, g.k1, &g.neg1, g.k2, &g.neg2);
   return g;
 }
-}  // namespace glv
+}  // namespace glv_host
 
 // out (XYZZ) = k * P for P affine (G1), k given as its GLV split.
 // One warp (launched with 32 threads; its 8 quads compute the same): the independent
 // products of each doubling and addition run on the lanes of a quad; lane 0 stores.
 __device__ void scale_point_glv(const uint32_t* __restrict__ P, const GlvSplit* __restrict__ gs,
                                 uint32_t* __restrict__ out) {
-  const Fq beta{{0xd782e155u, 0x71930c11u, 0xffbe3323u, 0xa6bb947cu, 0xd4741444u, 0xaa303344u, 0x26594943u,
-                 0x2c3b3f0du}};
+  Fq beta;
+  glv::beta_mont(beta.v);
   const GlvSplit g = *gs;
   Affine<Fq> p = ld_affine<Fq>(P);
   XYZZ<Fq> acc = XYZZ<Fq>::inf();
@@ -847,7 +779,7 @@ int cs_prove_device(cs_ctx* ctx, cs_pk* pk, const uint32_t* d_w, const uint32_t*
   uint32_t *outA = pts, *outB2 = pts + 32, *piC = pts + 160;
   uint32_t* rs = reinterpret_cast<uint32_t*>(base + P.rs);
   cudaStream_t s0 = ctx->stream;
-  const GlvSplit glv_rs[2] = {glv::split(s), glv::split(r)};  // s * pi_A, r * pi_B1
+  const GlvSplit glv_rs[2] = {glv_host::split(s), glv_host::split(r)};  // s * pi_A, r * pi_B1
   cudaEventRecord(ctx->ev_start, s0);
   // the call's scalars r, s and their GLV splits go to the device first; everything after
   // them depends only on the key, the witness buffer and the scratch layout
@@ -922,8 +854,8 @@ int cs_prove_batch_device(cs_ctx* ctx, cs_pk* pk, uint32_t k, const uint32_t* co
     BatchCall c{};
     std::memcpy(c.r, r + 8 * (size_t)i, 32);
     std::memcpy(c.s, s + 8 * (size_t)i, 32);
-    c.glv[0] = glv::split(c.s);
-    c.glv[1] = glv::split(c.r);
+    c.glv[0] = glv_host::split(c.s);
+    c.glv[1] = glv_host::split(c.r);
     c.d_w = d_w[i];
     c.d_proof = d_proof[i];
     hc[i] = c;

@@ -209,7 +209,11 @@ int cs_ctx_set_msm_affine_rounds(cs_ctx *ctx, int rounds);
 void cs_debug_fail_allocs(int count);
 
 /* Multi-exponentiation with host pointers: copies in, computes, copies the affine result
- * out, synchronises.  ec2 selects G2.  window = Pippenger window bits (0 = automatic). */
+ * out, synchronises.  ec2 selects G2.  window = Pippenger window bits (0 = automatic).
+ * G1 splits every scalar by the GLV endomorphism of BN254 (k = k1 + k2 lambda mod r with
+ * |k1|, |k2| < 2^127; k P = k1 P + k2 phi(P), phi(x, y) = (beta x, y)) and sorts the 2n
+ * half-scalars: ceil(128 / window) windows, half the bucket sets and half the window Horner
+ * of the full scalars' 254 / window + 1.  The result is the same point. */
 int cs_msm(cs_ctx *ctx, int ec2, const uint32_t *scalars, const uint32_t *points, uint32_t n,
            uint32_t *out_affine, int window);
 /* Same with device pointers, asynchronous on the context stream.  Scratch comes from the
@@ -218,7 +222,8 @@ int cs_msm_device(cs_ctx *ctx, int ec2, const uint32_t *d_scalars, const uint32_
                   uint32_t n, uint32_t *d_out_affine, int window);
 /* Scratch bytes one MSM of n terms needs (window 0 = automatic). */
 size_t cs_msm_workspace_bytes(uint32_t n, int ec2, int window);
-/* Window bits the automatic choice uses for n terms, and the resulting window count. */
+/* Window bits the automatic choice uses for n terms (G1: for the GLV split), and the window
+ * count of a full scalar (254 / window + 1: G2, fixed-base tables, batch instances). */
 int cs_msm_default_window(uint32_t n, int ec2);
 int cs_msm_num_windows(int window);
 
@@ -260,9 +265,10 @@ int cs_msm_batch_run(cs_ctx *ctx, cs_msm_batch *batch, int use_graph);
 void cs_msm_batch_destroy(cs_msm_batch *batch);
 size_t cs_msm_batch_workspace_bytes(const cs_msm_batch *batch);
 int cs_msm_batch_window(const cs_msm_batch *batch, uint32_t job);
-/* Window autotuner: times the MSM at each size 2^log_min..2^log_max for windows around the
- * cost-model choice and keeps the fastest per size (per device, process-wide); windows_out
- * (optional) receives them.  Synchronous. */
+/* Window autotuner for batched MSMs: times the MSM of full scalars (the form a batch instance
+ * runs) at each size 2^log_min..2^log_max for windows around the cost-model choice and keeps
+ * the fastest per size (per device, process-wide); windows_out (optional) receives them.
+ * Synchronous. */
 int cs_msm_autotune(cs_ctx *ctx, int ec2, uint32_t log_min, uint32_t log_max, int *windows_out);
 int cs_msm_tuned_window(cs_ctx *ctx, int ec2, uint32_t n);
 

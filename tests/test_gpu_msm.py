@@ -112,6 +112,32 @@ def test_msm_duplicates_cancellation_and_infinity(ctx, oracle, pts_g1):
     assert np.array_equal(ctx.msm(s2, pts[:80]), inf)
 
 
+def _glv_lambda():
+    """lambda of the G1 endomorphism (phi(P) = lambda P), from the split's lattice vector
+    (a1, b1): a1 + b1 lambda = 0 mod r."""
+    a1 = 0x89d3256894d213e3
+    b1 = -0x6f4d8248eeb859fc8211bbeb7d4f1128
+    lam = (-a1 * pow(b1, -1, R)) % R
+    assert (lam * lam + lam + 1) % R == 0
+    return lam
+
+
+def test_msm_glv_edge_scalars(ctx, oracle, pts_g1):
+    """G1 MSMs split every scalar as k1 + k2 lambda: scalars whose halves are zero, one,
+    negative or at the 2^127 bound, each alone (one term) and all together."""
+    lam = _glv_lambda()
+    ks = [1, 2, R - 1, R - 2, lam, lam + 1, lam - 1, R - lam, (lam * lam) % R, 2 * lam % R,
+          (1 << 127) - 1, 1 << 127, (1 << 128) - 1, 1 << 200, (1 << 253) + 12345, R + 5,
+          (1 << 256) - 1, 0x0be4e1541221250b6f4d8248eeb859fd, (R - 1) // 2, (R + 1) // 2]
+    s = ints_to_limbs(ks)
+    P = pts_g1[:len(ks)]
+    for i in range(len(ks)):
+        assert np.array_equal(ctx.msm(s[i:i + 1], P[i:i + 1]), oracle.msm(s[i:i + 1], P[i:i + 1])), hex(ks[i])
+    assert np.array_equal(ctx.msm(s, P), oracle.msm(s, P))
+    for w in (5, 11, 16):
+        assert np.array_equal(ctx.msm(s, P, window=w), oracle.msm(s, P)), w
+
+
 def test_msm_skewed_scalars_one_bucket(ctx, oracle, pts_g1):
     """All scalars equal: every entry lands in one bucket per window (split tasks)."""
     s = np.tile(ints_to_limbs([0xdeadbeef12345]), (4096, 1))
