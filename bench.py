@@ -28,8 +28,10 @@ call), wall clock; ``served_vs_plain`` = e2e / plain.  ``served_mix``: 8 circuit
 2^12..2^20 constraints (both ends and six seeded log-uniform sizes; the 2^20 one is the
 headline circuit), requests uniform over them, saturation and Poisson 50% / 90% with p50/p99.  ``batched_msm``: 64 G1 + 8 G2 MSMs of 2^floor(U(10,20))
 terms in one batch plan per group (autotuned windows, CUDA graph replay) vs one call per
-instance.  Also one BN128 G1 MSM of 2^20 terms (``g1_msm_2^20_ms``),
-whose bucket-accumulation kernel -- the dominant kernel of every proof -- carries the roofline.
+instance.  Also one BN128 G1 MSM of 2^20 terms (``g1_msm_2^20_ms``: generic bases, scalars split
+by GLV) and the fixed-base G1 MSM a proof runs four times over the same bases
+(``g1_fixed_msm_2^20_ms``), whose bucket-accumulation kernel -- the dominant kernel of every
+proof -- carries the roofline.
 
 ``proof_check``: every proof of the timed served run and of the e2e run equals the
 one-proof-per-call proof byte for byte; on rank 0 at N = 1 that proof also equals the
@@ -70,8 +72,8 @@ UNIT = "proofs/s (2^20 constraints)"
 PRODUCTS_PER_MONT = 136
 MONT_PER_MADD = 11     # mixed addition, 7M + 4S (the canonical count of the MSM cost model)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_accumulate launch of
-# the 2^20 G1 MSM (GLV split, window 16), from an ncu capture of that launch
-ACC_TRAFFIC_BYTES = 847_947_264 + 39_934_976
+# the 2^20-term fixed-base G1 MSM (window 20), from an ncu capture of that launch
+ACC_TRAFFIC_BYTES = 1_747_153_664 + 68_581_376
 L2_BYTES = 126 * 1024 * 1024
 LOG_M = 20
 R_INT, S_INT = 0x1234567890abcdef, 0xfedcba0987654321
@@ -260,16 +262,32 @@ class MsmWorkload:
         self.keep = g
 
     def step(self):
+        """The generic MSM (cs_msm_device): (ms, bucket-accumulation ms)."""
         self.ctx.msm_device(self.d_s.data_ptr(), self.d_p.data_ptr(), self.n, self.d_out.data_ptr())
         self.ctx.sync()
         return self.ctx.last_ms, self.ctx.last_phase_ms
 
-    def dominant_units(self):
-        """Bucket entries of one launch: the G1 MSM splits each scalar by GLV into two
-        half-scalars below 2^127, so 2n terms of ceil(128 / c) windows."""
+    def build_fixed(self):
+        """The fixed-base table of the proof's G1 MSMs over the same bases (window c: W = 254 / c
+        + 1 windows, table T[j n + i] = 2^(c j) P_i), built untimed."""
+        from cusnarks_b200 import Context
+        self.c_fixed = Context.msm_fixed_window(self.n)
+        pts = Context.msm_fixed_table_points(self.n, self.c_fixed)
+        self.d_table = self.torch.empty((pts, 16), dtype=self.torch.int32, device=self.d_p.device)
+        self.ctx.msm_fixed_table_device(self.d_p.data_ptr(), self.n, self.c_fixed, self.d_table.data_ptr())
+        self.ctx.sync()
+
+    def step_fixed(self):
+        """The fixed-base MSM a proof runs four times (cs_msm_fixed_device): (ms, accumulation ms)."""
+        self.ctx.msm_fixed_device(self.d_s.data_ptr(), self.d_table.data_ptr(), self.n, self.c_fixed,
+                                  self.d_out.data_ptr())
+        self.ctx.sync()
+        return self.ctx.last_ms, self.ctx.last_phase_ms
+
+    def fixed_units(self):
+        """Bucket entries of one fixed-base accumulation launch: n terms x (254 / c + 1) windows."""
         from cusnarks_b200._lib import lib
-        c = lib().cs_msm_default_window(self.n, 0)
-        return 2 * self.n * (-(-128 // c)), c
+        return self.n * lib().cs_msm_num_windows(self.c_fixed), self.c_fixed
 
 
 def sharded_msm_leg(ctx, world, rank, reps: int, log_n: int = 20, seed: int = 7):
@@ -541,17 +559,25 @@ def run_ours(args, world, rank, local):
         plain.prove(wl.circ.w, rr, ss)
     plain_ms = (time.perf_counter() - t0) * 1e3 / n_plain
     del plain
-    # the 2^20 G1 MSM and its dominant kernel
+    # the 2^20 G1 MSM (generic, GLV split) and the proof's dominant kernel: the bucket
+    # accumulation of its fixed-base G1 MSMs (same bases and scalars, fixed-base table)
     mw = MsmWorkload(ctx, 20, seed=7 + rank)
     for _ in range(3):
         mw.step()
-    msm_ms, acc_ms = [], []
+    msm_ms = []
     for _ in range(max(3, args.steps)):
-        t, a = mw.step()
-        msm_ms.append(t)
+        msm_ms.append(mw.step()[0])
+        wl.l2_flush()
+    mw.build_fixed()
+    for _ in range(3):
+        mw.step_fixed()
+    fixed_ms, acc_ms = [], []
+    for _ in range(max(3, args.steps)):
+        t, a = mw.step_fixed()
+        fixed_ms.append(t)
         acc_ms.append(a)
         wl.l2_flush()
-    units, window = mw.dominant_units()
+    units, window = mw.fixed_units()
     acc = statistics.mean(acc_ms)
     achieved = units * MONT_PER_MADD * PRODUCTS_PER_MONT / (acc * 1e-3)
     e2e_val = world * 1e3 / e2e_ms
@@ -588,12 +614,14 @@ def run_ours(args, world, rank, local):
                                     "with the call's scalars; wall clock"},
         "served_vs_plain": round(e2e_val * plain_ms / 1e3, 2),
         "g1_msm_2^20_ms": round(statistics.median(msm_ms), 3),
-        "roofline": {"bound": "int issue (ALU column sums + FP64 split products)", "kernel": "k_accumulate+k_combine (MSM bucket accumulation)",
+        "g1_fixed_msm_2^20_ms": round(statistics.median(fixed_ms), 3),
+        "roofline": {"bound": "int issue (ALU column sums + FP64 split products)",
+                     "kernel": "k_accumulate+k_combine (bucket accumulation of the proof's fixed-base G1 MSMs)",
                      "achieved": round(achieved / 1e12, 4), "peak": round(peak_wide / 1e12, 4),
                      "unit": "T wide products/s", "frac": round(achieved / peak_wide, 4),
                      "traffic": ACC_TRAFFIC_BYTES, "kernel_ms": round(acc, 4), "units_per_launch": units,
                      "window": window,
-                     "basis": "2^20 G1 MSM: 2N*ceil(128/c) bucket entries (GLV half-scalars) x 11 Montgomery products x 136 32x32->64 "
+                     "basis": "2^20-term fixed-base G1 MSM as in the proof: N*(254/c+1) bucket entries x 11 Montgomery products x 136 32x32->64 "
                               "products / kernel ms (CUDA events around the kernels); peak = live "
                               "mad.wide.u32 rate (cs_bench_pipe mode 3), the ceiling of a 32-bit CIOS "
                               "product (this kernel computes products in radix 2^52 on the FP64 pipe); "
