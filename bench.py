@@ -43,6 +43,10 @@ benchmark circuit through the reference's own CPU implementation (oracle/_ref, b
 the reference sources; the C restatement when that library is absent) on all host cores,
 stage by stage (QAP, H step, five multi-exponentiations).
 
+``per_config`` (rank 0, N = 1): the single-op configurations against the reference library
+on the same seeded inputs, results compared word for word -- one G1 MSM of 2^16 terms
+(config 1), the 2^20 NTT, INTT and H step (config 2): GPU device ms beside CPU wall ms.
+
 ``--impl reference``: the same CPU prover alone, in a process that never loads this
 library: the 2^20 circuit and key are built on the CPU (oracle/synth_cpu.py, word for word
 the GPU builder's), untimed; each step is the next stage of the 2^20 proving sequence (7
@@ -660,10 +664,86 @@ def run_ours(args, world, rank, local):
         line["proof_check"]["pairing"] = bool(verify(host["vk"], ref_proof, wl.circ.public_inputs))
         line["proof_check"]["basis"] += ("; on rank 0 it also equals the reference library's CPU proof and "
                                          "passes the Groth16 pairing check")
+        line["per_config"] = per_config_leg(ctx, reps=max(3, args.steps))
     if rank == 0:
         print(json.dumps(line), flush=True)
     wl.prover.close()
     ctx.close()
+
+
+def per_config_leg(ctx, reps: int):
+    """The single-op configurations, GPU against the reference's CPU library on the same seeded
+    inputs (results compared word for word): config 1, one G1 MSM of 2^16 terms
+    (ec_jacreduce_server_h); config 2, the 2^20 NTT and INTT (ntt_h / intt_h) and the 2^20 H
+    step (ntt_interpolandmul_server_h; the coset variant has no reference counterpart).  GPU:
+    device ms (CUDA events), median of reps; CPU: one call, wall clock, all host threads."""
+    import torch
+    from oracle.oracle import Oracle, RefLib, hstep_roots_table, random_field as fr_random
+    from cusnarks_b200.synth import random_field, g1_generator
+    if not RefLib.available():
+        return {"unavailable": "oracle/_ref (the reference library) is not built"}
+    ref, o = RefLib.get(), Oracle()
+    dev = torch.device("cuda", ctx.device)
+    out = {"cpu_threads": os.cpu_count() or 1}
+
+    def gpu_ms(call):
+        ts = []
+        for _ in range(reps + 1):
+            call()
+            ctx.sync()
+            ts.append(ctx.last_ms)
+        return statistics.median(ts[1:])
+
+    def cpu_s(call):
+        t0 = time.perf_counter()
+        r = call()
+        return r, time.perf_counter() - t0
+
+    def host(t):
+        return t.cpu().numpy().view(np.uint32)
+
+    # config 1
+    n = 1 << 16
+    rng = np.random.Generator(np.random.PCG64(16))
+    dk = torch.from_numpy(random_field(rng, n).view(np.int32)).to(dev)
+    s = random_field(rng, n)
+    ds = torch.from_numpy(s.view(np.int32)).to(dev)
+    g = torch.from_numpy(g1_generator().view(np.int32)).to(dev)
+    dp = torch.empty((n, 16), dtype=torch.int32, device=dev)
+    dout = torch.zeros(16, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    ctx.scmul_device(dk.data_ptr(), g.data_ptr(), n, dp.data_ptr(), point_stride_words=0)
+    ctx.sync()
+    ms = gpu_ms(lambda: ctx.msm_device(ds.data_ptr(), dp.data_ptr(), n, dout.data_ptr()))
+    want, sec = cpu_s(lambda: ref.msm(s, host(dp), 0, 6))
+    out["config1_g1_msm_2^16"] = {"gpu_ms": round(ms, 3), "cpu_ms": round(sec * 1e3, 1),
+                                  "equal": bool(np.array_equal(host(dout), want))}
+    # config 2
+    L = 20
+    rng = np.random.Generator(np.random.PCG64(220))
+    A = o.to_mont(fr_random(rng, 1 << L, 1), 1)  # Fr elements (pidx 1), as the config-2 tests draw them
+    B = o.to_mont(fr_random(rng, 1 << L, 1), 1)
+    dA, dB = torch.from_numpy(A.view(np.int32)).to(dev), torch.from_numpy(B.view(np.int32)).to(dev)
+    dF, dI = torch.empty_like(dA), torch.empty_like(dA)
+    dM = torch.zeros((2 << L, 8), dtype=torch.int32, device=dev)
+    dH = torch.zeros((1 << L, 8), dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    roots = o.find_roots(L)
+    f_ms = gpu_ms(lambda: ctx.ntt_device(dA.data_ptr(), dF.data_ptr(), L, 1))
+    i_ms = gpu_ms(lambda: ctx.ntt_device(dA.data_ptr(), dI.data_ptr(), L, -1, fmat=1))
+    F, f_s = cpu_s(lambda: ref.ntt(A, roots, L))
+    Iv, i_s = cpu_s(lambda: ref.intt(A, roots, L, 1, 1))
+    out["config2_ntt_2^20"] = {"gpu_ms": round(f_ms, 3), "cpu_ms": round(f_s * 1e3, 1),
+                               "equal": bool(np.array_equal(host(dF), F))}
+    out["config2_intt_2^20"] = {"gpu_ms": round(i_ms, 3), "cpu_ms": round(i_s * 1e3, 1),
+                                "equal": bool(np.array_equal(host(dI), Iv))}
+    h_ms = gpu_ms(lambda: ctx.hstep_device(0, dA.data_ptr(), dB.data_ptr(), 0, L, dM.data_ptr()))
+    M, h_s = cpu_s(lambda: ref.interpolandmul(A, B, hstep_roots_table(o, L), L, 2, os.cpu_count() or 1))
+    out["config2_hstep_2^20"] = {"gpu_ms": round(h_ms, 3), "cpu_ms": round(h_s * 1e3, 1),
+                                 "equal": bool(np.array_equal(host(dM), M))}
+    c_ms = gpu_ms(lambda: ctx.hstep_device(1, dA.data_ptr(), dB.data_ptr(), dB.data_ptr(), L, dH.data_ptr()))
+    out["config2_hstep_coset_2^20"] = {"gpu_ms": round(c_ms, 3)}
+    return out
 
 
 def run_reference(args, world, rank):

@@ -48,7 +48,11 @@ def g2_generator() -> np.ndarray:
 
 
 def random_field(rng: np.random.Generator, n: int, p: int = R) -> np.ndarray:
-    """(n, 8) uint32, uniform in [0, p) by rejection on the top limb then exact compare."""
+    """(n, 8) uint32, uniform in [0, p) by rejection on the top limb then exact compare.
+    p is the modulus itself (R or Q), at least 2^224 so a candidate passes with probability
+    at least 1/2 (a field index such as 1 would reject every candidate but zero)."""
+    if p < (1 << 224) or p >= (1 << 256):
+        raise ValueError("random_field: p must be a modulus in [2^224, 2^256)")
     top = p >> 224
     out = np.empty((n, 8), dtype=np.uint32)
     filled = 0
