@@ -615,11 +615,12 @@ bool prove_batch_ready(cs_ctx* ctx, const cs_pk* pk, uint32_t k) {
 uint32_t pk_n_vars(const cs_pk* pk) { return pk->n_vars; }
 // Grows the context's arenas to what a proof with this key needs (cs_prove would grow them
 // on its first call): lets the server allocate a slot's scratch right after admission.
-cudaError_t prove_reserve(cs_ctx* ctx, const cs_pk* pk) {
+// Grows the context's scratch arena and witness buffer to at least these sizes.
+cudaError_t ctx_reserve(cs_ctx* ctx, size_t work_bytes, size_t in_bytes) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
-  cudaError_t e = ctx->work.reserve(plan_prove(pk).total, ctx->stream);
-  if (e == cudaSuccess) e = ctx->in.reserve((size_t)pk->n_vars * 32 + 512, ctx->stream);
+  cudaError_t e = ctx->work.reserve(work_bytes, ctx->stream);
+  if (e == cudaSuccess) e = ctx->in.reserve(in_bytes, ctx->stream);
   return e;
 }
 }  // namespace csb

@@ -9,7 +9,9 @@
 //     and scratch arena) and takes the next request as soon as it is free AND the request
 //     is admitted by device memory: free memory (cudaMemGetInfo) minus the bytes promised
 //     to admitted requests whose slots have not grown yet must cover the slot's scratch
-//     growth plus `reserve`; an admitted slot grows its arenas at once and then withdraws
+//     growth plus `reserve`; a slot grows once for every registered key where that fits
+//     (else for the request's key), so it does not grow, free and synchronise the device
+//     again in steady state; an admitted slot grows its buffers at once and then withdraws
 //     its promise, since cudaMemGetInfo counts the memory from then on;
 //   * admitted proofs run concurrently on the device: one proof's MSM tails, QAP and
 //     H step overlap the next one's bucket accumulation;
@@ -38,7 +40,7 @@
 namespace csb {
 size_t prove_workspace_bytes(const cs_pk* pk);
 uint32_t pk_n_vars(const cs_pk* pk);
-cudaError_t prove_reserve(cs_ctx* ctx, const cs_pk* pk);
+cudaError_t ctx_reserve(cs_ctx* ctx, size_t work_bytes, size_t in_bytes);
 uint32_t pk_domain(const cs_pk* pk);
 bool pk_has_fixed(const cs_pk* pk);
 bool prove_batch_ready(cs_ctx* ctx, const cs_pk* pk, uint32_t k);
@@ -103,14 +105,44 @@ struct cs_server {
 
 namespace {
 
-// Bytes a slot must still allocate to run a proof with key pk (its arenas only grow).
-size_t growth(const cs_ctx* ctx, const cs_pk* pk, size_t pinned_have) {
-  const size_t ws = csb::prove_workspace_bytes(pk);
-  const size_t in = (size_t)csb::pk_n_vars(pk) * 32 + 512;
+// What a slot holds to prove with a set of keys: its context's scratch arena and witness
+// buffer, the pinned staging of host witnesses, and the device witnesses and proofs of a
+// same-key batch.
+struct SlotSizes {
+  size_t work = 0, in = 0, stage = 0, batch_in = 0;
+};
+
+// Batch size a slot may form for key pk (largest power of two <= max_batch, at least
+// kMinBatch; 1 when the key is not batched).
+uint32_t batch_cap(const cs_pk* pk, int max_batch) {
+  if (max_batch < (int)kMinBatch || csb::pk_domain(pk) > (1u << 16) || !csb::pk_has_fixed(pk)) return 1;
+  uint32_t k = 1;
+  while (k * 2 <= (uint32_t)max_batch) k *= 2;
+  return k;
+}
+
+void add_key_sizes(SlotSizes& z, const cs_pk* pk, int max_batch) {
+  const size_t wbytes = (size_t)csb::pk_n_vars(pk) * 32;
+  const uint32_t k = batch_cap(pk, max_batch);
+  z.work = std::max(z.work, csb::prove_workspace_bytes(pk));
+  z.in = std::max(z.in, wbytes + 512);
+  z.stage = std::max(z.stage, wbytes * k);
+  if (k > 1) z.batch_in = std::max(z.batch_in, (size_t)k * (((wbytes + 255) & ~size_t(255)) + 256));
+}
+
+SlotSizes slot_sizes(const std::vector<cs_pk*>& keys, int max_batch) {
+  SlotSizes z;
+  for (const cs_pk* pk : keys) add_key_sizes(z, pk, max_batch);
+  return z;
+}
+
+// Device bytes a slot must still allocate to hold `want` (its buffers only grow; each adds
+// an eighth of headroom when it grows).
+size_t growth(const cs_ctx* ctx, const csb::DeviceBuffer& batch_in, const SlotSizes& want) {
   size_t g = 0;
-  if (ws > ctx->work.bytes) g += ws + ws / 8;
-  if (in > ctx->in.bytes) g += in + in / 8;
-  (void)pinned_have;
+  if (want.work > ctx->work.bytes) g += want.work + want.work / 8;
+  if (want.in > ctx->in.bytes) g += want.in + want.in / 8;
+  if (want.batch_in > batch_in.bytes) g += want.batch_in + want.batch_in / 8;
   return g;
 }
 
@@ -131,6 +163,7 @@ void cs_server::worker(int slot) {
     std::shared_ptr<Request> rq;
     std::vector<std::shared_ptr<Request>> batch;  // requests proved together with rq
     size_t need = 0, batch_need = 0;
+    SlotSizes grow_to;  // what the slot grows to once admitted
     {
       std::unique_lock<std::mutex> lk(mu);
       for (;;) {
@@ -142,12 +175,20 @@ void cs_server::worker(int slot) {
           return;
         }
         if (!queue.empty()) {
-          need = growth(ctx, queue.front()->pk, stage.bytes);
-          if (need == 0) break;  // the slot already holds the scratch: nothing to admit
+          // A slot sizes itself for every registered key at once where memory allows, so it
+          // does not grow again in steady state (growing frees the old block: a device-wide
+          // synchronisation that stalls every slot); else for the head request's key alone.
+          grow_to = slot_sizes(keys, max_batch);
+          need = growth(ctx, batch_in, grow_to);
+          if (need == 0) break;  // the slot already holds it all: nothing to admit
           size_t free_b = 0, total_b = 0;
           cudaMemGetInfo(&free_b, &total_b);
           const size_t avail = free_b > promised ? free_b - promised : 0;
           if (avail >= need + reserve) break;
+          grow_to = SlotSizes{};
+          add_key_sizes(grow_to, queue.front()->pk, max_batch);
+          need = growth(ctx, batch_in, grow_to);
+          if (need == 0 || avail >= need + reserve) break;
           if (busy == 0) {  // nothing will free memory: refuse the head request
             auto bad = queue.front();
             queue.pop_front();
@@ -207,8 +248,11 @@ void cs_server::worker(int slot) {
     const size_t wbytes = (size_t)csb::pk_n_vars(pk) * 32;
     int st = CS_OK;
     std::string msg;
-    if (need) {  // grow the slot's scratch now; from here on free memory accounts for it
-      const cudaError_t ge = csb::prove_reserve(ctx, pk);
+    if (need) {  // grow the slot's buffers now; from here on free memory accounts for them
+      cudaError_t ge = csb::ctx_reserve(ctx, grow_to.work, grow_to.in);
+      if (ge == cudaSuccess)
+        ge = batch_in.reserve(grow_to.batch_in, static_cast<cudaStream_t>(cs_ctx_stream(ctx)));
+      if (ge == cudaSuccess) ge = stage.reserve(grow_to.stage);
       {
         std::lock_guard<std::mutex> lk(mu);
         promised = promised > need ? promised - need : 0;
