@@ -110,3 +110,29 @@ def test_same_key_batches_equal_alone(keys):
         assert st["batches"] >= 1 and 4 <= st["max_batch_seen"] <= 8, st
     finally:
         srv.close()
+
+
+def test_key_added_while_serving(keys):
+    """Slots size themselves for the keys registered when they first take work; a larger key
+    added later makes them grow once more.  Proofs before and after equal the lone proofs."""
+    from cusnarks_b200.server import ProveServer
+    (c0, _, p0), (c2, _, p2) = keys[0], keys[2]
+    alone0 = [p0.prove(c0.w, *_rs(i)) for i in range(6)]
+    alone2 = [p2.prove(c2.w, *_rs(50 + i)) for i in range(6)]
+    srv = ProveServer(0, slots=2, reserve_bytes=64 << 20, max_batch=4)
+    try:
+        k0 = srv.add_key(p0)
+        first = [srv.submit(k0, c0.w, *_rs(i)) for i in range(6)]
+        for i, t in enumerate(first):
+            assert np.array_equal(srv.wait(t, timeout=120.0)[0], alone0[i]), i
+        k2 = srv.add_key(p2)
+        mixed = []
+        for i in range(6):
+            mixed.append((alone2[i], srv.submit(k2, c2.w, *_rs(50 + i))))
+            mixed.append((alone0[i], srv.submit(k0, c0.w, *_rs(i))))
+        for want, t in mixed:
+            assert np.array_equal(srv.wait(t, timeout=120.0)[0], want)
+        st = srv.stats()
+        assert st["completed"] == 18 and st["failed"] == 0
+    finally:
+        srv.close()
