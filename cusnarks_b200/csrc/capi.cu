@@ -20,9 +20,6 @@ void note_launch(unsigned n) {
 }
 unsigned long long thread_launches() { return t_launches; }
 
-#ifndef CSB_PRIO_MODE
-#define CSB_PRIO_MODE 2  // G2 MSM and the QAP/H chain first (measured 32.0 -> 31.6 ms per 2^20 proof)
-#endif
 
 // Auxiliary streams of the prove pipeline: aux[0..3] carry the A, B1, B2 (G2) and C MSMs,
 // aux_h the QAP -> H step -> H MSM chain.  Priorities (lower number = higher priority)
@@ -31,10 +28,8 @@ cudaError_t ctx_aux_init(cs_ctx* ctx) {
   if (ctx->aux_ready) return cudaSuccess;
   int least = 0, greatest = 0;
   cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
-  int prio[4] = {least, least, least, least}, prio_h = least;
-  if (CSB_PRIO_MODE == 1) { prio[2] = greatest; }
-  if (CSB_PRIO_MODE == 2) { prio[2] = greatest; prio_h = greatest; }
-  if (CSB_PRIO_MODE == 3) { prio[2] = greatest < least ? greatest + 1 : greatest; prio_h = greatest; }
+  // the G2 MSM and the QAP / H chain first (measured 32.0 -> 31.6 ms per 2^20 proof)
+  int prio[4] = {least, least, greatest, least}, prio_h = greatest;
   for (int i = 0; i < 4 && e == cudaSuccess; i++)
     if (!ctx->aux[i]) e = cudaStreamCreateWithPriority(&ctx->aux[i], cudaStreamNonBlocking, prio[i]);
   if (e == cudaSuccess && !ctx->aux_h) e = cudaStreamCreateWithPriority(&ctx->aux_h, cudaStreamNonBlocking, prio_h);

@@ -324,23 +324,20 @@ CSB_DEV void st_xyzz(uint32_t* p, const XYZZ<F>& a) {
   st_field(p, a.X); st_field(p + W, a.Y); st_field(p + 2 * W, a.ZZ); st_field(p + 3 * W, a.ZZZ);
 }
 
-#ifndef CSB_QUAD_CALL_FQ2
-#define CSB_QUAD_CALL_FQ2 1
-#endif
-// Quad operations as calls: one body per kernel instead of one per use, for kernels that
-// chain many of them over Fq2, whose inlined copies overflow the register file.
+// Quad operations as calls over Fq2: one body per kernel instead of one per use, for kernels
+// that chain many of them, whose inlined copies overflow the register file.
 template <class F>
 __device__ __noinline__ XYZZ<F> xyzz_add_quad_call(const XYZZ<F> p, const XYZZ<F> q) { return xyzz_add_quad(p, q); }
 template <class F>
 __device__ __noinline__ XYZZ<F> xyzz_dbl_quad_call(const XYZZ<F> p) { return xyzz_dbl_quad(p); }
 template <class F>
 CSB_DEV XYZZ<F> add_q(const XYZZ<F>& p, const XYZZ<F>& q) {
-  if constexpr (CSB_QUAD_CALL_FQ2 && FieldWords<F>::value == 16) return xyzz_add_quad_call(p, q);
+  if constexpr (FieldWords<F>::value == 16) return xyzz_add_quad_call(p, q);
   else return xyzz_add_quad(p, q);
 }
 template <class F>
 CSB_DEV XYZZ<F> dbl_q(const XYZZ<F>& p) {
-  if constexpr (CSB_QUAD_CALL_FQ2 && FieldWords<F>::value == 16) return xyzz_dbl_quad_call(p);
+  if constexpr (FieldWords<F>::value == 16) return xyzz_dbl_quad_call(p);
   else return xyzz_dbl_quad(p);
 }
 

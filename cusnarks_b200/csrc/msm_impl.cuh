@@ -317,16 +317,11 @@ __global__ void k_task_emit(const uint32_t* __restrict__ offsets, uint32_t nb, u
   }
 }
 
-// Minimum resident blocks per SM asked of the compiler for the accumulation kernel
-// (0 = no register cap).
-#ifndef CSB_ACC_G2_MINB
-#define CSB_ACC_G2_MINB 3  // 168 registers: 12 warps per SM instead of 8 (measured faster)
-#endif
-#ifndef CSB_ACC_G1_MINB
-#define CSB_ACC_G1_MINB 0
-#endif
-template <class F> struct AccMinBlocks { static constexpr int value = CSB_ACC_G1_MINB; };
-template <> struct AccMinBlocks<Fq2> { static constexpr int value = CSB_ACC_G2_MINB; };
+// Minimum resident blocks per SM asked of the compiler for the accumulation kernel (0 = no
+// register cap): G2 at 3 (168 registers: 12 warps per SM instead of 8, measured faster), G1
+// uncapped (caps spilled and measured slower).
+template <class F> struct AccMinBlocks { static constexpr int value = 0; };
+template <> struct AccMinBlocks<Fq2> { static constexpr int value = 3; };
 
 // The accumulation's mixed addition: over Fq with lazily reduced coordinates (no final
 // conditional subtraction per product; the bucket is canonicalised when stored), over Fq2
@@ -665,9 +660,7 @@ __global__ void __launch_bounds__(128) k_reduce_level_quad2(const uint32_t* __re
 // Threads of the per-window sum (one block per window).  128 (4 warps, one per SM
 // sub-partition) shortens each dependent point operation enough to pay for the longer chains
 // of 32 virtual threads: 2^12 proof 2.00 -> 1.91 ms, G2 2^12 fixed-base MSM 1.68 -> 1.58 ms.
-#ifndef CSB_WSUM_THREADS
-#define CSB_WSUM_THREADS 128
-#endif
+constexpr int kWsumThreads = 128;
 template <class F, int THREADS>
 __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restrict__ y,
                                                         const uint32_t* __restrict__ z, uint32_t n1,
@@ -813,10 +806,7 @@ __global__ void k_store_inf(uint32_t* out) {
 // 10 of an XYZZ + affine addition.  Round r maps bucket b's c_b points at in_off[b] to
 // ceil(c_b / 2) points at out_off[b]; an odd last point is copied.  Points at infinity
 // inside the rounds are (0, 0), which is on neither curve.
-#ifndef CSB_AFF_K
-#define CSB_AFF_K 64
-#endif
-constexpr uint32_t kAffK = CSB_AFF_K;
+constexpr uint32_t kAffK = 64;  // 32 and 128 measured slower (G2 fixed-base 2^20)
 
 template <class F>
 CSB_DEV bool aff_zero(const Affine<F>& a) { return a.x.is_zero() && a.y.is_zero(); }
@@ -1258,7 +1248,7 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
     nseg = nnext;
     levels++;
   }
-  constexpr int WT = CSB_WSUM_THREADS;
+  constexpr int WT = kWsumThreads;
   k_window_sum<F, WT><<<WR, WT, 0, st>>>(y, z, nseg, 3 * levels, wsum);
   note_launch();
   k_finish<F><<<1, 32, 0, st>>>(wsum, WR, c, d_out);
