@@ -158,23 +158,30 @@ __device__ __noinline__ XYZZ<F> xyzz_dbl_cold(const XYZZ<F> p) { return xyzz_dbl
 
 // ------------------------------------------------ quad-parallel point operations -----
 // For chains that a point runs through alone (window Horner, scalar multiplication, the
-// buckets of a small MSM): the 4 lanes of an aligned quad hold the same point and each
-// computes one of the independent products of a dependency level, so a doubling costs 3
+// buckets of a small MSM): the lanes of an aligned group hold the same point and each
+// computes part of the independent products of a dependency level, so a doubling costs 3
 // product latencies instead of 9, an addition 4 instead of 14 and a mixed addition 4
-// instead of 10.  The shuffles use the full warp mask, so every lane of the warp must call
-// these together (the 8 quads may hold different points: the special cases -- infinity,
-// equal or opposite points -- are selected after the general formula, never branched
-// around it); every lane of a quad returns the same result.
-template <class F>
-CSB_DEV F quad_bcast(const F& v, int src) {
-  constexpr int FW = sizeof(F) / 4;
-  F o;
+// instead of 10.  A group is 4 lanes over Fq (a "quad": one product each) and 16 lanes over
+// Fq2 (twelve of them one Fq product each of the level's four Karatsuba products).  The
+// shuffles use the full warp mask, so every lane of the warp must call these together (the
+// warp's groups may hold different points: the special cases -- infinity, equal or opposite
+// points -- are selected after the general formula, never branched around it); every lane of
+// a group returns the same result.  The names keep "quad" for the group.
+template <class F> struct GroupLanes { static constexpr int value = 4; };
+template <> struct GroupLanes<Fq2> { static constexpr int value = 16; };
+
+template <int G, class T>
+CSB_DEV T grp_bcast(const T& v, int src) {
+  constexpr int TW = sizeof(T) / 4;
+  T o;
   uint32_t* ow = reinterpret_cast<uint32_t*>(&o);
   const uint32_t* vw = reinterpret_cast<const uint32_t*>(&v);
 #pragma unroll
-  for (int w = 0; w < FW; w++) ow[w] = __shfl_sync(0xffffffffu, vw[w], src, 4);
+  for (int w = 0; w < TW; w++) ow[w] = __shfl_sync(0xffffffffu, vw[w], src, G);
   return o;
 }
+template <class F>
+CSB_DEV F quad_bcast(const F& v, int src) { return grp_bcast<4>(v, src); }
 
 template <class F>
 CSB_DEV F pick4(int k, const F& v0, const F& v1, const F& v2, const F& v3) {
@@ -194,6 +201,30 @@ CSB_DEV void quad_mul4(const F& a0, const F& b0, const F& a1, const F& b1, const
   r1 = quad_bcast(r, 1);
   r2 = quad_bcast(r, 2);
   r3 = quad_bcast(r, 3);
+}
+// Over Fq2, in groups of 16 lanes: lane l < 12 computes part l mod 3 of Karatsuba product
+// l / 3 (a0 b0, a1 b1 or (a0 + a1)(b0 + b1), the Fq products Fq2's operator* forms), every lane
+// gathers the twelve and forms the four products as operator* does: the same bits, one Fq
+// product latency per level instead of three.
+template <>
+CSB_DEV void quad_mul4<Fq2>(const Fq2& a0, const Fq2& b0, const Fq2& a1, const Fq2& b1, const Fq2& a2,
+                            const Fq2& b2, const Fq2& a3, const Fq2& b3, Fq2& r0, Fq2& r1, Fq2& r2, Fq2& r3) {
+  const int l = threadIdx.x & 15;
+  const int j = l < 12 ? l / 3 : 0, part = l < 12 ? l - 3 * j : 0;
+  const Fq2 a = pick4(j, a0, a1, a2, a3), b = pick4(j, b0, b1, b2, b3);
+  const Fq x = part == 0 ? a.c0 : (part == 1 ? a.c1 : a.c0 + a.c1);
+  const Fq y = part == 0 ? b.c0 : (part == 1 ? b.c1 : b.c0 + b.c1);
+  const Fq p = x * y;
+  Fq2 r[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const Fq v0 = grp_bcast<16>(p, 3 * k), v1 = grp_bcast<16>(p, 3 * k + 1), s = grp_bcast<16>(p, 3 * k + 2);
+    r[k] = Fq2{v0 - v1, s - v0 - v1};
+  }
+  r0 = r[0];
+  r1 = r[1];
+  r2 = r[2];
+  r3 = r[3];
 }
 
 // dbl-2008-s-1, three levels of products

@@ -186,7 +186,8 @@ cudaError_t batch_impl(const MsmBatch& b, void* d_work, size_t work_bytes, cudaS
       nseg = nnext;
       levels++;
     }
-    k_window_sum<F, 256><<<WR, 256, 0, st>>>(y, z, nseg, 3 * levels, wsum + (size_t)G.window0 * XWD);
+    constexpr int WT = WsumThreads<F>::batch;
+    k_window_sum<F, WT><<<WR, WT, 0, st>>>(y, z, nseg, 3 * levels, wsum + (size_t)G.window0 * XWD);
     note_launch();
   }
   k_bfinish<F><<<(32 * b.njobs + 127) / 128, 128, 0, st>>>(b.d_jobs, b.njobs, wsum);

@@ -381,11 +381,12 @@ __global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate_quad
     const uint32_t* __restrict__ phix = nullptr) {
   constexpr int PW = 2 * FieldWords<F>::value;
   constexpr int XW = 4 * FieldWords<F>::value;
+  constexpr uint32_t G = GroupLanes<F>::value, QPW = 32 / G;  // lanes per group, groups per warp
   const uint32_t ntasks = counters[0];
   const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t qw = (threadIdx.x & 31) >> 2;  // quad within the warp
-  for (uint32_t base = warp0 * 8; base < ntasks; base += nwarps * 8) {  // warp-uniform
+  const uint32_t qw = (threadIdx.x & 31) / G;  // group within the warp
+  for (uint32_t base = warp0 * QPW; base < ntasks; base += nwarps * QPW) {  // warp-uniform
     const uint32_t t = base + qw;
     const bool valid = t < ntasks;
     const Task tk = valid ? tasks[t] : Task{0, 0, 0, 0};
@@ -409,7 +410,7 @@ __global__ void __launch_bounds__(128, AccMinBlocks<F>::value) k_accumulate_quad
       const bool take = live && (entries || !(p.x.is_zero() && p.y.is_zero()));
       acc = xyzz_select(take, nxt, acc);
     }
-    if (valid && (threadIdx.x & 3) == 0) {
+    if (valid && (threadIdx.x & (G - 1)) == 0) {
       uint32_t* dst = tk.dst < nb ? buckets + (size_t)tk.dst * XW : partials + (size_t)(tk.dst - nb) * XW;
       st_xyzz<F>(dst, acc);
     }
@@ -546,7 +547,8 @@ __global__ void __launch_bounds__(128) k_reduce_level_quad(const uint32_t* __res
                                                            uint32_t* __restrict__ yout,
                                                            uint32_t* __restrict__ zout) {
   constexpr int XW = 4 * FieldWords<F>::value;
-  const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 2;
+  constexpr uint32_t G = GroupLanes<F>::value;
+  const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const bool valid = g < (uint32_t)W * nout;
   const uint32_t j = valid ? g / nout : 0u, t = valid ? g % nout : 0u;
   const uint32_t* yj = y + (size_t)j * n * XW;
@@ -576,7 +578,7 @@ __global__ void __launch_bounds__(128) k_reduce_level_quad(const uint32_t* __res
       s = add_q(s, v);
     }
   }
-  if (valid && (threadIdx.x & 3) == 0) {
+  if (valid && (threadIdx.x & (G - 1)) == 0) {
     st_xyzz<F>(yout + ((size_t)j * nout + t) * XW, acc);
     st_xyzz<F>(zout + ((size_t)j * nout + t) * XW, s);
   }
@@ -606,7 +608,8 @@ __global__ void __launch_bounds__(128) k_reduce_level_quad2(const uint32_t* __re
                                                             uint32_t* __restrict__ yout,
                                                             uint32_t* __restrict__ zout) {
   constexpr int XW = 4 * FieldWords<F>::value;
-  const uint32_t gq = (blockIdx.x * blockDim.x + threadIdx.x) >> 2;
+  constexpr uint32_t G = GroupLanes<F>::value;
+  const uint32_t gq = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const uint32_t g = gq >> 1;
   const bool zq = (gq & 1) != 0;  // the odd quad of the pair sums the z values
   const bool valid = g < (uint32_t)W * nout;
@@ -643,8 +646,8 @@ __global__ void __launch_bounds__(128) k_reduce_level_quad2(const uint32_t* __re
   // the whole warp, so every lane takes part in the same steps (no extra latency)
 #pragma unroll 1
   for (int d = 0; d < 3 * level; d++) s = dbl_q(s);
-  s = add_q(s, shfl_down_xyzz(a, 4));  // even quads: + the odd neighbour's z sum
-  if (valid && !zq && (threadIdx.x & 3) == 0) {
+  s = add_q(s, shfl_down_xyzz(a, G));  // even groups: + the odd neighbour's z sum
+  if (valid && !zq && (threadIdx.x & (G - 1)) == 0) {
     st_xyzz<F>(yout + ((size_t)j * nout + t) * XW, a);
     st_xyzz<F>(zout + ((size_t)j * nout + t) * XW, s);
   }
@@ -652,32 +655,51 @@ __global__ void __launch_bounds__(128) k_reduce_level_quad2(const uint32_t* __re
 
 // Per-window sum after levels 0..L-1.  With y_t the segment totals and z_t the weighted
 // carries of the last level, S_j = sum_t (y_t + z_t) + G * sum_t t * y_t with G = 8^L =
-// 2^shift.  One block per window, E consecutive segments per thread u:
+// 2^shift.  One block per window, E consecutive segments per virtual thread u:
 //   V_u = Y_u + Z_u + G * sum_i i*y_{uE+i}      (Y_u, Z_u: the thread's totals)
 //   sum_t t*y_t = sum_u [sum_i i*y_{uE+i}] + E * sum_{u>=1} Suf(u),  Suf(u) = sum_{v>=u} Y_v
-// so S_j = sum_u (V_u + G E * Suf(u) [u >= 1]): a block suffix scan and a block reduction,
-// about 2E + 25 dependent point operations instead of a serial pass over the segments.
+// so S_j = sum_u (V_u + G E * Suf(u) [u >= 1]): a suffix scan and a reduction over the block's
+// virtual threads, about 2E + 2 log2(VT) + shift dependent point operations instead of a serial
+// pass over the segments.
 // Threads of the per-window sum (one block per window).  128 (4 warps, one per SM
 // sub-partition) shortens each dependent point operation enough to pay for the longer chains
 // of 32 virtual threads: 2^12 proof 2.00 -> 1.91 ms, G2 2^12 fixed-base MSM 1.68 -> 1.58 ms.
+// Over Fq2 (16-lane groups) 256 threads, 16 virtual threads, for the single MSM and batches
+// (128: G2 fixed-base 2^20 13.5 ms, 256: 13.0; 512 slower at every size).
 constexpr int kWsumThreads = 128;
+template <class F> struct WsumThreads { static constexpr int single = kWsumThreads, batch = 256; };
+template <> struct WsumThreads<Fq2> { static constexpr int single = 256, batch = 256; };
 template <class F, int THREADS>
 __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restrict__ y,
                                                         const uint32_t* __restrict__ z, uint32_t n1,
                                                         int shift, uint32_t* __restrict__ wsum) {
-  // Quad form: each quad of lanes is one virtual thread u running quad point operations, so
-  // the block has VT = THREADS / 4 virtual threads, 8 per warp.
+  // Group form: each group of G lanes is one virtual thread u running group point operations,
+  // so the block has VT = THREADS / G virtual threads.  The scan and the reduction across them
+  // go through shared memory (double-buffered Hillis-Steele steps); the group's first lane
+  // writes, every lane reads.
   constexpr int XW = 4 * FieldWords<F>::value;
-  constexpr int NW = THREADS / 32;
-  constexpr uint32_t VT = THREADS / 4;
-  static_assert(NW <= 8, "the warp totals are scanned by the 8 quads of one warp");
-  __shared__ uint32_t sh[NW][XW];
+  constexpr uint32_t G = GroupLanes<F>::value;
+  constexpr uint32_t VT = THREADS / G;
+  static_assert(VT >= 1 && (VT & (VT - 1)) == 0, "virtual threads: a power of two");
+  __shared__ uint32_t sh[2][VT][XW];
   const int j = blockIdx.x;
   const uint32_t* yj = y + (size_t)j * n1 * XW;
   const uint32_t* zj = z + (size_t)j * n1 * XW;
   const uint32_t E = (n1 + VT - 1) / VT;  // n1 is a power of two
-  const uint32_t u = threadIdx.x >> 2;
-  const int vl = (threadIdx.x & 31) >> 2, warp = threadIdx.x >> 5, q = threadIdx.x & 3;
+  const uint32_t u = threadIdx.x / G;
+  const bool lead = (threadIdx.x & (G - 1)) == 0;
+  auto put = [&](int b, uint32_t slot, const XYZZ<F>& v) {
+    if (lead) {
+      const uint32_t* w = reinterpret_cast<const uint32_t*>(&v);
+      for (int k = 0; k < XW; k++) sh[b][slot][k] = w[k];
+    }
+  };
+  auto get = [&](int b, uint32_t slot) {
+    XYZZ<F> v;
+    uint32_t* w = reinterpret_cast<uint32_t*>(&v);
+    for (int k = 0; k < XW; k++) w[k] = sh[b][slot][k];
+    return v;
+  };
   // the sums start at the thread's last segment (no additions to infinity)
   XYZZ<F> acc, zs, ws = XYZZ<F>::inf();
   {
@@ -701,78 +723,42 @@ __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restri
     for (int d = 0; d < shift; d++) ws = dbl_q(ws);
     V = add_q(V, ws);
   }
-  // inclusive suffix scan of acc over the 8 virtual lanes of the warp
+  // inclusive suffix scan of acc over the virtual threads: Suf(u)
   XYZZ<F> suf = acc;
+  int cur = 0;
+  put(cur, u, suf);
+  __syncthreads();
 #pragma unroll 1
-  for (int d = 1; d < 8; d <<= 1) {
-    const XYZZ<F> o = shfl_down_xyzz(suf, 4 * d);
-    suf = xyzz_select(vl + d < 8, add_q(suf, o), suf);
+  for (uint32_t d = 1; d < VT; d <<= 1) {
+    const bool has = u + d < VT;
+    const XYZZ<F> o = has ? get(cur, u + d) : XYZZ<F>::inf();
+    suf = xyzz_select(has, add_q(suf, o), suf);
+    cur ^= 1;
+    put(cur, u, suf);
+    __syncthreads();
   }
-  if (vl == 0 && q == 0) {
-    const uint32_t* w = reinterpret_cast<const uint32_t*>(&suf);
-    for (int k = 0; k < XW; k++) sh[warp][k] = w[k];
-  }
-  __syncthreads();
-  if (warp == 0) {
-    XYZZ<F> t = XYZZ<F>::inf();
-    if (vl < NW) {
-      uint32_t* w = reinterpret_cast<uint32_t*>(&t);
-      for (int k = 0; k < XW; k++) w[k] = sh[vl][k];
-    }
-    // exclusive suffix over warp totals: virtual lane w gets the totals of warps > w
-#pragma unroll 1
-    for (int d = 1; d < 8; d <<= 1) {
-      const XYZZ<F> o = shfl_down_xyzz(t, 4 * d);
-      t = xyzz_select(vl + d < 8, add_q(t, o), t);
-    }
-    XYZZ<F> excl = shfl_down_xyzz(t, 4);
-    if (vl == 7) excl = XYZZ<F>::inf();
-    __syncwarp();
-    if (vl < NW && q == 0) {
-      const uint32_t* w = reinterpret_cast<const uint32_t*>(&excl);
-      for (int k = 0; k < XW; k++) sh[vl][k] = w[k];
-    }
-  }
-  __syncthreads();
-  {
-    XYZZ<F> off;
-    uint32_t* w = reinterpret_cast<uint32_t*>(&off);
-    for (int k = 0; k < XW; k++) w[k] = sh[warp][k];
-    suf = add_q(suf, off);
-  }
-  __syncthreads();
   // C_u = V_u + 2^shift E * Suf(u) for u >= 1 (E is a power of two)
-  {  // computed by every quad (uniform), kept where u >= 1 and u E < n1
+  {  // computed by every group (uniform), kept where u >= 1 and u E < n1
 #pragma unroll 1
     for (uint32_t m = E; m > 1; m >>= 1) suf = dbl_q(suf);
 #pragma unroll 1
     for (int d = 0; d < shift; d++) suf = dbl_q(suf);
     V = xyzz_select(u >= 1 && u * E < n1, add_q(V, suf), V);
   }
-  // block reduction of V: over the warp's virtual lanes, then over the warps
-#pragma unroll 1
-  for (int d = 4; d > 0; d >>= 1) {
-    const XYZZ<F> o = shfl_down_xyzz(V, 4 * d);
-    V = add_q(V, o);  // virtual lanes >= 8 - d add stray values; only lane 0's sum is kept
-  }
-  if (vl == 0 && q == 0) {
-    const uint32_t* w = reinterpret_cast<const uint32_t*>(&V);
-    for (int k = 0; k < XW; k++) sh[warp][k] = w[k];
-  }
+  // reduction of V over the virtual threads
+  cur ^= 1;  // the buffer no step reads any more
+  put(cur, u, V);
   __syncthreads();
-  if (warp == 0) {
-    XYZZ<F> t = XYZZ<F>::inf();
-    if (vl < NW) {
-      uint32_t* w = reinterpret_cast<uint32_t*>(&t);
-      for (int k = 0; k < XW; k++) w[k] = sh[vl][k];
-    }
 #pragma unroll 1
-    for (int d = 4; d > 0; d >>= 1) {
-      const XYZZ<F> o = shfl_down_xyzz(t, 4 * d);
-      t = add_q(t, o);
-    }
-    if (vl == 0 && q == 0) st_xyzz<F>(wsum + (size_t)j * XW, t);
+  for (uint32_t d = VT / 2; d >= 1; d >>= 1) {
+    const bool has = u < d;
+    const XYZZ<F> o = has ? get(cur, u + d) : XYZZ<F>::inf();
+    V = xyzz_select(has, add_q(V, o), V);
+    cur ^= 1;
+    put(cur, u, V);
+    __syncthreads();
   }
+  if (u == 0 && lead) st_xyzz<F>(wsum + (size_t)j * XW, V);
 }
 
 // sum_j 2^(c j) S_j (Horner over the windows) and the affine result.
@@ -1068,17 +1054,22 @@ int accumulate_grid(int dev, int sms) {
 }
 
 // One level of the bucket reduction (level 0: y = the buckets, z = null): one thread per
-// output segment while the level is too large to run four times over in the resident
-// threads (least work, for full GPUs), else one quad per segment (quad point operations:
-// about a third of the chain's latency for a fifth more work).
+// output segment while the level's groups would not fit the resident threads (least work,
+// for full GPUs), else one group per segment (group point operations: a fraction of the
+// chain's latency for a little more work).
 template <class F>
 void reduce_level(const uint32_t* y, const uint32_t* z, uint32_t n, uint32_t nout, int W, int level,
                   uint32_t* yout, uint32_t* zout, uint64_t resident, cudaStream_t st) {
   const uint64_t outs = (uint64_t)W * nout;
-  if (z && outs * 8 <= resident)
-    k_reduce_level_quad2<F><<<(uint32_t)((outs * 8 + 127) / 128), 128, 0, st>>>(y, z, n, nout, W, level, yout, zout);
-  else if (outs * 4 <= resident)
-    k_reduce_level_quad<F><<<(uint32_t)((outs * 4 + 127) / 128), 128, 0, st>>>(y, z, n, nout, W, level, yout, zout);
+  // group forms while their lanes fit the resident threads once (G lanes per point
+  // operation: 4 over Fq, 16 over Fq2); letting 16-lane groups run up to four times over
+  // slowed a 2^20 proof 26.0 -> 26.8 ms and a batch of 16 proofs of 2^12 3.57 -> 3.94 ms
+  constexpr uint64_t G = GroupLanes<F>::value;
+  if (z && outs * 2 * G <= resident)
+    k_reduce_level_quad2<F><<<(uint32_t)((outs * 2 * G + 127) / 128), 128, 0, st>>>(y, z, n, nout, W, level, yout,
+                                                                                   zout);
+  else if (outs * G <= resident)
+    k_reduce_level_quad<F><<<(uint32_t)((outs * G + 127) / 128), 128, 0, st>>>(y, z, n, nout, W, level, yout, zout);
   else
     k_reduce_level<F><<<(uint32_t)((outs + 127) / 128), 128, 0, st>>>(y, z, n, nout, W, level, yout, zout);
   note_launch();
@@ -1248,7 +1239,7 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
     nseg = nnext;
     levels++;
   }
-  constexpr int WT = kWsumThreads;
+  constexpr int WT = WsumThreads<F>::single;
   k_window_sum<F, WT><<<WR, WT, 0, st>>>(y, z, nseg, 3 * levels, wsum);
   note_launch();
   k_finish<F><<<1, 32, 0, st>>>(wsum, WR, c, d_out);
