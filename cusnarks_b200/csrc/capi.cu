@@ -33,7 +33,7 @@ cudaError_t ctx_aux_init(cs_ctx* ctx) {
   for (int i = 0; i < 4 && e == cudaSuccess; i++)
     if (!ctx->aux[i]) e = cudaStreamCreateWithPriority(&ctx->aux[i], cudaStreamNonBlocking, prio[i]);
   if (e == cudaSuccess && !ctx->aux_h) e = cudaStreamCreateWithPriority(&ctx->aux_h, cudaStreamNonBlocking, prio_h);
-  for (int i = 0; i < 8 && e == cudaSuccess; i++)
+  for (int i = 0; i < cs_ctx::kAuxEvents && e == cudaSuccess; i++)
     if (!ctx->aux_ev[i]) e = cudaEventCreate(&ctx->aux_ev[i]);  // timed: prove stage times
   if (e == cudaSuccess) ctx->aux_ready = true;
   return e;
@@ -186,7 +186,7 @@ void cs_ctx_destroy(cs_ctx* ctx) {
   for (int i = 0; i < 4; i++)
     if (ctx->aux[i]) { cudaStreamSynchronize(ctx->aux[i]); cudaStreamDestroy(ctx->aux[i]); }
   if (ctx->aux_h) { cudaStreamSynchronize(ctx->aux_h); cudaStreamDestroy(ctx->aux_h); }
-  for (int i = 0; i < 8; i++)
+  for (int i = 0; i < cs_ctx::kAuxEvents; i++)
     if (ctx->aux_ev[i]) cudaEventDestroy(ctx->aux_ev[i]);
   delete ctx;
 }

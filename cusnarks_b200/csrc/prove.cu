@@ -324,14 +324,20 @@ cudaError_t prove_body(cs_ctx* ctx, cs_pk* pk, const ProvePlan& P, const uint32_
        (e = cudaMemcpyAsync(M + (size_t)(2 * m - 1) * 8, rs + 16, 32, cudaMemcpyDeviceToDevice, sh)) == cudaSuccess &&
        (e = run_msm(false, M + (size_t)m * 8, pk->h_ext, pk->fh, m, outH, P.ms_h, P.bytes_h, sh, &share_h)) == cudaSuccess;
   if (!ok) { *where = "prove QAP/H"; return e; }
-  for (int i = 0; i < 4; i++) {
+  // pi_C needs the A, B1, C and H chains but not the G2 MSM: it runs on the H stream while
+  // B2 may still be running, and the context stream joins both (2^12 proof: the G2 chain ends
+  // last, so pi_C's affine conversion no longer follows it)
+  cudaEventRecord(ctx->aux_ev[5], sh);  // H MSM done (stage times)
+  for (int i : {0, 1, 3}) {
     cudaEventRecord(ctx->aux_ev[1 + i], ctx->aux[i]);
-    cudaStreamWaitEvent(s0, ctx->aux_ev[1 + i], 0);
+    cudaStreamWaitEvent(sh, ctx->aux_ev[1 + i], 0);
   }
-  cudaEventRecord(ctx->aux_ev[5], sh);
-  cudaStreamWaitEvent(s0, ctx->aux_ev[5], 0);
-  k_final_c<<<1, 32, 0, s0>>>(outH, outC, sA, rB1, piC);
+  k_final_c<<<1, 32, 0, sh>>>(outH, outC, sA, rB1, piC);
   note_launch();
+  cudaEventRecord(ctx->aux_ev[3], ctx->aux[2]);  // B2 done
+  cudaEventRecord(ctx->aux_ev[8], sh);           // pi_C done
+  cudaStreamWaitEvent(s0, ctx->aux_ev[3], 0);
+  cudaStreamWaitEvent(s0, ctx->aux_ev[8], 0);
   return cudaGetLastError();
 }
 

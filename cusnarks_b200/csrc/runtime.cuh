@@ -95,7 +95,8 @@ struct cs_ctx {
   // auxiliary streams / events for fork-join pipelines (prove), created on first use
   cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaStream_t aux_h = nullptr;  // QAP -> H step -> H MSM chain of a proof
-  cudaEvent_t aux_ev[8] = {nullptr};
+  static constexpr int kAuxEvents = 9;
+  cudaEvent_t aux_ev[kAuxEvents] = {nullptr};
   bool aux_ready = false;
   // Proof launch sequences captured as CUDA graphs (prove.cu): one per key, witness buffer
   // and scratch arena, replayed while all three are those of the capture.
