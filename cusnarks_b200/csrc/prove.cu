@@ -488,13 +488,17 @@ __global__ void k_batch_rs(char* __restrict__ base, size_t per, size_t o_rs, siz
   M[threadIdx.x] = rs[threadIdx.x];
 }
 
-// pi_C of every proof (block k) and the proof words to the caller's buffer.
+// pi_C of every proof (block k): needs the G1 MSMs, their scalings and the H MSMs, not G2.
+__global__ void k_batch_pic(char* __restrict__ base, size_t per, size_t o_pts) {
+  uint32_t* pts = reinterpret_cast<uint32_t*>(base + (size_t)blockIdx.x * per + o_pts);
+  if (threadIdx.x == 0) final_c(pts + 80, pts + 64, pts + 96, pts + 128, pts + 160);
+}
+
+// The proof words of every proof (block k) to the caller's buffer.
 __global__ void k_batch_final(const BatchCall* __restrict__ calls, char* __restrict__ base, size_t per,
                               size_t o_pts) {
   const uint32_t k = blockIdx.x;
-  uint32_t* pts = reinterpret_cast<uint32_t*>(base + (size_t)k * per + o_pts);
-  if (threadIdx.x == 0) final_c(pts + 80, pts + 64, pts + 96, pts + 128, pts + 160);
-  __syncthreads();
+  const uint32_t* pts = reinterpret_cast<const uint32_t*>(base + (size_t)k * per + o_pts);
   const uint32_t t = threadIdx.x;  // 64 threads: pi_A (16) | pi_B (32) | pi_C (16)
   if (t < 64) {
     const uint32_t v = t < 16 ? pts[t] : t < 48 ? pts[32 + (t - 16)] : pts[160 + (t - 48)];
@@ -530,12 +534,15 @@ cudaError_t prove_batch_body(cs_ctx* ctx, cs_pk* pk, ProveBatch& B, Domain* dom1
     note_launch();
   }
   if ((e = batch_enqueue(B.g1h, sh)) != cudaSuccess) { *where = "prove batch H MSMs"; return e; }
+  // pi_C beside the G2 batch (on the H stream once the G1 side is done), then the proof words
   cudaEventRecord(ctx->aux_ev[1], sa);
+  cudaStreamWaitEvent(sh, ctx->aux_ev[1], 0);
+  k_batch_pic<<<K, 32, 0, sh>>>(base, B.per, B.o_pts);
   cudaEventRecord(ctx->aux_ev[2], sb);
   cudaEventRecord(ctx->aux_ev[5], sh);
-  for (int i : {1, 2, 5}) cudaStreamWaitEvent(s0, ctx->aux_ev[i], 0);
+  for (int i : {2, 5}) cudaStreamWaitEvent(s0, ctx->aux_ev[i], 0);
   k_batch_final<<<K, 64, 0, s0>>>(B.calls(), base, B.per, B.o_pts);
-  note_launch();
+  note_launch(2);
   return cudaGetLastError();
 }
 
