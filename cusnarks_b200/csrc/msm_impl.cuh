@@ -658,9 +658,9 @@ __global__ void __launch_bounds__(128) k_reduce_level_quad2(const uint32_t* __re
 // 2^shift.  One block per window, E consecutive segments per virtual thread u:
 //   V_u = Y_u + Z_u + G * sum_i i*y_{uE+i}      (Y_u, Z_u: the thread's totals)
 //   sum_t t*y_t = sum_u [sum_i i*y_{uE+i}] + E * sum_{u>=1} Suf(u),  Suf(u) = sum_{v>=u} Y_v
-// so S_j = sum_u (V_u + G E * Suf(u) [u >= 1]): a suffix scan and a reduction over the block's
-// virtual threads, about 2E + 2 log2(VT) + shift dependent point operations instead of a serial
-// pass over the segments.
+// so S_j = sum_u (Y_u + Z_u + G (W_u + E Suf(u) [u >= 1])) with W_u = sum_i i*y_{uE+i}: a suffix
+// scan and a reduction over the block's virtual threads, about 3E + 2 log2(VT) + shift
+// dependent point operations instead of a serial pass over the segments.
 // Threads of the per-window sum (one block per window).  128 (4 warps, one per SM
 // sub-partition) shortens each dependent point operation enough to pay for the longer chains
 // of 32 virtual threads: 2^12 proof 2.00 -> 1.91 ms, G2 2^12 fixed-base MSM 1.68 -> 1.58 ms.
@@ -716,13 +716,9 @@ __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restri
     acc = add_q(acc, in ? ld_xyzz<F>(yj + (size_t)idx * XW) : XYZZ<F>::inf());
     zs = add_q(zs, in ? ld_xyzz<F>(zj + (size_t)idx * XW) : XYZZ<F>::inf());
   }
-  // V = acc + zs + 2^shift ws (ws is infinity with one segment per thread)
+  // V_u = acc + zs + 2^shift (ws + E Suf(u) [u >= 1]): one chain of shift doublings for both
+  // terms (ws is infinity with one segment per thread)
   XYZZ<F> V = add_q(acc, zs);
-  if (E > 1) {  // uniform
-#pragma unroll 1
-    for (int d = 0; d < shift; d++) ws = dbl_q(ws);
-    V = add_q(V, ws);
-  }
   // inclusive suffix scan of acc over the virtual threads: Suf(u)
   XYZZ<F> suf = acc;
   int cur = 0;
@@ -737,13 +733,13 @@ __global__ void __launch_bounds__(THREADS) k_window_sum(const uint32_t* __restri
     put(cur, u, suf);
     __syncthreads();
   }
-  // C_u = V_u + 2^shift E * Suf(u) for u >= 1 (E is a power of two)
-  {  // computed by every group (uniform), kept where u >= 1 and u E < n1
+  {  // computed by every group (uniform); E Suf(u) kept where u >= 1 and u E < n1
 #pragma unroll 1
-    for (uint32_t m = E; m > 1; m >>= 1) suf = dbl_q(suf);
+    for (uint32_t m = E; m > 1; m >>= 1) suf = dbl_q(suf);  // E is a power of two
+    XYZZ<F> T = xyzz_select(u >= 1 && u * E < n1, add_q(ws, suf), ws);
 #pragma unroll 1
-    for (int d = 0; d < shift; d++) suf = dbl_q(suf);
-    V = xyzz_select(u >= 1 && u * E < n1, add_q(V, suf), V);
+    for (int d = 0; d < shift; d++) T = dbl_q(T);
+    V = add_q(V, T);
   }
   // reduction of V over the virtual threads
   cur ^= 1;  // the buffer no step reads any more
