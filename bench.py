@@ -78,6 +78,9 @@ MONT_PER_MADD = 11     # mixed addition, 7M + 4S (the canonical count of the MSM
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_accumulate launch of
 # the 2^20-term fixed-base G1 MSM (window 20), from an ncu capture of that launch
 ACC_TRAFFIC_BYTES = 1_747_153_664 + 68_581_376
+# smsp__issue_active (fraction of cycles issuing) and the busiest pipes of the same capture:
+# the counter view of the roofline fraction below, whose peak is a builder-measured rate
+ACC_NCU = {"issue_active": 0.593, "pipe_alu": 0.535, "pipe_fp64": 0.485}
 L2_BYTES = 126 * 1024 * 1024
 LOG_M = 20
 R_INT, S_INT = 0x1234567890abcdef, 0xfedcba0987654321
@@ -623,7 +626,8 @@ def run_ours(args, world, rank, local):
                      "kernel": "k_accumulate+k_combine (bucket accumulation of the proof's fixed-base G1 MSMs)",
                      "achieved": round(achieved / 1e12, 4), "peak": round(peak_wide / 1e12, 4),
                      "unit": "T wide products/s", "frac": round(achieved / peak_wide, 4),
-                     "traffic": ACC_TRAFFIC_BYTES, "kernel_ms": round(acc, 4), "units_per_launch": units,
+                     "traffic": ACC_TRAFFIC_BYTES, "ncu": ACC_NCU,
+                     "kernel_ms": round(acc, 4), "units_per_launch": units,
                      "window": window,
                      "basis": "2^20-term fixed-base G1 MSM as in the proof: N*(254/c+1) bucket entries x 11 Montgomery products x 136 32x32->64 "
                               "products / kernel ms (CUDA events around the kernels); peak = live "
