@@ -19,11 +19,11 @@ int msm_window_model(uint32_t n, bool glv) {
   return best;
 }
 
-size_t msm_workspace_bytes(uint32_t n, int c, bool ec2, int affine_mode, int glv_mode) {
+size_t msm_workspace_bytes(uint32_t n, int c, bool ec2, int affine_mode, int glv_mode, int min_task) {
   if (c <= 0) c = msm_default_window(n, ec2);
   const int xb = ec2 ? 256 : 128;
   const bool glv = msm_detail::use_glv(ec2, false, glv_mode, affine_mode, n);
-  return msm_detail::make_layout(n, c, xb, msm_detail::kMinTask, false,
+  return msm_detail::make_layout(n, c, xb, min_task > 0 ? (uint32_t)min_task : 0u, false,
                                  msm_detail::layout_affine(ec2, affine_mode, n, c, false, glv), glv).total;
 }
 
@@ -52,7 +52,7 @@ size_t msm_fixed_table_work_bytes(uint32_t n, bool ec2) {
 
 size_t msm_fixed_workspace_bytes(uint32_t n, int c, bool ec2, int affine_mode) {
   if (c <= 0) c = msm_fixed_window(n, ec2);
-  return msm_detail::make_layout(n, c, ec2 ? 256 : 128, msm_detail::kMinTask, true,
+  return msm_detail::make_layout(n, c, ec2 ? 256 : 128, 0u, true,
                                  msm_detail::layout_affine(ec2, affine_mode, n, c, true)).total;
 }
 

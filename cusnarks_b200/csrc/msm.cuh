@@ -87,7 +87,9 @@ cudaError_t msm_batch_g2(const MsmBatch& b, void* d_work, size_t work_bytes, cud
 
 struct MsmConfig {
   int c = 0;          // window bits; 0 = pick from N
-  int task = 0;       // max points per accumulation task, 32..96 (0: 64, or 96 for buckets of 48+)
+  int task = 0;       // points per accumulation task, 8..96 (0: automatic)
+  int min_task = 0;   // shortest task the workspace is sized for (0: automatic, by the MSM's
+                      // entries; msm_workspace_bytes takes the same value)
   int affine = -1;    // batch-affine halving rounds before the XYZZ accumulation: -1 auto, 0 off
   int glv = -1;       // generic G1 MSMs: split the scalars by the GLV endomorphism (-1 auto = on, 0 off)
   // optional events recorded around the bucket-accumulation kernels (phase timing)
@@ -105,7 +107,8 @@ struct MsmConfig {
 // Bytes of device scratch one MSM of n terms needs (G2 when ec2).
 // affine_mode: batch-affine rounds the MSM will run (-1 automatic, 0 none, > 0 that many).
 // glv_mode: as MsmConfig::glv (G1 only).
-size_t msm_workspace_bytes(uint32_t n, int c, bool ec2, int affine_mode = -1, int glv_mode = -1);
+// min_task: the MsmConfig::min_task the call will use (0 automatic).
+size_t msm_workspace_bytes(uint32_t n, int c, bool ec2, int affine_mode = -1, int glv_mode = -1, int min_task = 0);
 // Window for n terms: G1 for the GLV split (2n terms of 128 bits), G2 for n of 254 bits.
 int msm_default_window(uint32_t n, bool ec2);
 // The cost model's window for n terms with (glv) or without the GLV split.

@@ -18,11 +18,15 @@ constexpr uint32_t NEG_BIT = 0x80000000u;
 // (terms below 2^30).
 constexpr uint32_t PHI_BIT = 0x40000000u;
 constexpr uint32_t kMinTask = 32;  // workspace bounds assume tasks of at least this size
-// ... except for MSMs of at most kSmallEntries bucket entries, whose bounds assume tasks of
-// kLatMinTask: the latency form splits their buckets in tasks of 16 (2^12 fixed-base G1 MSM
-// 0.469 -> 0.445 ms, 2^12 proof 1.586 -> 1.533 ms against 32; 8 is slower: more partial sums)
+// ... except for smaller MSMs: their bounds assume tasks of layout_min_task(entries), down to 8
+// entries, so the bound stays near 65,536 tasks.  The latency form splits buckets of MSMs of
+// at most kSmallEntries entries in tasks of 16 (2^12 fixed-base G1 MSM 0.469 -> 0.445 ms, 2^12
+// proof 1.586 -> 1.533 ms against 32; 8 is slower: more partial sums).
 constexpr size_t kSmallEntries = 1u << 19;
 constexpr uint32_t kLatMinTask = 16;
+inline uint32_t layout_min_task(uint64_t entries) {
+  return (uint32_t)std::min<uint64_t>(kMinTask, std::max<uint64_t>(8, entries / 65536));
+}
 
 __host__ __device__ inline int num_windows(int c) { return SCALAR_BITS / c + 1; }
 // Windows of a GLV half-scalar (|k1|, |k2| < 2^127): c W >= 128 leaves the top digit at most
@@ -957,6 +961,7 @@ struct Layout {
 
 static inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// task_len: the shortest task the MSM will run (0: automatic, layout_min_task of its entries).
 inline Layout make_layout(uint32_t n, int c, int xyzz_bytes, uint32_t task_len, bool fixed = false,
                           bool affine = true, bool glv = false) {
   const int W = msm_windows(c, glv);
@@ -964,7 +969,7 @@ inline Layout make_layout(uint32_t n, int c, int xyzz_bytes, uint32_t task_len, 
   const size_t nb = fixed ? ((size_t)1 << (c - 1)) : (size_t)W << (c - 1);
   const int WR = fixed ? 1 : W;  // bucket sets reduced
   const size_t ne = nt * W;
-  if (ne <= kSmallEntries) task_len = std::min<uint32_t>(task_len, kLatMinTask);
+  if (task_len == 0) task_len = layout_min_task(ne);
   const size_t max_tasks = nb + ne / task_len + 1;
   const size_t max_partials = 2 * (ne / task_len) + 1;
   const size_t n1 = ((size_t)1 << (c - 1)) / 8 + 1;
@@ -1097,7 +1102,6 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   if (FIXED && cfg.c <= 0) return cudaErrorInvalidValue;  // the table fixes the window
   const int c = cfg.c > 0 ? cfg.c : msm_default_window(n_in, EC2);
   if (c < 4 || c > 24) return cudaErrorInvalidValue;
-  uint32_t task_len = cfg.task > 0 ? (uint32_t)cfg.task : 64u;  // automatic: 64, or 96 below
   const bool glv = use_glv(EC2, FIXED, cfg.glv, cfg.affine, n_in);
   const int W = msm_windows(c, glv);
   // entry positions are uint32 and fixed-base entries carry a table index below the sign bit
@@ -1112,14 +1116,26 @@ cudaError_t msm_impl(const uint32_t* d_scalars, const uint32_t* d_points, uint32
   // four times over runs in latency form (one quad per task, shortest tasks)
   const uint64_t resident = (uint64_t)accumulate_grid<F>(dev, sms) * 128;
   const bool latency_mode = rounds_req == 0 && ((uint64_t)nb + (uint64_t)n * W / kMinTask + 1) * 4 <= resident;
-  // Automatic tile: 96 entries where buckets average 48 or more (a GLV-split 2^20 MSM averages
-  // 64: tiles of 64 split half its buckets and the partial sums cost a combine pass; 2^20
-  // 5.16 -> 5.07 ms, 2^22 17.8 -> 17.3 ms), else 64; the latency form the shortest.
-  if (cfg.task <= 0 && (uint64_t)n * W >= 48ull * nb) task_len = 96;
-  if (task_len < kMinTask) task_len = kMinTask;
+  // Automatic tile: about one task per resident thread, so a mid-size MSM (too many tasks for
+  // the latency form, too few to fill the GPU at 64 entries a task) still keeps every thread
+  // busy; 64 entries at most, or 96 where buckets average 48 or more (a GLV-split 2^20 MSM
+  // averages 64: tiles of 64 split half its buckets and the partial sums cost a combine pass;
+  // 2^20 5.16 -> 5.07 ms, 2^22 17.8 -> 17.3 ms); the latency form the shortest.
+  const uint64_t ne = (uint64_t)n * W;
+  const uint32_t tmin = cfg.min_task > 0 ? (uint32_t)cfg.min_task : layout_min_task(ne);  // the layout's bound
+  uint32_t task_len;
+  if (cfg.task > 0) {
+    task_len = (uint32_t)cfg.task;
+  } else {
+    const uint64_t room = resident > nb / 2 + 1024 ? resident - nb / 2 : resident / 2;  // split buckets
+    task_len = (uint32_t)std::min<uint64_t>(64, (ne + room - 1) / room);
+    if (task_len == 64 && ne >= 48ull * nb) task_len = 96;
+  }
+  if (latency_mode) task_len = ne <= kSmallEntries ? kLatMinTask : kMinTask;
+  task_len = std::max(task_len, tmin);  // the workspace is sized for tasks of at least tmin entries
   if (task_len > (uint32_t)kMaxTask) task_len = kMaxTask;
-  if (latency_mode) task_len = (uint64_t)n * W <= kSmallEntries ? kLatMinTask : kMinTask;
-  const Layout L = make_layout(n_in, c, XB, kMinTask, FIXED, layout_affine(EC2, cfg.affine, n_in, c, FIXED, glv), glv);
+  const Layout L = make_layout(n_in, c, XB, cfg.min_task > 0 ? (uint32_t)cfg.min_task : 0u, FIXED,
+                               layout_affine(EC2, cfg.affine, n_in, c, FIXED, glv), glv);
   if (work_bytes < L.total || d_work == nullptr) return cudaErrorInvalidValue;
   char* base = static_cast<char*>(d_work);
   uint32_t* counters = reinterpret_cast<uint32_t*>(base + L.counters);

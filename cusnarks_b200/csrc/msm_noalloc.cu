@@ -23,6 +23,7 @@
 namespace {
 
 constexpr size_t kScratchBytes = 32ull << 20;  // 32 MiB: G1 MSMs of up to 2^16 terms
+constexpr int kTask = 32;  // shortest accumulation task: the array's size is fixed on it
 static __device__ __align__(256) unsigned char g_msm_scratch[kScratchBytes];
 
 std::mutex g_mu;
@@ -39,7 +40,7 @@ uint32_t cs_msm_g1_noalloc_max_terms(void) {
   uint32_t lo = 0, hi = 1u << 24;
   while (lo < hi) {  // largest n whose automatic-window workspace fits the array
     const uint32_t mid = lo + (hi - lo + 1) / 2;
-    if (csb::msm_workspace_bytes(mid, 0, false, 0, 0) <= kScratchBytes) lo = mid; else hi = mid - 1;
+    if (csb::msm_workspace_bytes(mid, 0, false, 0, 0, kTask) <= kScratchBytes) lo = mid; else hi = mid - 1;
   }
   return lo;
 }
@@ -53,7 +54,7 @@ int cs_msm_g1_noalloc(const uint32_t* d_scalars, const uint32_t* d_points, uint3
     t_noalloc_err = "cs_msm_g1_noalloc: null pointer argument";
     return CS_ERR_ARG;
   }
-  const size_t need = csb::msm_workspace_bytes(n, 0, false, 0, 0);
+  const size_t need = csb::msm_workspace_bytes(n, 0, false, 0, 0, kTask);
   if (need > kScratchBytes) {
     t_noalloc_err = "cs_msm_g1_noalloc: " + std::to_string(n) + " terms need " + std::to_string(need) +
                     " bytes of scratch, above the fixed " + std::to_string(kScratchBytes) +
@@ -87,6 +88,7 @@ int cs_msm_g1_noalloc(const uint32_t* d_scalars, const uint32_t* d_points, uint3
   csb::MsmConfig cfg;  // automatic window, no timing events
   cfg.affine = 0;      // XYZZ accumulation only: the fixed array is sized without round buffers
   cfg.glv = 0;         // nor the GLV split's buffers (2n scalars and points)
+  cfg.min_task = kTask;  // and for tasks of at least 32 entries
   e = csb::msm_g1(d_scalars, d_points, n, d_out_affine, scratch, kScratchBytes, cfg,
                   static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) {
