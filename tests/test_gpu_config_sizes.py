@@ -188,3 +188,25 @@ def test_prove_2e22_verifies(ctx):
     bad = circ.public_inputs.copy()
     bad[0, 0] ^= 1
     assert not verify(pk["vk"], proof, bad)
+
+
+@pytest.mark.parametrize("log_m", [15, 17])
+def test_prove_mid_sizes_match_cpu(ctx, oracle, log_m):
+    """Proofs of 2^15 and 2^17 constraints, where the MSMs are too large for the latency form
+    and too small to fill the GPU at full-length tasks (their accumulation tasks are sized to
+    the GPU): byte for byte the CPU proving sequence (the reference library where built),
+    and the pairing check."""
+    from cusnarks_b200.groth import SyntheticCircuit, setup_pk, pk_to_host, Prover
+    from oracle.oracle import RefLib
+    from oracle.prover import cpu_prove, verify
+    circ = SyntheticCircuit(ctx, log_m, seed=130 + log_m)
+    pk = setup_pk(ctx, circ, seed=131 + log_m)
+    host = pk_to_host(pk)
+    prover = Prover(ctx, pk)
+    try:
+        proof = prover.prove(circ.w, ints_to_limbs([BENCH_R])[0], ints_to_limbs([BENCH_S])[0])
+    finally:
+        prover.close()
+    ref = RefLib.get() if RefLib.available() else None
+    assert np.array_equal(proof, cpu_prove(oracle, host, circ.w, BENCH_R, BENCH_S, ref=ref))
+    assert verify(host["vk"], proof, circ.public_inputs)
