@@ -11,7 +11,8 @@ reference's own CPU library (oracle/_ref), never GPU against GPU:
   fixed-base table and the G1 MSMs the throughput form of the bucket accumulation.
 The CPU builder of the benchmark circuit and key (oracle/synth_cpu.py, which bench.py's
 reference arm uses) is checked against the GPU builder word for word.  A 2^22-constraint proof
-is checked by the pairing equation.
+is checked by the pairing equation; proofs of 2^15 and 2^17 constraints and a generic G2 MSM of
+2^15 terms (mid sizes, whose accumulation tasks are sized to the GPU) against the CPU.
 """
 import numpy as np
 import pytest
@@ -210,3 +211,18 @@ def test_prove_mid_sizes_match_cpu(ctx, oracle, log_m):
     ref = RefLib.get() if RefLib.available() else None
     assert np.array_equal(proof, cpu_prove(oracle, host, circ.w, BENCH_R, BENCH_S, ref=ref))
     assert verify(host["vk"], proof, circ.public_inputs)
+
+
+def test_g2_generic_msm_2e15(ctx, oracle):
+    """A generic (no table) G2 MSM of 2^15 terms, a mid size whose accumulation tasks are sized
+    to the GPU: equal to the oracle (and the reference library where built)."""
+    from oracle.oracle import RefLib
+    from oracle.synth_cpu import fixed_base_mul
+    n = 1 << 15
+    rng = np.random.Generator(np.random.PCG64(315))
+    pts = fixed_base_mul(oracle, random_field(rng, n, 1), ec2=True)
+    s = random_field(rng, n, 1)
+    want = oracle.msm(s, pts, ec2=1)
+    if RefLib.available():
+        assert np.array_equal(RefLib.get().msm(s, pts, 1, 6), want)
+    assert np.array_equal(ctx.msm(s, pts, ec2=True), want)
