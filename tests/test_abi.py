@@ -84,3 +84,19 @@ def test_reference_cython_module_links_this_library():
         sys.path.remove(d)
     for name in ("ec_jacreduce_h", "ntt_h", "intt_h", "ntt_interpolandmul_h", "mpoly_eval_h"):
         assert callable(getattr(mod, name))
+
+
+def test_window_and_workspace_queries_need_no_device():
+    """The sizing queries are host arithmetic: windows by the cost models (G1 for 2n
+    GLV half-scalars, G2 for full scalars), scratch bytes for each, and the allocation-free
+    entry point's term limit, which stays at or above 2^16 terms."""
+    from cusnarks_b200 import lib
+    L = lib()
+    assert L.cs_msm_default_window(1 << 20, 0) == 16   # G1: 2^21 half-scalars of 8 windows
+    assert L.cs_msm_num_windows(16) == 16               # a full scalar: 254 / 16 + 1
+    for n in (1 << 10, 1 << 16, 1 << 20):
+        for ec2 in (0, 1):
+            assert L.cs_msm_workspace_bytes(n, ec2, 0) > 0
+            assert L.cs_msm_fixed_workspace_bytes(n, ec2, 0) > 0
+    assert L.cs_msm_noalloc_scratch_bytes() == 32 << 20
+    assert L.cs_msm_g1_noalloc_max_terms() >= 1 << 16
